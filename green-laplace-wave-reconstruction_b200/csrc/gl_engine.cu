@@ -1,0 +1,1748 @@
+// Host side of the Green--Laplace engine: plan creation, workspace layout,
+// the per-group launch sequence and the C ABI declared in include/gl_engine.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gl_engine.h"
+#include "gl_kernels.cuh"
+
+using namespace gl;
+
+// ---------------------------------------------------------------------------
+// error plumbing
+// ---------------------------------------------------------------------------
+
+static thread_local std::string g_last_error;
+
+static gl_status fail(gl_status s, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return s;
+}
+
+#define CUDA_TRY(expr)                                                               \
+  do {                                                                               \
+    cudaError_t e_ = (expr);                                                         \
+    if (e_ != cudaSuccess)                                                           \
+      return fail(GL_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(e_));      \
+  } while (0)
+
+#define LAUNCH_CHECK(what)                                                           \
+  do {                                                                               \
+    cudaError_t e_ = cudaGetLastError();                                             \
+    if (e_ != cudaSuccess)                                                           \
+      return fail(GL_ERR_CUDA, "launch of %s failed: %s", what, cudaGetErrorString(e_)); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// analysis kernels
+// ---------------------------------------------------------------------------
+
+// Geometry planes of a box on the reference grid.  kx follows numpy's
+// 2*pi*fftfreq(nx, d=lx/nx) evaluation order (_spectral.py:9-16).
+__global__ void geo_kernel(double* geo, Box box, int nx, int ny, double lx, double ly,
+                           double depth) {
+  const int plane = box.w * box.h;
+  const double valx = 1.0 / ((double)nx * (lx / (double)nx));
+  const double valy = 1.0 / ((double)ny * (ly / (double)ny));
+  const double two_pi = 6.283185307179586;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
+    const int mx = box.x0 + i % box.w;
+    const int my = box.y0 + i / box.w;
+    const double kx = two_pi * ((double)mx * valx);
+    const double ky = two_pi * ((double)my * valy);
+    const double qx = depth * kx, qy = depth * ky;
+    const double q = hypot(qx, qy);
+    const double a = q * tanh(q);
+    geo[i] = qx;
+    geo[plane + i] = qy;
+    geo[2 * plane + i] = q;
+    geo[3 * plane + i] = sqrt(a);
+    geo[4 * plane + i] = a;
+    geo[5 * plane + i] = sqrt(a);
+  }
+}
+
+__global__ void twiddle_kernel(cplx* tw) {
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < TW_N; m += gridDim.x * blockDim.x) {
+    double s, c;
+    sincospi(2.0 * (double)m / (double)TW_N, &s, &c);
+    tw[m] = cmk(c, -s);
+  }
+}
+
+__global__ void slots_init_kernel(UnitSlots* slots, int n) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  UnitSlots s;
+  memset(&s, 0, sizeof s);
+  s.nu_min = BITS_POS_INF;
+  s.peak_flat = ~0ull;
+  s.chan_min[0] = s.chan_min[1] = BITS_POS_INF;
+  s.pad[0] = BITS_POS_INF;  // q_min
+  slots[u] = s;
+}
+
+// Full-grid spectra -> box; max |s| over the whole grid; largest |s| outside
+// the box (pad[1]) so a support outside the plan is reported.
+__global__ void extract_kernel(const cplx* full, cplx* boxv, Box box, int nx, int ny,
+                               UnitSlots* slots) {
+  const int u = blockIdx.y;
+  const size_t plane = (size_t)nx * ny;
+  const cplx* s = full + (size_t)u * plane;
+  double lmax = 0.0, lout = 0.0;
+  for (size_t f = (size_t)blockIdx.x * blockDim.x + threadIdx.x; f < plane;
+       f += (size_t)gridDim.x * blockDim.x) {
+    const int iy = (int)(f / nx), ix = (int)(f % nx);
+    const int mx = ix < nx / 2 ? ix : ix - nx;
+    const int my = iy < ny / 2 ? iy : iy - ny;
+    const cplx v = s[f];
+    const double m = cabs_(v);
+    lmax = (m > lmax || m != m) ? m : lmax;
+    const int bx = mx - box.x0, by = my - box.y0;
+    if (bx >= 0 && bx < box.w && by >= 0 && by < box.h) {
+      boxv[(size_t)u * box.w * box.h + by * box.w + bx] = v;
+    } else {
+      lout = (m > lout || m != m) ? m : lout;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double a = __shfl_xor_sync(0xffffffffu, lmax, o);
+    const double b = __shfl_xor_sync(0xffffffffu, lout, o);
+    lmax = (a > lmax || a != a) ? a : lmax;
+    lout = (b > lout || b != b) ? b : lout;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_nonneg(&slots[u].smax, lmax);
+    atomic_max_nonneg(&slots[u].pad[1], lout);
+  }
+}
+
+__global__ void box_max_kernel(const cplx* boxv, int plane, UnitSlots* slots) {
+  const int u = blockIdx.y;
+  double lmax = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
+    const double m = cabs_(boxv[(size_t)u * plane + i]);
+    lmax = (m > lmax || m != m) ? m : lmax;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double a = __shfl_xor_sync(0xffffffffu, lmax, o);
+    lmax = (a > lmax || a != a) ? a : lmax;
+  }
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&slots[u].smax, lmax);
+}
+
+// Parent support and its reductions (spatial.py:163-178, _order3.py:33-47).
+__global__ void support_kernel(const cplx* boxv, const double* geo, Box box, UnitSlots* slots,
+                               unsigned char* s1) {
+  const int u = blockIdx.y;
+  const int plane = box.w * box.h;
+  const double smax = as_double(slots[u].smax);
+  const double thr = 1.0e-13 * (smax > 1.0 ? smax : 1.0);
+  double numin = INFINITY, numax = 0.0, amax = 0.0, qmin = INFINITY;
+  unsigned long long cnt = 0, bad = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
+    const cplx v = boxv[(size_t)u * plane + i];
+    const double m = cabs_(v);
+    if (!(m == m) || m == INFINITY) bad = 1;
+    const bool in = m > thr;
+    s1[(size_t)u * plane + i] = in ? 1 : 0;
+    if (in) {
+      const double nu = geo[3 * plane + i];
+      const double q = geo[2 * plane + i];
+      numin = fmin(numin, nu);
+      numax = fmax(numax, nu);
+      qmin = fmin(qmin, q);
+      const double a2 = m * m;
+      amax = fmax(amax, a2);
+      ++cnt;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    numin = fmin(numin, __shfl_xor_sync(0xffffffffu, numin, o));
+    numax = fmax(numax, __shfl_xor_sync(0xffffffffu, numax, o));
+    qmin = fmin(qmin, __shfl_xor_sync(0xffffffffu, qmin, o));
+    amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (cnt) {
+      atomicMin(&slots[u].nu_min, (unsigned long long)__double_as_longlong(numin));
+      atomicMin(&slots[u].pad[0], (unsigned long long)__double_as_longlong(qmin));
+      atomic_max_nonneg(&slots[u].nu_max, numax);
+      atomic_max_nonneg(&slots[u].amp2_max, amax);
+      atomicAdd(&slots[u].count, cnt);
+    }
+    if (bad) atomicOr(&slots[u].nonfinite, 1ull);
+  }
+}
+
+// First argmax of |s|^2 in reference flat order; radial channel masks and
+// their nu ranges (spatial.py:322-337).
+__global__ void peak_kernel(const cplx* boxv, const double* geo, Box box, int nx, int ny,
+                            UnitSlots* slots, const unsigned char* s1, unsigned char* chan,
+                            int want_channels) {
+  const int u = blockIdx.y;
+  const int plane = box.w * box.h;
+  const double amax = as_double(slots[u].amp2_max);
+  const double lo = as_double(slots[u].nu_min), hi = as_double(slots[u].nu_max);
+  const double step = (hi - lo) / 2.0;
+  const double mid = step == 0.0 ? lo : step + lo;
+  unsigned long long best = ~0ull;
+  double cmin0 = INFINITY, cmax0 = 0.0, cmin1 = INFINITY, cmax1 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
+    const bool in = s1[(size_t)u * plane + i];
+    unsigned char c0 = 0, c1 = 0;
+    if (in) {
+      const double m = cabs_(boxv[(size_t)u * plane + i]);
+      if (m * m == amax) {
+        const int mx = box.x0 + i % box.w, my = box.y0 + i / box.w;
+        const unsigned long long flat =
+            (unsigned long long)wrap(my, ny) * (unsigned long long)nx + (unsigned long long)wrap(mx, nx);
+        best = flat < best ? flat : best;
+      }
+      if (want_channels) {
+        const double nu = geo[3 * plane + i];
+        if (nu >= lo && nu < mid) {
+          c0 = 1;
+          cmin0 = fmin(cmin0, nu);
+          cmax0 = fmax(cmax0, nu);
+        }
+        if (nu >= mid && nu <= hi) {
+          c1 = 1;
+          cmin1 = fmin(cmin1, nu);
+          cmax1 = fmax(cmax1, nu);
+        }
+      }
+    }
+    if (want_channels) {
+      chan[((size_t)u * 2 + 0) * plane + i] = c0;
+      chan[((size_t)u * 2 + 1) * plane + i] = c1;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long ob = __shfl_xor_sync(0xffffffffu, best, o);
+    best = ob < best ? ob : best;
+    cmin0 = fmin(cmin0, __shfl_xor_sync(0xffffffffu, cmin0, o));
+    cmax0 = fmax(cmax0, __shfl_xor_sync(0xffffffffu, cmax0, o));
+    cmin1 = fmin(cmin1, __shfl_xor_sync(0xffffffffu, cmin1, o));
+    cmax1 = fmax(cmax1, __shfl_xor_sync(0xffffffffu, cmax1, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&slots[u].peak_flat, best);
+    if (want_channels) {
+      if (cmin0 != INFINITY) {
+        atomicMin(&slots[u].chan_min[0], (unsigned long long)__double_as_longlong(cmin0));
+        atomic_max_nonneg(&slots[u].chan_max[0], cmax0);
+      }
+      if (cmin1 != INFINITY) {
+        atomicMin(&slots[u].chan_min[1], (unsigned long long)__double_as_longlong(cmin1));
+        atomic_max_nonneg(&slots[u].chan_max[1], cmax1);
+      }
+    }
+  }
+}
+
+// Byte masks [job][h][w] -> forward / reversed bitset rows [job][h][words].
+__global__ void bitrows_kernel(const unsigned char* bytes, int h, int w, int words,
+                               unsigned long long* fwd, unsigned long long* rev) {
+  const int job = blockIdx.y;
+  const int total = h * words;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int row = t / words, wi = t % words;
+    const unsigned char* r = bytes + ((size_t)job * h + row) * w;
+    unsigned long long f = 0ull, b = 0ull;
+    for (int bit = 0; bit < 64; ++bit) {
+      const int x = wi * 64 + bit;
+      if (x < w) {
+        if (r[x]) f |= 1ull << bit;
+        if (r[w - 1 - x]) b |= 1ull << bit;
+      }
+    }
+    fwd[((size_t)job * h + row) * words + wi] = f;
+    rev[((size_t)job * h + row) * words + wi] = b;
+  }
+}
+
+// C = A (+) B as byte masks; optional max sqrt(A) over C (geoC planes).
+struct MinkArgs {
+  const unsigned long long* a;  // fwd rows of A
+  int ha, wa, wwa;
+  long long a_job_stride;       // words between jobs
+  const unsigned long long* brev;
+  int hb, wb, wwb;
+  long long b_job_stride;
+  unsigned char* c;             // [job][hc][wc]
+  int hc, wc;
+  long long c_job_stride;       // bytes between jobs
+  const double* geoc;
+  UnitSlots* slots;
+  int which;                    // 2: sqa_max2, 3: sqa_max3, 0: none
+};
+
+__global__ void minkowski_kernel(MinkArgs m) {
+  const int job = blockIdx.y;
+  const unsigned long long* A = m.a + job * m.a_job_stride;
+  const unsigned long long* B = m.brev + job * m.b_job_stride;
+  unsigned char* C = m.c + job * m.c_job_stride;
+  const int plane = m.hc * m.wc;
+  double lmax = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
+    const int ox = i % m.wc, oy = i / m.wc;
+    const bool in = minkowski_bin(A, m.ha, m.wa, m.wwa, B, m.hb, m.wb, m.wwb, ox, oy);
+    C[i] = in ? 1 : 0;
+    if (in && m.geoc) lmax = fmax(lmax, m.geoc[5 * plane + i]);
+  }
+  if (m.which) {
+    for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    if ((threadIdx.x & 31) == 0)
+      atomic_max_nonneg(m.which == 2 ? &m.slots[job].sqa_max2 : &m.slots[job].sqa_max3, lmax);
+  }
+}
+
+struct ScalarArgs {
+  const UnitSlots* slots;
+  UnitScalars* us;
+  const double* geo1;
+  Box box;
+  int nx, ny;
+  int order;
+  int want_eta22, want_psi22, want_o3;
+  int allow_below;
+  int full_input;
+};
+
+// Scales, shifts and status per unit (spatial.py:179-189, 246-268;
+// _order3.py:35-52).
+__global__ void scalars_kernel(ScalarArgs a, int n) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n) return;
+  const UnitSlots& s = a.slots[u];
+  UnitScalars r;
+  memset(&r, 0, sizeof r);
+  int status = 0;
+  if (s.nonfinite) status = GL_ERR_COMPONENTS;
+  if (!status && s.count == 0) status = GL_ERR_EMPTY_SUPPORT;
+  const double smax = as_double(s.smax);
+  if (!status && a.full_input) {
+    const double thr = 1.0e-13 * (smax > 1.0 ? smax : 1.0);
+    if (as_double(s.pad[1]) > thr) status = GL_ERR_OUTSIDE_PLAN;
+  }
+  const double qmin = as_double(s.pad[0]);
+  if (!status && a.want_o3 && !(qmin > 0.5)) status = GL_ERR_ORDER3_DOMAIN;
+  if (!status && a.want_psi22 && qmin < 0.3 && !a.allow_below) status = GL_ERR_ORDER2_DOMAIN;
+  r.nu_min = as_double(s.nu_min);
+  r.nu_max = as_double(s.nu_max);
+  if (!status) {
+    const unsigned long long flat = s.peak_flat;
+    const int ix = (int)(flat % (unsigned long long)a.nx), iy = (int)(flat / (unsigned long long)a.nx);
+    const int mx = ix < a.nx / 2 ? ix : ix - a.nx;
+    const int my = iy < a.ny / 2 ? iy : iy - a.ny;
+    const int i = (my - a.box.y0) * a.box.w + (mx - a.box.x0);
+    const double qp = a.geo1[2 * a.box.w * a.box.h + i];
+    r.peak_q = qp;
+    const double pnu = sqrt(qp * tanh(qp));
+    const double sqa2 = as_double(s.sqa_max2);
+    r.shift2 = 0.5 * (r.nu_min + sqa2 / 2.0);
+    if (a.want_eta22) {
+      const double t1 = 2.0 * sqrt(qp * tanh(qp));
+      r.lam22 = sqrt(t1 * t1 - 2.0 * qp * tanh(2.0 * qp));
+      if (!(r.lam22 > 0.0) || !isfinite(r.lam22)) status = GL_ERR_SCALE;
+    }
+    if (a.want_psi22) {
+      const double pout = sqrt(2.0 * qp * tanh(2.0 * qp));
+      r.lam_minus = 2.0 * pnu - pout;
+      r.lam_plus = 2.0 * pnu + pout;
+      if (!(r.lam_minus > 0.0) || !isfinite(r.lam_minus) || !(r.lam_plus > 0.0) ||
+          !isfinite(r.lam_plus))
+        status = GL_ERR_SCALE;
+      int cc = 0;
+      for (int c = 0; c < 2; ++c) {
+        if (s.chan_min[c] != BITS_POS_INF) {
+          r.chan_id[cc] = c;
+          r.chan_shift[cc] = 0.5 * (as_double(s.chan_min[c]) + as_double(s.chan_max[c]));
+          ++cc;
+        }
+      }
+      r.chan_count = cc;
+      const double step = (r.nu_max - r.nu_min) / 2.0;
+      r.edge_mid = step == 0.0 ? r.nu_min : step + r.nu_min;
+    }
+    if (a.want_o3) {
+      const double sqa3 = as_double(s.sqa_max3);
+      r.shift3 = 0.5 * (r.nu_min + sqa3 / 3.0);
+      r.lam2 = 2.0 * pnu - sqrt(2.0 * qp * tanh(2.0 * qp));
+      r.lam3 = 3.0 * pnu - sqrt(3.0 * qp * tanh(3.0 * qp));
+      if (!(r.lam2 > 0.0) || !(r.lam3 > 0.0)) status = GL_ERR_SCALE;
+    }
+  }
+  r.status = status;
+  a.us[u] = r;
+}
+
+// Deposit N^2 (a+ib)/h e^{-i omega t} per bin segment (gl_spectral_surface.m:123-149).
+__global__ void deposit_kernel(int n_seg, const int* seg_off, const int* seg_bin,
+                               const double* ab, const double* omega, const double* times,
+                               double scale, double depth, cplx* out, int plane) {
+  const int u = blockIdx.y;
+  const double t = times[u];
+  for (int sgi = blockIdx.x * blockDim.x + threadIdx.x; sgi < n_seg; sgi += gridDim.x * blockDim.x) {
+    cplx acc = czero();
+    for (int k = seg_off[sgi]; k < seg_off[sgi + 1]; ++k) {
+      const cplx amp = cmk(ab[2 * k] / depth, ab[2 * k + 1] / depth);
+      double s, c;
+      sincos(omega[k] * t, &s, &c);
+      acc = cadd(acc, cmul(cscale(scale, amp), cmk(c, -s)));
+    }
+    out[(size_t)u * plane + seg_bin[sgi]] = acc;
+  }
+}
+
+__global__ void status_kernel(const UnitScalars* us, int n, int* out) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < n && out) out[u] = us[u].status;
+}
+
+__global__ void nonfinite_kernel(const void* outp, size_t per_unit, int real_only,
+                                 UnitScalars* us) {
+  const int u = blockIdx.y;
+  unsigned int bad = 0;
+  if (real_only) {
+    const double* o = reinterpret_cast<const double*>(outp) + (size_t)u * per_unit;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < per_unit;
+         i += (size_t)gridDim.x * blockDim.x)
+      if (!isfinite(o[i])) bad = 1;
+  } else {
+    const cplx* o = reinterpret_cast<const cplx*>(outp) + (size_t)u * per_unit;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < per_unit;
+         i += (size_t)gridDim.x * blockDim.x)
+      if (!isfinite(o[i].x) || !isfinite(o[i].y)) bad = 1;
+  }
+  bad = __any_sync(0xffffffffu, bad);
+  if (bad && (threadIdx.x & 31) == 0) atomicCAS(&us[u].status, 0, (int)GL_ERR_NONFINITE);
+}
+
+// ---------------------------------------------------------------------------
+// host helpers: Gauss--Laguerre (Golub--Welsch) and dispersion
+// ---------------------------------------------------------------------------
+
+// Eigenvalues of the symmetric tridiagonal Jacobi matrix by implicit-shift QL
+// iterations, tracking the first row of the eigenvector matrix so that the
+// Gauss weights are its squares (Golub & Welsch 1969).
+static bool jacobi_eigen(int n, std::vector<double>& d, std::vector<double> e,
+                         std::vector<double>& z) {
+  z.assign(n, 0.0);
+  z[0] = 1.0;
+  e.resize(n, 0.0);
+  for (int l = 0; l < n; ++l) {
+    int iter = 0;
+    while (true) {
+      int m = l;
+      for (; m < n - 1; ++m) {
+        const double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
+        if (std::fabs(e[m]) <= 1e-300 + 2.220446049250313e-16 * dd) break;
+      }
+      if (m == l) break;
+      if (++iter > 100) return false;
+      double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+      double r = std::hypot(g, 1.0);
+      g = d[m] - d[l] + e[l] / (g + (g >= 0 ? r : -r));
+      double s = 1.0, c = 1.0, p = 0.0;
+      int i = m - 1;
+      bool underflow = false;
+      for (; i >= l; --i) {
+        double f = s * e[i], b = c * e[i];
+        r = std::hypot(f, g);
+        e[i + 1] = r;
+        if (r == 0.0) {
+          d[i + 1] -= p;
+          e[m] = 0.0;
+          underflow = true;
+          break;
+        }
+        s = f / r;
+        c = g / r;
+        g = d[i + 1] - p;
+        r = (d[i] - g) * s + 2.0 * c * b;
+        p = s * r;
+        d[i + 1] = g + p;
+        g = c * r - b;
+        const double zf = z[i + 1];
+        z[i + 1] = s * z[i] + c * zf;
+        z[i] = c * z[i] - s * zf;
+      }
+      if (underflow) continue;
+      d[l] -= p;
+      e[l] = g;
+      e[m] = 0.0;
+    }
+  }
+  return true;
+}
+
+static gl_status gauss_laguerre(int rank, double* nodes, double* weights) {
+  if (rank < 1 || rank > MAX_RANK) return fail(GL_ERR_RANK, "rank must be an integer from 1 to %d", MAX_RANK);
+  std::vector<double> d(rank), e(rank, 0.0), z;
+  for (int i = 0; i < rank; ++i) d[i] = 2.0 * (i + 1) - 1.0;
+  for (int i = 0; i + 1 < rank; ++i) e[i] = (double)(i + 1);
+  if (!jacobi_eigen(rank, d, e, z)) return fail(GL_ERR_RANK, "Golub-Welsch iteration did not converge");
+  std::vector<int> idx(rank);
+  for (int i = 0; i < rank; ++i) idx[i] = i;
+  std::sort(idx.begin(), idx.end(), [&](int a, int b) { return d[a] < d[b]; });
+  for (int i = 0; i < rank; ++i) {
+    nodes[i] = d[idx[i]];
+    weights[i] = z[idx[i]] * z[idx[i]];
+  }
+  // moment gate: sum w x^k = k! for k < 2 rank (quadrature.py:23-30)
+  double fact = 1.0;
+  for (int deg = 0; deg < 2 * rank; ++deg) {
+    if (deg > 0) fact *= deg;
+    long double sum = 0.0L;
+    for (int i = 0; i < rank; ++i) sum += (long double)weights[i] * powl((long double)nodes[i], deg);
+    const double rel = std::fabs((double)sum - fact) / std::max(1.0, fact);
+    if (rel > 3.0e-11)
+      return fail(GL_ERR_RANK, "Gauss--Laguerre moment check failed at rank=%d, degree=%d", rank, deg);
+  }
+  return GL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// plan
+// ---------------------------------------------------------------------------
+
+struct gl_plan {
+  gl_plan_desc d;
+  int comps;                    // GL_COMP_* actually produced
+  int ncomp;
+  int comp_ids[6];
+  int ncx, ncy, lncx, lncy, lnx, lny;
+  Box b1, b2, b3;
+  int ww1, ww2;                 // bitset words per row (S1, S2)
+  bool want_eta22, want_psi22, want_o3, want_first;
+  double* geo1 = nullptr;
+  double* geo2 = nullptr;
+  double* geo3 = nullptr;
+  cplx* tw = nullptr;
+  double* nodes = nullptr;      // device: [eta22 | psi22 | inner | outer] nodes then weights
+  double h_nodes[4][MAX_RANK], h_weights[4][MAX_RANK];
+  int ranks[4];
+  double* comp_scale = nullptr; // device: physical scale per output component
+  double h_comp_scale[6];
+  double floor_rel;
+  int group;
+  // workspace layout (byte offsets), for `group` units
+  size_t ws_total;
+  size_t o_slots, o_us, o_box, o_s1, o_s1f, o_s1r, o_s2, o_s2f, o_s2r, o_s3, o_ch, o_chf, o_chr,
+      o_pm, o_out22, o_outp22, o_out33, o_scratch;
+  size_t scratch_bytes;
+};
+
+static int ilog2(int v) {
+  int l = 0;
+  while ((1 << l) < v) ++l;
+  return l;
+}
+static bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
+static int next_pow2(int v) {
+  int p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
+
+struct Bump {
+  size_t off = 0;
+  size_t take(size_t bytes) {
+    const size_t o = off;
+    off = align_up(off + bytes);
+    return o;
+  }
+};
+
+static const int ROW_GMAX = 4;
+static const size_t SMEM_LIMIT = 227 * 1024;
+
+static size_t row_smem(int nbanks, int ncx) {
+  return (size_t)(nbanks + ROW_GMAX) * ncx * sizeof(cplx);
+}
+
+// Scratch bytes of each stage, for `g` units.
+static size_t stage_scratch(const gl_plan* p, int g) {
+  const size_t c = sizeof(cplx);
+  const size_t b1 = (size_t)p->b1.w * p->b1.h, b2 = (size_t)p->b2.w * p->b2.h,
+               b3 = (size_t)p->b3.w * p->b3.h;
+  const size_t ncy = p->ncy;
+  size_t need = 0;
+  auto upd = [&](size_t v) { need = std::max(need, v); };
+  if (p->want_eta22) {
+    const size_t J = p->ranks[0];
+    Bump b;
+    b.take(g * J * 8 * p->b1.w * ncy * c);
+    b.take(g * J * 2 * p->b2.w * ncy * c);
+    b.take(g * J * 2 * b2 * c);
+    b.take(g * J * 2 * 8);
+    upd(b.off);
+  }
+  if (p->want_psi22) {
+    Bump b;
+    b.take((size_t)g * 8 * 8 * p->b1.w * ncy * c);   // P: jobs (g,2,2,2), 8 banks
+    b.take((size_t)g * 4 * 8 * p->b2.w * ncy * c);   // Q
+    b.take((size_t)g * 4 * 8 * b2 * c);              // R
+    b.take((size_t)g * 2 * p->b1.w * ncy * c);       // contact P
+    b.take((size_t)g * 1 * p->b2.w * ncy * c);       // contact Q
+    b.take((size_t)g * b2 * c);                      // contact R
+    upd(b.off);
+  }
+  if (p->want_o3) {
+    const size_t J = p->ranks[3], I = p->ranks[2];
+    Bump b;
+    b.take(g * J * 4 * b2 * c);  // E
+    b.take(g * J * 8 * 16);      // maxima (E, R_O, F)
+    const size_t base = b.off;
+    Bump in = b;
+    in.take(g * J * I * 12 * p->b1.w * ncy * c);
+    in.take(g * J * I * 4 * p->b2.w * ncy * c);
+    in.take(g * J * I * 4 * b2 * c);
+    in.take(g * J * I * 4 * 8);
+    upd(in.off);
+    Bump out = b;
+    out.take(g * J * 12 * p->b1.w * ncy * c);
+    out.take(g * J * 9 * p->b2.w * ncy * c);
+    out.take(g * J * 4 * p->b3.w * ncy * c);
+    out.take(g * J * 4 * b3 * c);
+    out.take(g * J * 2 * b3 * c);
+    upd(out.off);
+    (void)base;
+  }
+  // final column transforms at the reference ny
+  {
+    const size_t wmax = std::max({(size_t)p->b1.w, (size_t)p->b2.w, (size_t)p->b3.w});
+    upd((size_t)g * 2 * wmax * p->d.ny * c);
+  }
+  (void)b1;
+  return need;
+}
+
+static void plan_free(gl_plan* p) {
+  if (!p) return;
+  cudaFree(p->geo1);
+  cudaFree(p->geo2);
+  cudaFree(p->geo3);
+  cudaFree(p->tw);
+  cudaFree(p->nodes);
+  cudaFree(p->comp_scale);
+  delete p;
+}
+
+extern "C" gl_status gl_plan_create(gl_plan** out, const gl_plan_desc* desc) {
+  if (!out || !desc) return fail(GL_ERR_INVALID_ARGUMENT, "null plan or descriptor");
+  *out = nullptr;
+  const gl_plan_desc& d = *desc;
+  if (d.order < 1 || d.order > 3) return fail(GL_ERR_INVALID_ARGUMENT, "order must be 1, 2, or 3");
+  if (!(d.lx > 0) || !(d.ly > 0) || !std::isfinite(d.lx) || !std::isfinite(d.ly))
+    return fail(GL_ERR_INVALID_ARGUMENT, "positive domain lengths and positive even grid sizes are required");
+  if (d.nx < 2 || d.ny < 2 || (d.nx % 2) || (d.ny % 2))
+    return fail(GL_ERR_INVALID_ARGUMENT, "positive domain lengths and positive even grid sizes are required");
+  if (!is_pow2(d.nx) || !is_pow2(d.ny) || d.nx < 16 || d.ny < 16 || d.nx > TW_N || d.ny > TW_N)
+    return fail(GL_ERR_UNSUPPORTED, "the GPU engine runs power-of-two grids from 16 to %d (got %d x %d)",
+                TW_N, d.ny, d.nx);
+  if (!(d.depth > 0) || !(d.gravity > 0) || !std::isfinite(d.depth) || !std::isfinite(d.gravity))
+    return fail(GL_ERR_INVALID_ARGUMENT, "depth and gravity must be positive");
+  if (d.max_units < 1) return fail(GL_ERR_INVALID_ARGUMENT, "max_units must be >= 1");
+  if (d.output != GL_OUT_COMPLEX && d.output != GL_OUT_REAL)
+    return fail(GL_ERR_INVALID_ARGUMENT, "unknown output mode");
+  if (d.grid != GL_GRID_COMPACT && d.grid != GL_GRID_REFERENCE)
+    return fail(GL_ERR_INVALID_ARGUMENT, "unknown grid mode");
+  int all = GL_COMP_ETA11 | GL_COMP_PSI11;
+  if (d.order >= 2) all |= GL_COMP_ETA22 | GL_COMP_PSI22;
+  if (d.order >= 3) all |= GL_COMP_ETA33 | GL_COMP_PSI33;
+  int comps = d.components ? d.components : all;
+  if (comps & ~all) return fail(GL_ERR_INVALID_ARGUMENT, "component mask asks for a component above the order");
+  if (d.order >= 2 && (d.eta22_rank < 1 || d.eta22_rank > 16))
+    return fail(GL_ERR_RANK, "eta22_rank must be an integer from 1 to 16");
+  const int inner = d.inner_rank ? d.inner_rank : 4, outer = d.outer_rank ? d.outer_rank : 4;
+  if ((comps & (GL_COMP_ETA33 | GL_COMP_PSI33)) &&
+      !((inner == 4 || inner == 6 || inner == 8 || inner == 10 || inner == 12) &&
+        (outer == 3 || outer == 4 || outer == 6 || outer == 8 || outer == 10)))
+    return fail(GL_ERR_RANK, "unsupported inner or outer third-order GL rank");
+  if (d.box_w < 1 || d.box_h < 1) return fail(GL_ERR_INVALID_ARGUMENT, "empty parent box");
+  if (d.box_x0 < 1)
+    return fail(GL_ERR_SUPPORT, "strict-forward nonzero analytic eta1 support is required");
+  const int xmax = d.box_x0 + d.box_w - 1;
+  const int ymax = std::max(std::abs(d.box_y0), std::abs(d.box_y0 + d.box_h - 1));
+  if (xmax >= d.nx / 2 || ymax >= d.ny / 2)
+    return fail(GL_ERR_NYQUIST, "An input component reaches or exceeds a Nyquist boundary.");
+  const bool o3 = comps & (GL_COMP_ETA33 | GL_COMP_PSI33);
+  const bool o2 = comps & (GL_COMP_ETA22 | GL_COMP_PSI22);
+  if (o3 && (3 * xmax >= d.nx / 2 || 3 * ymax >= d.ny / 2))
+    return fail(GL_ERR_ALIAS, "cubic output support reaches a Nyquist boundary");
+  if (o2 && (2 * xmax >= d.nx / 2 || 2 * ymax >= d.ny / 2))
+    return fail(GL_ERR_ALIAS, "quadratic output support reaches a Nyquist boundary");
+
+  gl_plan* p = new gl_plan();
+  p->d = d;
+  p->d.inner_rank = inner;
+  p->d.outer_rank = outer;
+  p->comps = comps;
+  p->ncomp = 0;
+  for (int b = 0; b < 6; ++b)
+    if (comps & (1 << b)) p->comp_ids[p->ncomp++] = 1 << b;
+  p->want_first = comps & (GL_COMP_ETA11 | GL_COMP_PSI11);
+  p->want_eta22 = comps & GL_COMP_ETA22;
+  p->want_psi22 = comps & GL_COMP_PSI22;
+  p->want_o3 = o3;
+  p->b1 = Box{d.box_x0, d.box_y0, d.box_w, d.box_h};
+  p->b2 = Box{2 * d.box_x0, 2 * d.box_y0, 2 * (d.box_w - 1) + 1, 2 * (d.box_h - 1) + 1};
+  p->b3 = Box{3 * d.box_x0, 3 * d.box_y0, 3 * (d.box_w - 1) + 1, 3 * (d.box_h - 1) + 1};
+  p->ww1 = (p->b1.w + 63) / 64;
+  p->ww2 = (p->b2.w + 63) / 64;
+  const int deg = o3 ? 3 : (o2 ? 2 : 1);
+  if (d.grid == GL_GRID_REFERENCE || deg == 1) {
+    p->ncx = d.nx;
+    p->ncy = d.ny;
+  } else {
+    const Box& bd = deg == 3 ? p->b3 : p->b2;
+    p->ncx = std::min(d.nx, std::max(16, next_pow2(bd.w)));
+    p->ncy = std::min(d.ny, std::max(16, next_pow2(bd.h)));
+  }
+  p->lncx = ilog2(p->ncx);
+  p->lncy = ilog2(p->ncy);
+  p->lnx = ilog2(d.nx);
+  p->lny = ilog2(d.ny);
+  const int max_banks = o3 ? 21 : (p->want_psi22 ? 16 : 8);
+  if (deg > 1 && row_smem(max_banks, p->ncx) > SMEM_LIMIT) {
+    plan_free(p);
+    return fail(GL_ERR_UNSUPPORTED,
+                "product grid %d x %d exceeds the shared-memory row budget (use the compact grid)",
+                d.ny, d.nx);
+  }
+  p->floor_rel = 16.0 * 2.220446049250313e-16 * std::max(1.0, std::log2((double)d.nx * (double)d.ny));
+  p->ranks[0] = d.order >= 2 ? d.eta22_rank : 1;
+  p->ranks[1] = 2;
+  p->ranks[2] = inner;
+  p->ranks[3] = outer;
+  for (int k = 0; k < 4; ++k) {
+    if (k == 1) continue;
+    gl_status st = gauss_laguerre(p->ranks[k], p->h_nodes[k], p->h_weights[k]);
+    if (st != GL_OK) {
+      plan_free(p);
+      return st;
+    }
+  }
+  {  // fixed dual-branch GL2 rule (spatial.py:269-275)
+    const double r2 = std::sqrt(2.0);
+    p->h_nodes[1][0] = 2.0 - r2;
+    p->h_nodes[1][1] = 2.0 + r2;
+    p->h_weights[1][0] = p->h_nodes[1][0] / (4.0 * (r2 - 1.0) * (r2 - 1.0));
+    p->h_weights[1][1] = p->h_nodes[1][1] / (4.0 * (r2 + 1.0) * (r2 + 1.0));
+  }
+  const double pscale = d.depth * std::sqrt(d.gravity * d.depth);
+  for (int c = 0; c < p->ncomp; ++c) {
+    const int id = p->comp_ids[c];
+    p->h_comp_scale[c] = (id == GL_COMP_ETA11 || id == GL_COMP_ETA22 || id == GL_COMP_ETA33) ? d.depth : pscale;
+  }
+  // device tables
+  cudaError_t e = cudaSuccess;
+  auto geo_alloc = [&](double** g, const Box& b) {
+    if (e == cudaSuccess) e = cudaMalloc(g, sizeof(double) * 6 * b.w * b.h);
+    if (e == cudaSuccess) {
+      const int plane = b.w * b.h;
+      geo_kernel<<<std::min(1024, (plane + 255) / 256), 256>>>(*g, b, d.nx, d.ny, d.lx, d.ly, d.depth);
+      e = cudaGetLastError();
+    }
+  };
+  geo_alloc(&p->geo1, p->b1);
+  geo_alloc(&p->geo2, p->b2);
+  geo_alloc(&p->geo3, p->b3);
+  if (e == cudaSuccess) e = cudaMalloc(&p->tw, sizeof(cplx) * TW_N);
+  if (e == cudaSuccess) {
+    twiddle_kernel<<<TW_N / 256, 256>>>(p->tw);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&p->nodes, sizeof(double) * 8 * MAX_RANK);
+  if (e == cudaSuccess) {
+    double host[8 * MAX_RANK];
+    for (int k = 0; k < 4; ++k) {
+      std::memcpy(host + k * MAX_RANK, p->h_nodes[k], sizeof(double) * MAX_RANK);
+      std::memcpy(host + (4 + k) * MAX_RANK, p->h_weights[k], sizeof(double) * MAX_RANK);
+    }
+    e = cudaMemcpy(p->nodes, host, sizeof host, cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&p->comp_scale, sizeof(double) * 6);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(p->comp_scale, p->h_comp_scale, sizeof(double) * 6, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    plan_free(p);
+    return fail(GL_ERR_CUDA, "plan set-up failed: %s", cudaGetErrorString(e));
+  }
+  // workspace layout
+  const int g = d.max_units;
+  p->group = g;
+  const size_t c = sizeof(cplx);
+  const size_t b1 = (size_t)p->b1.w * p->b1.h, b2 = (size_t)p->b2.w * p->b2.h,
+               b3 = (size_t)p->b3.w * p->b3.h;
+  Bump b;
+  p->o_slots = b.take(g * sizeof(UnitSlots));
+  p->o_us = b.take(g * sizeof(UnitScalars));
+  p->o_box = b.take(g * b1 * c);
+  p->o_s1 = b.take(g * b1);
+  p->o_s1f = b.take((size_t)g * p->b1.h * p->ww1 * 8);
+  p->o_s1r = b.take((size_t)g * p->b1.h * p->ww1 * 8);
+  p->o_s2 = b.take(g * b2);
+  p->o_s2f = b.take((size_t)g * p->b2.h * p->ww2 * 8);
+  p->o_s2r = b.take((size_t)g * p->b2.h * p->ww2 * 8);
+  p->o_s3 = b.take(g * b3);
+  p->o_ch = b.take(g * 2 * b1);
+  p->o_chf = b.take((size_t)g * 2 * p->b1.h * p->ww1 * 8);
+  p->o_chr = b.take((size_t)g * 2 * p->b1.h * p->ww1 * 8);
+  p->o_pm = b.take(g * 3 * b2);
+  p->o_out22 = b.take(g * b2 * c);
+  p->o_outp22 = b.take(g * b2 * c);
+  p->o_out33 = b.take(g * 2 * b3 * c);
+  p->scratch_bytes = stage_scratch(p, g);
+  p->o_scratch = b.take(p->scratch_bytes);
+  p->ws_total = b.off;
+  *out = p;
+  return GL_OK;
+}
+
+extern "C" void gl_plan_destroy(gl_plan* plan) { plan_free(plan); }
+
+extern "C" gl_status gl_plan_get_info(const gl_plan* p, gl_plan_info* info) {
+  if (!p || !info) return fail(GL_ERR_INVALID_ARGUMENT, "null plan or info");
+  std::memset(info, 0, sizeof *info);
+  info->ncx = p->ncx;
+  info->ncy = p->ncy;
+  const Box* bs[3] = {&p->b1, &p->b2, &p->b3};
+  int* dst[3] = {info->box1, info->box2, info->box3};
+  for (int k = 0; k < 3; ++k) {
+    dst[k][0] = bs[k]->x0;
+    dst[k][1] = bs[k]->y0;
+    dst[k][2] = bs[k]->w;
+    dst[k][3] = bs[k]->h;
+  }
+  info->n_components = p->ncomp;
+  for (int k = 0; k < p->ncomp; ++k) info->component_ids[k] = p->comp_ids[k];
+  double t = 0;
+  if (p->comps & GL_COMP_ETA11) t += 1;
+  if (p->comps & GL_COMP_PSI11) t += 1;
+  if (p->want_eta22) t += 10.0 * p->ranks[0] + 3;
+  if (p->want_psi22) t += 108;
+  if (p->want_o3) t += p->ranks[3] * (25.0 + 16.0 * p->ranks[2]) + 5;
+  info->transforms_per_unit = t;
+  return GL_OK;
+}
+
+extern "C" gl_status gl_workspace_size(const gl_plan* p, size_t* bytes) {
+  if (!p || !bytes) return fail(GL_ERR_INVALID_ARGUMENT, "null plan or size pointer");
+  *bytes = p->ws_total;
+  return GL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+
+static int grid_for(size_t n, int threads, int cap = 4096) {
+  size_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > (size_t)cap) b = cap;
+  return (int)b;
+}
+
+static gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
+  const int cw = std::max(1, 2048 / a.n);
+  const size_t smem = (size_t)3 * cw * a.n * sizeof(cplx);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(col_ifft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    attr = true;
+  }
+  dim3 grid((a.box.w + cw - 1) / cw, njobs);
+  col_ifft_kernel<<<grid, 256, smem, st>>>(a, tw, cw);
+  LAUNCH_CHECK("col_ifft_kernel");
+  return GL_OK;
+}
+
+static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
+  int nb = 0;
+  for (int g = 0; g < a.ngrp; ++g) nb += a.grp[g].nb;
+  const size_t smem = row_smem(nb, a.nx);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    attr = true;
+  }
+  dim3 grid(a.ny, njobs);
+  row_kernel<<<grid, 256, smem, st>>>(a, tw);
+  LAUNCH_CHECK("row_kernel");
+  return GL_OK;
+}
+
+static gl_status launch_col_fft(const ColFftArgs& a, int njs, cudaStream_t st, const cplx* tw) {
+  const int cw = std::max(1, 2048 / a.n);
+  const size_t smem = (size_t)2 * cw * a.n * sizeof(cplx);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(col_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    attr = true;
+  }
+  dim3 grid((a.box.w + cw - 1) / cw, njs);
+  col_fft_kernel<<<grid, 256, smem, st>>>(a, tw, cw);
+  LAUNCH_CHECK("col_fft_kernel");
+  return GL_OK;
+}
+
+static gl_status launch_out_rows(const OutArgs& a0, int nuc, cudaStream_t st, const cplx* tw) {
+  OutArgs a = a0;
+  a.rows = std::max(1, 2048 / a.nx);
+  const size_t smem = (size_t)2 * a.rows * a.nx * sizeof(cplx);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(out_row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    attr = true;
+  }
+  dim3 grid((a.ny + a.rows - 1) / a.rows, nuc);
+  out_row_kernel<<<grid, 256, smem, st>>>(a, tw);
+  LAUNCH_CHECK("out_row_kernel");
+  return GL_OK;
+}
+
+template <class T>
+static T* at(void* ws, size_t off) {
+  return reinterpret_cast<T*>(reinterpret_cast<char*>(ws) + off);
+}
+
+static void mink_args(MinkArgs& m, const unsigned long long* a, int ha, int wa, int wwa,
+                      const unsigned long long* brev, int hb, int wb, int wwb, unsigned char* c,
+                      const double* geoc, UnitSlots* slots, int which) {
+  m.a = a;
+  m.ha = ha;
+  m.wa = wa;
+  m.wwa = wwa;
+  m.a_job_stride = (long long)ha * wwa;
+  m.brev = brev;
+  m.hb = hb;
+  m.wb = wb;
+  m.wwb = wwb;
+  m.b_job_stride = (long long)hb * wwb;
+  m.c = c;
+  m.hc = ha + hb - 1;
+  m.wc = wa + wb - 1;
+  m.c_job_stride = (long long)m.hc * m.wc;
+  m.geoc = geoc;
+  m.slots = slots;
+  m.which = which;
+}
+
+// Final transform of box spectra `spec` ([unit][nb][box]) to the reference
+// grid, writing output planes comp_offset.. of each unit.
+static gl_status final_output(gl_plan* p, int gu, const Box& box, const double* geo,
+                              const cplx* spec, long long spec_stride, int nb, const int* mults,
+                              const int* srcs, int comp_offset, void* outputs, void* scratch,
+                              cudaStream_t st, const double* comp_scale_dev) {
+  ColArgs a;
+  std::memset(&a, 0, sizeof a);
+  a.kind = COL_PLAIN;
+  a.nbanks = nb;
+  for (int k = 0; k < nb; ++k) {
+    a.mult[k] = mults[k];
+    a.src_of[k] = srcs[k];
+  }
+  a.box = box;
+  a.geo = geo;
+  a.spec = spec;
+  a.spec_job_stride = spec_stride;
+  a.spec_sub_stride = (long long)box.w * box.h;
+  a.jobs_per_unit = 1;
+  a.out = reinterpret_cast<cplx*>(scratch);
+  a.n = p->d.ny;
+  a.log2n = p->lny;
+  a.scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
+  gl_status s = launch_col_ifft(a, gu, st, p->tw);
+  if (s != GL_OK) return s;
+  OutArgs o;
+  std::memset(&o, 0, sizeof o);
+  o.in = reinterpret_cast<cplx*>(scratch);
+  o.w = box.w;
+  o.x0 = box.x0;
+  o.nx = p->d.nx;
+  o.log2nx = p->lnx;
+  o.ny = p->d.ny;
+  o.ncomp = nb;
+  o.comp_offset = comp_offset;
+  o.out_ncomp = p->ncomp;
+  o.comp_scale = comp_scale_dev + comp_offset;
+  o.out = outputs;
+  o.real_only = p->d.output == GL_OUT_REAL;
+  return launch_out_rows(o, gu * nb, st, p->tw);
+}
+
+static int comp_slot(const gl_plan* p, int id) {
+  for (int k = 0; k < p->ncomp; ++k)
+    if (p->comp_ids[k] == id) return k;
+  return -1;
+}
+
+// ---------------------------------------------------------------------------
+// one group of units
+// ---------------------------------------------------------------------------
+
+static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, void* outputs,
+                           void* ws, int* status, cudaStream_t st) {
+  const int T = 256;
+  const Box B1 = p->b1, B2 = p->b2, B3 = p->b3;
+  const int pl1 = B1.w * B1.h, pl2 = B2.w * B2.h, pl3 = B3.w * B3.h;
+  UnitSlots* slots = at<UnitSlots>(ws, p->o_slots);
+  UnitScalars* us = at<UnitScalars>(ws, p->o_us);
+  cplx* boxv = at<cplx>(ws, p->o_box);
+  unsigned char* s1 = at<unsigned char>(ws, p->o_s1);
+  unsigned long long* s1f = at<unsigned long long>(ws, p->o_s1f);
+  unsigned long long* s1r = at<unsigned long long>(ws, p->o_s1r);
+  unsigned char* s2 = at<unsigned char>(ws, p->o_s2);
+  unsigned long long* s2f = at<unsigned long long>(ws, p->o_s2f);
+  unsigned long long* s2r = at<unsigned long long>(ws, p->o_s2r);
+  unsigned char* s3 = at<unsigned char>(ws, p->o_s3);
+  unsigned char* ch = at<unsigned char>(ws, p->o_ch);
+  unsigned long long* chf = at<unsigned long long>(ws, p->o_chf);
+  unsigned long long* chr = at<unsigned long long>(ws, p->o_chr);
+  unsigned char* pm = at<unsigned char>(ws, p->o_pm);
+  cplx* out22 = at<cplx>(ws, p->o_out22);
+  cplx* outp22 = at<cplx>(ws, p->o_outp22);
+  cplx* out33 = at<cplx>(ws, p->o_out33);
+  char* scratch = at<char>(ws, p->o_scratch);
+  const double* dn = p->nodes;  // [k*MAX_RANK] nodes, [(4+k)*MAX_RANK] weights
+  gl_status s;
+
+  slots_init_kernel<<<(gu + 63) / 64, 64, 0, st>>>(slots, gu);
+  LAUNCH_CHECK("slots_init_kernel");
+  const cplx* spec = boxv;
+  if (layout == GL_SPECTRA_FULL) {
+    CUDA_TRY(cudaMemsetAsync(boxv, 0, sizeof(cplx) * (size_t)gu * pl1, st));
+    dim3 g(grid_for((size_t)p->d.nx * p->d.ny, T, 1024), gu);
+    extract_kernel<<<g, T, 0, st>>>(reinterpret_cast<const cplx*>(spectra), boxv, B1, p->d.nx,
+                                    p->d.ny, slots);
+    LAUNCH_CHECK("extract_kernel");
+  } else {
+    spec = reinterpret_cast<const cplx*>(spectra);
+    dim3 g(grid_for(pl1, T, 64), gu);
+    box_max_kernel<<<g, T, 0, st>>>(spec, pl1, slots);
+    LAUNCH_CHECK("box_max_kernel");
+  }
+  {
+    dim3 g(grid_for(pl1, T, 64), gu);
+    support_kernel<<<g, T, 0, st>>>(spec, p->geo1, B1, slots, s1);
+    LAUNCH_CHECK("support_kernel");
+    peak_kernel<<<g, T, 0, st>>>(spec, p->geo1, B1, p->d.nx, p->d.ny, slots, s1, ch,
+                                 p->want_psi22 ? 1 : 0);
+    LAUNCH_CHECK("peak_kernel");
+  }
+  const bool need_s2 = p->want_eta22 || p->want_psi22 || p->want_o3;
+  if (need_s2) {
+    dim3 g(grid_for(B1.h * p->ww1, T, 64), gu);
+    bitrows_kernel<<<g, T, 0, st>>>(s1, B1.h, B1.w, p->ww1, s1f, s1r);
+    LAUNCH_CHECK("bitrows_kernel");
+    MinkArgs m;
+    mink_args(m, s1f, B1.h, B1.w, p->ww1, s1r, B1.h, B1.w, p->ww1, s2, p->geo2, slots, 2);
+    dim3 g2(grid_for(pl2, T, 256), gu);
+    minkowski_kernel<<<g2, T, 0, st>>>(m);
+    LAUNCH_CHECK("minkowski_kernel");
+  }
+  if (p->want_o3) {
+    dim3 g(grid_for(B2.h * p->ww2, T, 64), gu);
+    bitrows_kernel<<<g, T, 0, st>>>(s2, B2.h, B2.w, p->ww2, s2f, s2r);
+    LAUNCH_CHECK("bitrows_kernel");
+    MinkArgs m;
+    mink_args(m, s2f, B2.h, B2.w, p->ww2, s1r, B1.h, B1.w, p->ww1, s3, p->geo3, slots, 3);
+    dim3 g3(grid_for(pl3, T, 512), gu);
+    minkowski_kernel<<<g3, T, 0, st>>>(m);
+    LAUNCH_CHECK("minkowski_kernel");
+  }
+  if (p->want_psi22) {
+    dim3 g(grid_for(B1.h * p->ww1, T, 64), gu * 2);
+    bitrows_kernel<<<g, T, 0, st>>>(ch, B1.h, B1.w, p->ww1, chf, chr);
+    LAUNCH_CHECK("bitrows_kernel");
+    const long long cstride = (long long)B1.h * p->ww1;
+    const int pairs[3][2] = {{0, 0}, {0, 1}, {1, 1}};
+    for (int k = 0; k < 3; ++k) {
+      MinkArgs m;
+      mink_args(m, chf + pairs[k][0] * cstride, B1.h, B1.w, p->ww1, chr + pairs[k][1] * cstride,
+                B1.h, B1.w, p->ww1, pm + (size_t)k * pl2, nullptr, slots, 0);
+      m.a_job_stride = 2 * cstride;
+      m.b_job_stride = 2 * cstride;
+      m.c_job_stride = 3LL * pl2;
+      dim3 g2(grid_for(pl2, T, 256), gu);
+      minkowski_kernel<<<g2, T, 0, st>>>(m);
+      LAUNCH_CHECK("minkowski_kernel");
+    }
+  }
+  {
+    ScalarArgs a;
+    a.slots = slots;
+    a.us = us;
+    a.geo1 = p->geo1;
+    a.box = B1;
+    a.nx = p->d.nx;
+    a.ny = p->d.ny;
+    a.order = p->d.order;
+    a.want_eta22 = p->want_eta22;
+    a.want_psi22 = p->want_psi22;
+    a.want_o3 = p->want_o3;
+    a.allow_below = p->d.allow_below_model_parent_domain;
+    a.full_input = layout == GL_SPECTRA_FULL;
+    scalars_kernel<<<(gu + 63) / 64, 64, 0, st>>>(a, gu);
+    LAUNCH_CHECK("scalars_kernel");
+  }
+  const double fwd_scale = ((double)p->d.nx * (double)p->d.ny) / ((double)p->ncx * (double)p->ncy);
+  const double inv_scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
+  const int ncy = p->ncy;
+
+  // ---------------- eta22 (spatial.py:156-231) ----------------
+  if (p->want_eta22) {
+    const int J = p->ranks[0];
+    const int njobs = gu * J;
+    Bump b;
+    cplx* P = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs * 8 * B1.w * ncy * sizeof(cplx)));
+    cplx* Q = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs * 2 * B2.w * ncy * sizeof(cplx)));
+    cplx* R = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs * 2 * pl2 * sizeof(cplx)));
+    unsigned long long* mx = reinterpret_cast<unsigned long long*>(scratch + b.take((size_t)njobs * 2 * 8));
+    CUDA_TRY(cudaMemsetAsync(mx, 0, (size_t)njobs * 2 * 8, st));
+    ColArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.kind = COL_ETA22;
+    a.nbanks = 8;
+    const int m8[8] = {M_ONE, M_NU, M_NU2, M_QX_DIVNU, M_QY_DIVNU, M_Q2_DIVNU, M_QX, M_QY};
+    for (int k = 0; k < 8; ++k) a.mult[k] = m8[k];
+    a.box = B1;
+    a.geo = p->geo1;
+    a.spec = spec;
+    a.spec_job_stride = pl1;
+    a.jobs_per_unit = J;
+    a.us = us;
+    a.nodes = dn + 0 * MAX_RANK;
+    a.out = P;
+    a.n = ncy;
+    a.log2n = p->lncy;
+    a.scale = inv_scale;
+    if ((s = launch_col_ifft(a, njobs, st, p->tw)) != GL_OK) return s;
+    RowArgs r;
+    std::memset(&r, 0, sizeof r);
+    r.kind = ROW_ETA22;
+    r.grp[0] = BankGroup{P, 8, B1.x0, B1.w};
+    r.ngrp = 1;
+    r.nout = 2;
+    r.out_x0 = B2.x0;
+    r.out_w = B2.w;
+    r.out = Q;
+    r.nx = p->ncx;
+    r.log2nx = p->lncx;
+    r.ny = ncy;
+    r.us = us;
+    r.jobs_per_unit = J;
+    r.gmax = ROW_GMAX;
+    if ((s = launch_row(r, njobs, st, p->tw)) != GL_OK) return s;
+    ColFftArgs f;
+    f.in = Q;
+    f.out = R;
+    f.box = B2;
+    f.n = ncy;
+    f.log2n = p->lncy;
+    f.nsrc = 2;
+    f.jobs_per_unit = J;
+    f.mask = s2;
+    f.maxslot = mx;
+    f.scale = fwd_scale;
+    if ((s = launch_col_fft(f, njobs * 2, st, p->tw)) != GL_OK) return s;
+    AccArgs c;
+    std::memset(&c, 0, sizeof c);
+    c.us = us;
+    c.geo = p->geo2;
+    c.box = B2;
+    c.in = R;
+    c.maxin = mx;
+    c.out = out22;
+    c.nodes = dn + 0 * MAX_RANK;
+    c.weights = dn + 4 * MAX_RANK;
+    c.nnodes = J;
+    c.floor_rel = p->floor_rel;
+    dim3 g(grid_for(pl2, T, 256), gu);
+    acc_eta22_kernel<<<g, T, 0, st>>>(c);
+    LAUNCH_CHECK("acc_eta22_kernel");
+  }
+
+  // ---------------- psi22 (spatial.py:234-414) ----------------
+  if (p->want_psi22) {
+    const int njobs_c = gu * 2 * 2 * 2;  // (unit, branch, node, channel)
+    const int njobs_r = gu * 2 * 2;      // (unit, branch, node)
+    Bump b;
+    cplx* P = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs_c * 8 * B1.w * ncy * sizeof(cplx)));
+    cplx* Q = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs_r * 8 * B2.w * ncy * sizeof(cplx)));
+    cplx* R = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs_r * 8 * pl2 * sizeof(cplx)));
+    cplx* Pc = reinterpret_cast<cplx*>(scratch + b.take((size_t)gu * 2 * B1.w * ncy * sizeof(cplx)));
+    cplx* Qc = reinterpret_cast<cplx*>(scratch + b.take((size_t)gu * 1 * B2.w * ncy * sizeof(cplx)));
+    cplx* Rc = reinterpret_cast<cplx*>(scratch + b.take((size_t)gu * pl2 * sizeof(cplx)));
+    ColArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.kind = COL_PSI22;
+    a.nbanks = 8;
+    const int m8[8] = {M_ONE, M_NU, M_NU2, M_QX_DIVNU, M_QY_DIVNU, M_Q2_DIVNU, M_QX, M_QY};
+    for (int k = 0; k < 8; ++k) a.mult[k] = m8[k];
+    a.box = B1;
+    a.geo = p->geo1;
+    a.spec = spec;
+    a.spec_job_stride = pl1;
+    a.jobs_per_unit = 8;
+    a.us = us;
+    a.nodes = dn + 1 * MAX_RANK;
+    a.n_inner = 2;
+    a.chan_mask = ch;
+    a.out = P;
+    a.n = ncy;
+    a.log2n = p->lncy;
+    a.scale = inv_scale;
+    if ((s = launch_col_ifft(a, njobs_c, st, p->tw)) != GL_OK) return s;
+    RowArgs r;
+    std::memset(&r, 0, sizeof r);
+    r.kind = ROW_PSI22;
+    // job (unit, branch, node): its two channels are consecutive col jobs,
+    // so a row job sees 16 consecutive banks.
+    r.grp[0] = BankGroup{P, 16, B1.x0, B1.w};
+    r.ngrp = 1;
+    r.nout = 8;
+    r.out_x0 = B2.x0;
+    r.out_w = B2.w;
+    r.out = Q;
+    r.nx = p->ncx;
+    r.log2nx = p->lncx;
+    r.ny = ncy;
+    r.us = us;
+    r.jobs_per_unit = 4;
+    r.gmax = ROW_GMAX;
+    if ((s = launch_row(r, njobs_r, st, p->tw)) != GL_OK) return s;
+    ColFftArgs f;
+    f.in = Q;
+    f.out = R;
+    f.box = B2;
+    f.n = ncy;
+    f.log2n = p->lncy;
+    f.nsrc = 8;
+    f.jobs_per_unit = 4;
+    f.mask = nullptr;
+    f.maxslot = nullptr;
+    f.scale = fwd_scale;
+    if ((s = launch_col_fft(f, njobs_r * 8, st, p->tw)) != GL_OK) return s;
+    // Taylor contact 0.5 eta11 phi1z
+    ColArgs cc;
+    std::memset(&cc, 0, sizeof cc);
+    cc.kind = COL_PLAIN;
+    cc.nbanks = 2;
+    cc.mult[0] = M_ONE;
+    cc.mult[1] = M_NU;
+    cc.src_of[0] = 0;
+    cc.src_of[1] = 0;
+    cc.box = B1;
+    cc.geo = p->geo1;
+    cc.spec = spec;
+    cc.spec_job_stride = pl1;
+    cc.jobs_per_unit = 1;
+    cc.out = Pc;
+    cc.n = ncy;
+    cc.log2n = p->lncy;
+    cc.scale = inv_scale;
+    if ((s = launch_col_ifft(cc, gu, st, p->tw)) != GL_OK) return s;
+    RowArgs rc;
+    std::memset(&rc, 0, sizeof rc);
+    rc.kind = ROW_CONTACT22;
+    rc.grp[0] = BankGroup{Pc, 2, B1.x0, B1.w};
+    rc.ngrp = 1;
+    rc.nout = 1;
+    rc.out_x0 = B2.x0;
+    rc.out_w = B2.w;
+    rc.out = Qc;
+    rc.nx = p->ncx;
+    rc.log2nx = p->lncx;
+    rc.ny = ncy;
+    rc.us = us;
+    rc.jobs_per_unit = 1;
+    rc.gmax = ROW_GMAX;
+    if ((s = launch_row(rc, gu, st, p->tw)) != GL_OK) return s;
+    ColFftArgs fc = f;
+    fc.in = Qc;
+    fc.out = Rc;
+    fc.nsrc = 1;
+    fc.jobs_per_unit = 1;
+    if ((s = launch_col_fft(fc, gu, st, p->tw)) != GL_OK) return s;
+    AccArgs c;
+    std::memset(&c, 0, sizeof c);
+    c.us = us;
+    c.geo = p->geo2;
+    c.box = B2;
+    c.in = R;
+    c.out = outp22;
+    c.mask = s2;
+    c.pmask = pm;
+    c.extra = Rc;
+    c.nodes = dn + 1 * MAX_RANK;
+    c.weights = dn + 5 * MAX_RANK;
+    c.nnodes = 2;
+    dim3 g(grid_for(pl2, T, 256), gu);
+    acc_psi22_kernel<<<g, T, 0, st>>>(c);
+    LAUNCH_CHECK("acc_psi22_kernel");
+  }
+
+  // ---------------- order 3 (_order3.py:18-148) ----------------
+  if (p->want_o3) {
+    const int J = p->ranks[3], I = p->ranks[2];
+    const int nuj = gu * J;
+    const int njobs = nuj * I;
+    Bump b;
+    cplx* E = reinterpret_cast<cplx*>(scratch + b.take((size_t)nuj * 4 * pl2 * sizeof(cplx)));
+    unsigned long long* mxs = reinterpret_cast<unsigned long long*>(scratch + b.take((size_t)nuj * 8 * 16));
+    unsigned long long* maxEt = mxs;                 // [nuj]
+    unsigned long long* maxRO = mxs + nuj;           // [nuj][4]
+    unsigned long long* maxF = mxs + 5 * nuj;        // [nuj][2]
+    CUDA_TRY(cudaMemsetAsync(mxs, 0, (size_t)nuj * 8 * 8, st));
+    // inner stage buffers
+    Bump bi = b;
+    cplx* PI = reinterpret_cast<cplx*>(scratch + bi.take((size_t)njobs * 12 * B1.w * ncy * sizeof(cplx)));
+    cplx* QI = reinterpret_cast<cplx*>(scratch + bi.take((size_t)njobs * 4 * B2.w * ncy * sizeof(cplx)));
+    cplx* RI = reinterpret_cast<cplx*>(scratch + bi.take((size_t)njobs * 4 * pl2 * sizeof(cplx)));
+    unsigned long long* maxRI = reinterpret_cast<unsigned long long*>(scratch + bi.take((size_t)njobs * 4 * 8));
+    CUDA_TRY(cudaMemsetAsync(maxRI, 0, (size_t)njobs * 4 * 8, st));
+    {
+      ColArgs a;
+      std::memset(&a, 0, sizeof a);
+      a.kind = COL_INNER;
+      a.nbanks = 12;
+      const int m12[12] = {M_ONE, M_NU, M_NU2, M_NU3, M_QX_SNU, M_QY_SNU,
+                           M_QX, M_QY, M_Q2_SNU, M_Q2, M_NUQX, M_NUQY};
+      for (int k = 0; k < 12; ++k) a.mult[k] = m12[k];
+      a.box = B1;
+      a.geo = p->geo1;
+      a.spec = spec;
+      a.spec_job_stride = pl1;
+      a.jobs_per_unit = J * I;
+      a.us = us;
+      a.nodes = dn + 3 * MAX_RANK;
+      a.nodes2 = dn + 2 * MAX_RANK;
+      a.n_inner = I;
+      a.n_outer = J;
+      a.out = PI;
+      a.n = ncy;
+      a.log2n = p->lncy;
+      a.scale = inv_scale;
+      if ((s = launch_col_ifft(a, njobs, st, p->tw)) != GL_OK) return s;
+      RowArgs r;
+      std::memset(&r, 0, sizeof r);
+      r.kind = ROW_INNER;
+      r.grp[0] = BankGroup{PI, 12, B1.x0, B1.w};
+      r.ngrp = 1;
+      r.nout = 4;
+      r.out_x0 = B2.x0;
+      r.out_w = B2.w;
+      r.out = QI;
+      r.nx = p->ncx;
+      r.log2nx = p->lncx;
+      r.ny = ncy;
+      r.us = us;
+      r.jobs_per_unit = J * I;
+      r.gmax = ROW_GMAX;
+      if ((s = launch_row(r, njobs, st, p->tw)) != GL_OK) return s;
+      ColFftArgs f;
+      f.in = QI;
+      f.out = RI;
+      f.box = B2;
+      f.n = ncy;
+      f.log2n = p->lncy;
+      f.nsrc = 4;
+      f.jobs_per_unit = J * I;
+      f.mask = s2;
+      f.maxslot = maxRI;
+      f.scale = fwd_scale;
+      if ((s = launch_col_fft(f, njobs * 4, st, p->tw)) != GL_OK) return s;
+      AccArgs c;
+      std::memset(&c, 0, sizeof c);
+      c.us = us;
+      c.geo = p->geo2;
+      c.box = B2;
+      c.in = RI;
+      c.maxin = maxRI;
+      c.out = E;
+      c.maxout = maxEt;
+      c.mask = s2;
+      c.nodes = dn + 2 * MAX_RANK;
+      c.weights = dn + 6 * MAX_RANK;
+      c.nnodes = I;
+      c.nsub = J;
+      c.floor_rel = p->floor_rel;
+      dim3 g(grid_for(pl2, T, 128), nuj);
+      acc_inner_kernel<<<g, T, 0, st>>>(c);
+      LAUNCH_CHECK("acc_inner_kernel");
+    }
+    // outer stage buffers (reuse the inner region)
+    Bump bo = b;
+    cplx* P1 = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 12 * B1.w * ncy * sizeof(cplx)));
+    cplx* P2 = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 9 * B2.w * ncy * sizeof(cplx)));
+    cplx* QO = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 4 * B3.w * ncy * sizeof(cplx)));
+    cplx* RO = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 4 * pl3 * sizeof(cplx)));
+    cplx* FO = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 2 * pl3 * sizeof(cplx)));
+    {
+      ColArgs a;
+      std::memset(&a, 0, sizeof a);
+      a.kind = COL_OUTER1;
+      a.nbanks = 12;
+      const int m12[12] = {M_ONE, M_IQX, M_IQY, M_QX_SNU, M_QY_SNU, M_MI_NU,
+                           M_NUQX, M_NUQY, M_MI_Q2_SNU, M_MI_Q2NU, M_MINUS_A, M_MINUS_Q2};
+      for (int k = 0; k < 12; ++k) a.mult[k] = m12[k];
+      a.box = B1;
+      a.geo = p->geo1;
+      a.spec = spec;
+      a.spec_job_stride = pl1;
+      a.jobs_per_unit = J;
+      a.us = us;
+      a.nodes = dn + 3 * MAX_RANK;
+      a.out = P1;
+      a.n = ncy;
+      a.log2n = p->lncy;
+      a.scale = inv_scale;
+      if ((s = launch_col_ifft(a, nuj, st, p->tw)) != GL_OK) return s;
+      ColArgs a2;
+      std::memset(&a2, 0, sizeof a2);
+      a2.kind = COL_OUTER2;
+      a2.nbanks = 9;
+      const int m9[9] = {M_ONE, M_IQX, M_IQY, M_IQX, M_IQY, M_A, M_Q2, M_A, M_ONE};
+      const int src9[9] = {0, 0, 0, 2, 2, 2, 2, 3, 1};
+      for (int k = 0; k < 9; ++k) {
+        a2.mult[k] = m9[k];
+        a2.src_of[k] = src9[k];
+      }
+      a2.box = B2;
+      a2.geo = p->geo2;
+      a2.spec = E;
+      a2.spec_job_stride = 4LL * pl2;
+      a2.spec_sub_stride = pl2;
+      a2.jobs_per_unit = J;
+      a2.us = us;
+      a2.floor_max = maxEt;
+      a2.floor_rel = p->floor_rel;
+      a2.out = P2;
+      a2.n = ncy;
+      a2.log2n = p->lncy;
+      a2.scale = inv_scale;
+      if ((s = launch_col_ifft(a2, nuj, st, p->tw)) != GL_OK) return s;
+      RowArgs r;
+      std::memset(&r, 0, sizeof r);
+      r.kind = ROW_OUTER;
+      r.grp[0] = BankGroup{P1, 12, B1.x0, B1.w};
+      r.grp[1] = BankGroup{P2, 9, B2.x0, B2.w};
+      r.ngrp = 2;
+      r.nout = 4;
+      r.out_x0 = B3.x0;
+      r.out_w = B3.w;
+      r.out = QO;
+      r.nx = p->ncx;
+      r.log2nx = p->lncx;
+      r.ny = ncy;
+      r.us = us;
+      r.jobs_per_unit = J;
+      r.gmax = ROW_GMAX;
+      if ((s = launch_row(r, nuj, st, p->tw)) != GL_OK) return s;
+      ColFftArgs f;
+      f.in = QO;
+      f.out = RO;
+      f.box = B3;
+      f.n = ncy;
+      f.log2n = p->lncy;
+      f.nsrc = 4;
+      f.jobs_per_unit = J;
+      f.mask = s3;
+      f.maxslot = maxRO;
+      f.scale = fwd_scale;
+      if ((s = launch_col_fft(f, nuj * 4, st, p->tw)) != GL_OK) return s;
+      AccArgs c;
+      std::memset(&c, 0, sizeof c);
+      c.us = us;
+      c.geo = p->geo3;
+      c.box = B3;
+      c.in = RO;
+      c.maxin = maxRO;
+      c.out = FO;
+      c.maxout = maxF;
+      c.mask = s3;
+      c.floor_rel = p->floor_rel;
+      c.nsub = J;
+      dim3 g(grid_for(pl3, T, 128), nuj);
+      acc_outer_combine_kernel<<<g, T, 0, st>>>(c);
+      LAUNCH_CHECK("acc_outer_combine_kernel");
+      c.out = out33;
+      c.extra = FO;
+      c.nodes = dn + 3 * MAX_RANK;
+      c.weights = dn + 7 * MAX_RANK;
+      c.nnodes = J;
+      dim3 g2(grid_for(pl3, T, 256), gu);
+      acc_outer_kernel<<<g2, T, 0, st>>>(c, maxF);
+      LAUNCH_CHECK("acc_outer_kernel");
+    }
+  }
+
+  // ---------------- outputs on the reference grid ----------------
+  if (p->want_first) {
+    int mults[2], n = 0, off = -1;
+    if (p->comps & GL_COMP_ETA11) {
+      mults[n++] = M_ONE;
+      off = comp_slot(p, GL_COMP_ETA11);
+    }
+    if (p->comps & GL_COMP_PSI11) {
+      mults[n++] = M_PSI11;
+      if (off < 0) off = comp_slot(p, GL_COMP_PSI11);
+    }
+    const int srcs[2] = {0, 0};  // both read the parent spectrum
+    if ((s = final_output(p, gu, B1, p->geo1, spec, pl1, n, mults, srcs, off, outputs, scratch, st,
+                          p->comp_scale)) != GL_OK)
+      return s;
+  }
+  if (p->want_eta22) {
+    const int m1[1] = {M_ONE}, z1[1] = {0};
+    if ((s = final_output(p, gu, B2, p->geo2, out22, pl2, 1, m1, z1, comp_slot(p, GL_COMP_ETA22),
+                          outputs, scratch, st, p->comp_scale)) != GL_OK)
+      return s;
+  }
+  if (p->want_psi22) {
+    const int m1[1] = {M_ONE}, z1[1] = {0};
+    if ((s = final_output(p, gu, B2, p->geo2, outp22, pl2, 1, m1, z1, comp_slot(p, GL_COMP_PSI22),
+                          outputs, scratch, st, p->comp_scale)) != GL_OK)
+      return s;
+  }
+  if (p->want_o3) {
+    const int m2[2] = {M_ONE, M_ONE}, s01[2] = {0, 1};
+    const int ce = comp_slot(p, GL_COMP_ETA33), cp = comp_slot(p, GL_COMP_PSI33);
+    if (ce >= 0 && cp >= 0) {
+      if ((s = final_output(p, gu, B3, p->geo3, out33, 2LL * pl3, 2, m2, s01, ce, outputs, scratch, st,
+                            p->comp_scale)) != GL_OK)
+        return s;
+    } else {
+      const int which = ce >= 0 ? 0 : 1;
+      if ((s = final_output(p, gu, B3, p->geo3, out33 + (size_t)which * pl3, 2LL * pl3, 1, m2,
+                            s01, ce >= 0 ? ce : cp, outputs, scratch, st, p->comp_scale)) != GL_OK)
+        return s;
+    }
+  }
+  {
+    const size_t per_unit = (size_t)p->ncomp * p->d.nx * p->d.ny;
+    dim3 g(grid_for(per_unit, T, 256), gu);
+    nonfinite_kernel<<<g, T, 0, st>>>(outputs, per_unit, p->d.output == GL_OUT_REAL, us);
+    LAUNCH_CHECK("nonfinite_kernel");
+  }
+  if (status) {
+    status_kernel<<<(gu + 63) / 64, 64, 0, st>>>(us, gu, status);
+    LAUNCH_CHECK("status_kernel");
+  }
+  return GL_OK;
+}
+
+extern "C" gl_status gl_execute(gl_plan* p, int n_units, const void* d_spectra, int layout,
+                                void* d_outputs, void* d_ws, size_t ws_bytes, int* d_status,
+                                void* stream) {
+  if (!p) return fail(GL_ERR_INVALID_ARGUMENT, "null plan");
+  if (n_units < 0) return fail(GL_ERR_INVALID_ARGUMENT, "negative unit count");
+  if (n_units == 0) return GL_OK;
+  if (!d_spectra || !d_outputs) return fail(GL_ERR_INVALID_ARGUMENT, "null spectra or outputs");
+  if (layout != GL_SPECTRA_FULL && layout != GL_SPECTRA_BOX)
+    return fail(GL_ERR_INVALID_ARGUMENT, "unknown spectra layout");
+  if (!d_ws || ws_bytes < p->ws_total || (reinterpret_cast<uintptr_t>(d_ws) & 255))
+    return fail(GL_ERR_WORKSPACE, "workspace must be 256-byte aligned and at least %zu bytes", p->ws_total);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const size_t in_unit = layout == GL_SPECTRA_FULL ? (size_t)p->d.nx * p->d.ny
+                                                   : (size_t)p->b1.w * p->b1.h;
+  const size_t out_unit = (size_t)p->ncomp * p->d.nx * p->d.ny *
+                          (p->d.output == GL_OUT_REAL ? sizeof(double) : sizeof(cplx));
+  for (int u0 = 0; u0 < n_units; u0 += p->group) {
+    const int gu = std::min(p->group, n_units - u0);
+    const void* in = reinterpret_cast<const cplx*>(d_spectra) + (size_t)u0 * in_unit;
+    void* outp = reinterpret_cast<char*>(d_outputs) + (size_t)u0 * out_unit;
+    gl_status s = run_group(p, gu, in, layout, outp, d_ws, d_status ? d_status + u0 : nullptr, st);
+    if (s != GL_OK) return s;
+  }
+  return GL_OK;
+}
+
+extern "C" gl_status gl_deposit_modes(const gl_plan* p, int n_units, int n_seg, const int* seg_off,
+                                      const int* seg_bin, int n_modes, const double* ab,
+                                      const double* omega, const double* times, void* out,
+                                      void* stream) {
+  if (!p) return fail(GL_ERR_INVALID_ARGUMENT, "null plan");
+  if (n_units < 0 || n_seg < 0 || n_modes < 0) return fail(GL_ERR_INVALID_ARGUMENT, "negative size");
+  if (n_units == 0) return GL_OK;
+  if (!out || (n_seg && (!seg_off || !seg_bin || !ab || !omega)) || !times)
+    return fail(GL_ERR_INVALID_ARGUMENT, "null deposit buffer");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const int plane = p->b1.w * p->b1.h;
+  CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(cplx) * (size_t)n_units * plane, st));
+  if (n_seg == 0) return GL_OK;
+  dim3 g(grid_for(n_seg, 128, 256), n_units);
+  deposit_kernel<<<g, 128, 0, st>>>(n_seg, seg_off, seg_bin, ab, omega, times,
+                                    (double)p->d.nx * (double)p->d.ny, p->d.depth,
+                                    reinterpret_cast<cplx*>(out), plane);
+  LAUNCH_CHECK("deposit_kernel");
+  return GL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// plain batched 2-D FFT on the reference grid (numpy fft2 / ifft2 conventions)
+// ---------------------------------------------------------------------------
+
+template <int SIGN>
+__global__ void fft2_rows_kernel(const cplx* in, cplx* out, int nx, int log2nx, int ny, int rows,
+                                 double scale, const cplx* __restrict__ tw) {
+  extern __shared__ cplx smem[];
+  const int b = blockIdx.y;
+  const int y0 = blockIdx.x * rows;
+  const int r = min(rows, ny - y0);
+  cplx* buf = smem;
+  cplx* tmp = smem + (size_t)rows * nx;
+  const size_t base = ((size_t)b * ny + y0) * nx;
+  for (int t = threadIdx.x; t < r * nx; t += blockDim.x) buf[t] = in[base + t];
+  __syncthreads();
+  fft_rows<SIGN>(buf, tmp, nx, log2nx, r, rows, tw);
+  for (int t = threadIdx.x; t < r * nx; t += blockDim.x) out[base + t] = cscale(scale, buf[t]);
+}
+
+template <int SIGN>
+__global__ void fft2_cols_kernel(cplx* data, int nx, int ny, int log2ny, int cw,
+                                 const cplx* __restrict__ tw) {
+  extern __shared__ cplx smem[];
+  const int b = blockIdx.y;
+  const int x0 = blockIdx.x * cw;
+  const int c = min(cw, nx - x0);
+  cplx* buf = smem;
+  cplx* tmp = smem + (size_t)cw * ny;
+  cplx* d = data + (size_t)b * nx * ny;
+  for (int t = threadIdx.x; t < c * ny; t += blockDim.x) {
+    const int y = t / c, k = t % c;
+    buf[k * ny + y] = d[(size_t)y * nx + x0 + k];
+  }
+  __syncthreads();
+  fft_rows<SIGN>(buf, tmp, ny, log2ny, c, cw, tw);
+  for (int t = threadIdx.x; t < c * ny; t += blockDim.x) {
+    const int y = t / c, k = t % c;
+    d[(size_t)y * nx + x0 + k] = buf[k * ny + y];
+  }
+}
+
+static cplx* g_tw_global[64] = {nullptr};
+
+static gl_status device_twiddles(cplx** out) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(GL_ERR_CUDA, "device index out of range");
+  if (!g_tw_global[dev]) {
+    cplx* tw = nullptr;
+    CUDA_TRY(cudaMalloc(&tw, sizeof(cplx) * TW_N));
+    twiddle_kernel<<<TW_N / 256, 256>>>(tw);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaDeviceSynchronize());
+    g_tw_global[dev] = tw;
+  }
+  *out = g_tw_global[dev];
+  return GL_OK;
+}
+
+extern "C" gl_status gl_fft2(int batch, int nx, int ny, const void* d_in, void* d_out, int inverse,
+                             void* stream) {
+  if (batch < 0 || !d_in || !d_out) return fail(GL_ERR_INVALID_ARGUMENT, "bad fft2 arguments");
+  if (!is_pow2(nx) || !is_pow2(ny) || nx < 2 || ny < 2 || nx > TW_N || ny > TW_N)
+    return fail(GL_ERR_UNSUPPORTED, "gl_fft2 runs power-of-two sizes from 2 to %d", TW_N);
+  if (batch == 0) return GL_OK;
+  cplx* tw = nullptr;
+  gl_status s = device_twiddles(&tw);
+  if (s != GL_OK) return s;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const int rows = std::max(1, 2048 / nx);
+  const int cw = std::max(1, 2048 / ny);
+  const size_t smr = (size_t)2 * rows * nx * sizeof(cplx), smc = (size_t)2 * cw * ny * sizeof(cplx);
+  const double scale = inverse ? 1.0 / ((double)nx * (double)ny) : 1.0;
+  dim3 gr((ny + rows - 1) / rows, batch), gc((nx + cw - 1) / cw, batch);
+  const cplx* in = reinterpret_cast<const cplx*>(d_in);
+  cplx* out = reinterpret_cast<cplx*>(d_out);
+  if (inverse) {
+    cudaFuncSetAttribute(fft2_rows_kernel<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    cudaFuncSetAttribute(fft2_cols_kernel<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    fft2_rows_kernel<+1><<<gr, 256, smr, st>>>(in, out, nx, ilog2(nx), ny, rows, scale, tw);
+    LAUNCH_CHECK("fft2_rows_kernel");
+    fft2_cols_kernel<+1><<<gc, 256, smc, st>>>(out, nx, ny, ilog2(ny), cw, tw);
+    LAUNCH_CHECK("fft2_cols_kernel");
+  } else {
+    cudaFuncSetAttribute(fft2_rows_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    cudaFuncSetAttribute(fft2_cols_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    fft2_rows_kernel<-1><<<gr, 256, smr, st>>>(in, out, nx, ilog2(nx), ny, rows, scale, tw);
+    LAUNCH_CHECK("fft2_rows_kernel");
+    fft2_cols_kernel<-1><<<gc, 256, smc, st>>>(out, nx, ny, ilog2(ny), cw, tw);
+    LAUNCH_CHECK("fft2_cols_kernel");
+  }
+  return GL_OK;
+}
+
+extern "C" gl_status gl_gauss_laguerre(int rank, double* nodes, double* weights) {
+  if (!nodes || !weights) return fail(GL_ERR_INVALID_ARGUMENT, "null output");
+  return gauss_laguerre(rank, nodes, weights);
+}
+
+// Newton iteration of dispersion.py:19-42 (40 steps, damped to q/2, rtol gate).
+extern "C" gl_status gl_dispersion_solve(int n, const double* omega, double depth, double gravity,
+                                         double* q_out) {
+  if (n < 0 || (n && (!omega || !q_out))) return fail(GL_ERR_INVALID_ARGUMENT, "bad arguments");
+  if (!(depth > 0) || !(gravity > 0))
+    return fail(GL_ERR_INVALID_ARGUMENT, "depth and gravity must be positive and omega nonnegative");
+  const double tiny = 2.2250738585072014e-308;
+  std::vector<double> target(n), q(n);
+  for (int i = 0; i < n; ++i) {
+    if (!(omega[i] >= 0))
+      return fail(GL_ERR_INVALID_ARGUMENT, "depth and gravity must be positive and omega nonnegative");
+    target[i] = omega[i] * omega[i] * depth / gravity;
+    q[i] = std::max(target[i] < 1.0 ? std::sqrt(target[i]) : target[i], tiny);
+  }
+  for (int it = 0; it < 40; ++it) {
+    double worst = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double t = std::tanh(q[i]);
+      const double res = q[i] * t - target[i];
+      const double der = t + q[i] * (1.0 - t * t);
+      const double upd = res / std::max(der, tiny);
+      const double cand = std::max(q[i] - upd, 0.5 * q[i]);
+      worst = std::max(worst, std::fabs(cand - q[i]) / std::max(1.0, q[i]));
+      q[i] = cand;
+    }
+    if (worst < 5.0e-15) break;
+  }
+  for (int i = 0; i < n; ++i) {
+    const double lhs = q[i] * std::tanh(q[i]);
+    if (!(std::fabs(lhs - target[i]) <= 2.0e-15 + 2.0e-13 * std::fabs(target[i])))
+      return fail(GL_ERR_INVALID_ARGUMENT, "finite-depth dispersion solve did not converge");
+    q_out[i] = q[i];
+  }
+  return GL_OK;
+}
+
+extern "C" size_t gl_get_last_error(char* buffer, size_t length) {
+  if (buffer && length) {
+    const size_t n = std::min(length - 1, g_last_error.size());
+    std::memcpy(buffer, g_last_error.data(), n);
+    buffer[n] = 0;
+  }
+  return g_last_error.size();
+}
+
+extern "C" const char* gl_version(void) { return "gl-b200 0.1.0 (sm_100a)"; }

@@ -1,0 +1,703 @@
+// Device kernels of the Green--Laplace engine.
+//
+// Every GL stage of the reference (eta22, psi22, the nested order-3 graph)
+// is the same three-step pattern: Fourier multiplier banks -> inverse FFTs ->
+// pointwise products -> forward FFTs -> support mask / roundoff floor ->
+// per-node weighted accumulation.  The engine runs it on a "compact grid"
+// (Ncx x Ncy, the smallest power-of-two grid on which every product of the
+// stage is alias-free; Ncx = Nx, Ncy = Ny reproduces the reference's own grid)
+// with the spectra held in small boxes around their supports:
+//
+//   col_ifft_kernel  spectral box columns -> multiplier banks -> inverse FFT
+//                    along y (only the box's columns carry data);
+//   row_kernel       one physical row: inverse FFT along x of every bank,
+//                    the stage's pointwise products, forward FFT along x, and
+//                    only the output box's columns are kept;
+//   col_fft_kernel   forward FFT along y of the kept columns, output-box rows
+//                    kept, support mask applied, per-spectrum max |.| taken;
+//   *_acc kernels    roundoff floor + per-node accumulation, elementwise;
+//   out_row_kernel   final inverse FFT along x on the reference grid.
+#pragma once
+#include "gl_analysis.cuh"
+#include "gl_fft.cuh"
+
+namespace gl {
+
+// ---------------------------------------------------------------------------
+// FFT helpers over grouped shared-memory rows
+// ---------------------------------------------------------------------------
+
+// In-place transform of `cnt` rows of length n held in `data`, in groups of
+// at most `gmax` rows through the ping-pong buffer `tmp` (gmax*n values).
+template <int SIGN>
+__device__ void fft_rows(cplx* data, cplx* tmp, int n, int log2n, int cnt, int gmax,
+                         const cplx* __restrict__ tw) {
+  for (int g0 = 0; g0 < cnt; g0 += gmax) {
+    const int g = cnt - g0 < gmax ? cnt - g0 : gmax;
+    cplx* base = data + (size_t)g0 * n;
+    cplx* res = fft_batch<SIGN>(base, tmp, n, log2n, g, tw);
+    if (res != base) {
+      for (int i = threadIdx.x; i < g * n; i += blockDim.x) base[i] = res[i];
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// multiplier banks
+// ---------------------------------------------------------------------------
+
+enum Mult : int {
+  M_ONE = 0, M_NU, M_NU2, M_NU3, M_QX_SNU, M_QY_SNU, M_Q2_SNU, M_QX, M_QY, M_Q2,
+  M_NUQX, M_NUQY, M_IQX, M_IQY, M_MI_NU, M_MI_Q2_SNU, M_MI_Q2NU, M_MINUS_A, M_MINUS_Q2,
+  M_A, M_PSI11,
+  // order-2 banks divide after the multiply: (s * qx) / safe_nu (spatial.py:199-201)
+  M_QX_DIVNU, M_QY_DIVNU, M_Q2_DIVNU
+};
+
+struct BinGeo {
+  double qx, qy, q, nu, a, sqa;
+};
+
+GL_D BinGeo load_geo(const double* geo, int plane, int i) {
+  BinGeo g;
+  g.qx = geo[i];
+  g.qy = geo[plane + i];
+  g.q = geo[2 * plane + i];
+  g.nu = geo[3 * plane + i];
+  g.a = geo[4 * plane + i];
+  g.sqa = geo[5 * plane + i];
+  return g;
+}
+
+// value = multiplier(bin) * s, in the evaluation order of the reference's
+// NumPy expressions (_order3.py:151-193, spatial.py:196-203).
+GL_D cplx apply_mult(int m, const BinGeo& g, cplx s) {
+  switch (m) {
+    case M_ONE: return s;
+    case M_NU: return cscale(g.nu, s);
+    case M_NU2: return cscale(g.nu * g.nu, s);
+    case M_NU3: return cscale(g.nu * g.nu * g.nu, s);
+    case M_QX_SNU: return cscale(g.qx / safe_nu(g.nu), s);
+    case M_QY_SNU: return cscale(g.qy / safe_nu(g.nu), s);
+    case M_Q2_SNU: return cscale((g.q * g.q) / safe_nu(g.nu), s);
+    case M_QX: return cscale(g.qx, s);
+    case M_QY: return cscale(g.qy, s);
+    case M_Q2: return cscale(g.q * g.q, s);
+    case M_NUQX: return cscale(g.nu * g.qx, s);
+    case M_NUQY: return cscale(g.nu * g.qy, s);
+    case M_IQX: return cmuli(cscale(g.qx, s));
+    case M_IQY: return cmuli(cscale(g.qy, s));
+    case M_MI_NU: return cmulmi(cscale(g.nu, s));
+    case M_MI_Q2_SNU: return cmulmi(cscale((g.q * g.q) / safe_nu(g.nu), s));
+    case M_MI_Q2NU: return cmulmi(cscale((g.q * g.q) * g.nu, s));
+    case M_MINUS_A: return cscale(-g.a, s);
+    case M_MINUS_Q2: return cscale(-(g.q * g.q), s);
+    case M_A: return cscale(g.a, s);
+    case M_PSI11: return g.nu > 0.0 ? cmk(s.y / g.nu, -s.x / g.nu) : czero();
+    case M_QX_DIVNU: { const cplx t = cscale(g.qx, s); const double sn = safe_nu(g.nu); return cmk(t.x / sn, t.y / sn); }
+    case M_QY_DIVNU: { const cplx t = cscale(g.qy, s); const double sn = safe_nu(g.nu); return cmk(t.x / sn, t.y / sn); }
+    case M_Q2_DIVNU: { const cplx t = cscale(g.q * g.q, s); const double sn = safe_nu(g.nu); return cmk(t.x / sn, t.y / sn); }
+  }
+  return czero();
+}
+
+// ---------------------------------------------------------------------------
+// column inverse FFT (spectral box -> banks along y)
+// ---------------------------------------------------------------------------
+
+enum ColKind : int {
+  COL_PLAIN = 0,   // bank k reads spectrum k of the job (no damping)
+  COL_ETA22,       // s e^{-tau_n (nu - shift)}
+  COL_PSI22,       // (s mask_c) e^{-tau (nu - shift_c)}
+  COL_INNER,       // (s e^{-tau3 (nu - shift3)}) e^{-tau2 (nu - shift2)}
+  COL_OUTER1,      // s e^{-tau3 (nu - shift3)}
+  COL_OUTER2,      // pair spectra E (eta, eta_t floored, phi, phi_t)
+};
+
+constexpr int MAX_BANKS = 24;
+
+struct ColArgs {
+  int kind;
+  int nbanks;
+  int mult[MAX_BANKS];     // multiplier per bank
+  int src_of[MAX_BANKS];   // spectrum index per bank (COL_PLAIN / COL_OUTER2)
+  Box box;                 // input box (modes)
+  const double* geo;       // geometry planes of the input box
+  const cplx* spec;        // input spectra
+  long long spec_job_stride;  // elements between jobs' spectra
+  long long spec_sub_stride;  // elements between spectra within a job
+  int jobs_per_unit;       // jobs sharing one unit's scalars / masks
+  // damping parameters
+  const UnitScalars* us;
+  const double* nodes;     // GL nodes (outer for OUTER*, eta22 for ETA22)
+  const double* nodes2;    // inner nodes
+  int n_inner;             // inner rank (COL_INNER) / nodes per branch (PSI22)
+  int n_outer;
+  const unsigned char* chan_mask;  // [unit][2][h][w] (COL_PSI22)
+  const unsigned long long* floor_max;  // per-job max for floored spectra
+  double floor_rel;
+  // output
+  cplx* out;               // [job][bank][w][n]
+  int n, log2n;            // transform length along y
+  double scale;            // applied to the inverse transform (1/(Nx Ny))
+};
+
+// Damping base value of the job at box bin i (COL_ETA22/PSI22/INNER/OUTER1).
+GL_D cplx col_base(const ColArgs& a, int job, int i, const BinGeo& g, int by, int bx) {
+  const int unit = job / a.jobs_per_unit;
+  const int sub = job % a.jobs_per_unit;
+  const UnitScalars& u = a.us[unit];
+  const cplx* s = a.spec + (long long)unit * a.spec_job_stride;
+  cplx v = s[i];
+  switch (a.kind) {
+    case COL_ETA22: {
+      const double tau = a.nodes[sub] / u.lam22;
+      return cscale(exp(-tau * (g.nu - u.shift2)), v);
+    }
+    case COL_PSI22: {
+      // sub = (branch * n_inner + node) * chan_count + channel
+      const int chan = sub % 2;
+      const int bn = sub / 2;
+      const int branch = bn / a.n_inner;
+      const int node = bn % a.n_inner;
+      if (chan >= u.chan_count) return czero();
+      const double lam = branch == 0 ? u.lam_minus : u.lam_plus;
+      const double tau = a.nodes[node] / lam;
+      const int cid = u.chan_id[chan];
+      const unsigned char m =
+          a.chan_mask[((size_t)unit * 2 + cid) * a.box.w * a.box.h + i];
+      cplx sm = m ? v : cscale(0.0, v);
+      return cscale(exp(-tau * (g.nu - u.chan_shift[chan])), sm);
+    }
+    case COL_INNER: {
+      const int jo = sub / a.n_inner;
+      const int ii = sub % a.n_inner;
+      const double tau3 = a.nodes[jo] / u.lam3;
+      const double tau2 = a.nodes2[ii] / u.lam2;
+      cplx d3 = cscale(exp(-tau3 * (g.nu - u.shift3)), v);
+      return cscale(exp(-tau2 * (g.nu - u.shift2)), d3);
+    }
+    case COL_OUTER1: {
+      const double tau3 = a.nodes[sub] / u.lam3;
+      return cscale(exp(-tau3 * (g.nu - u.shift3)), v);
+    }
+  }
+  return v;
+}
+
+__global__ void col_ifft_kernel(ColArgs a, const cplx* __restrict__ tw, int cw) {
+  extern __shared__ cplx smem[];
+  const int job = blockIdx.y;
+  const int x_first = blockIdx.x * cw;
+  const int ncol = min(cw, a.box.w - x_first);
+  const int n = a.n;
+  cplx* base = smem;                 // cw * h
+  cplx* buf = smem + (size_t)cw * n;  // cw * n
+  cplx* tmp = buf + (size_t)cw * n;   // cw * n
+  const int h = a.box.h;
+  const int plane = a.box.w * a.box.h;
+  const bool shared_base = a.kind != COL_PLAIN && a.kind != COL_OUTER2;
+  if (shared_base) {
+    for (int t = threadIdx.x; t < ncol * h; t += blockDim.x) {
+      const int c = t / h, by = t % h;
+      const int bx = x_first + c;
+      const int i = by * a.box.w + bx;
+      BinGeo g = load_geo(a.geo, plane, i);
+      base[c * h + by] = col_base(a, job, i, g, by, bx);
+    }
+  }
+  const int unit = job / a.jobs_per_unit;
+  for (int k = 0; k < a.nbanks; ++k) {
+    for (int t = threadIdx.x; t < ncol * n; t += blockDim.x) buf[t] = czero();
+    __syncthreads();
+    for (int t = threadIdx.x; t < ncol * h; t += blockDim.x) {
+      const int c = t / h, by = t % h;
+      const int bx = x_first + c;
+      const int i = by * a.box.w + bx;
+      BinGeo g = load_geo(a.geo, plane, i);
+      cplx v;
+      if (shared_base) {
+        v = base[c * h + by];
+      } else {
+        const cplx* s = a.spec + (long long)job * a.spec_job_stride +
+                        (long long)a.src_of[k] * a.spec_sub_stride;
+        v = s[i];
+        if (a.kind == COL_OUTER2 && a.src_of[k] == 1 && a.floor_max) {
+          const double pk = as_double(a.floor_max[job]);
+          if (cabs_(v) < a.floor_rel * pk) v = czero();
+        }
+      }
+      v = apply_mult(a.mult[k], g, v);
+      const int my = a.box.y0 + by;
+      buf[c * n + wrap(my, n)] = v;
+    }
+    __syncthreads();
+    fft_rows<+1>(buf, tmp, n, a.log2n, ncol, cw, tw);
+    cplx* dst = a.out + (((size_t)job * a.nbanks + k) * a.box.w + x_first) * n;
+    for (int t = threadIdx.x; t < ncol * n; t += blockDim.x) dst[t] = cscale(a.scale, buf[t]);
+    __syncthreads();
+  }
+  (void)unit;
+}
+
+// ---------------------------------------------------------------------------
+// row kernel: inverse FFT along x, products, forward FFT along x
+// ---------------------------------------------------------------------------
+
+enum RowKind : int { ROW_ETA22 = 0, ROW_PSI22, ROW_CONTACT22, ROW_INNER, ROW_OUTER };
+
+struct BankGroup {
+  const cplx* data;  // [job][nb][w][n_y]
+  int nb;            // banks in the group
+  int x0, w;         // box columns (modes)
+};
+
+struct RowArgs {
+  int kind;
+  BankGroup grp[2];
+  int ngrp;
+  int nout;
+  int out_x0, out_w;       // kept output columns (modes)
+  cplx* out;               // [job][nout][out_w][n_y]
+  int nx, log2nx;          // compact grid along x
+  int ny;                  // compact grid along y (column length of inputs)
+  const UnitScalars* us;
+  int jobs_per_unit;
+  int gmax;                // FFT group size (rows through tmp)
+};
+
+// Pointwise products of each stage; `b` points at the bank rows (bank k at
+// b + k*n), outputs overwrite the first rows at the same point.
+GL_D void row_products(int kind, cplx* b, int n, int p, int chan_count) {
+#define BK(k) b[(k) * n + p]
+  switch (kind) {
+    case ROW_ETA22: {  // spatial.py:204-205
+      cplx v = BK(0), v1 = BK(1), v2 = BK(2), hx = BK(3), hy = BK(4), rad = BK(5), jx = BK(6),
+           jy = BK(7);
+      cplx sd = csub(csub(cadd(cmul(cscale(2.0, v), v2), csq(v1)), csq(hx)), csq(hy));
+      cplx sk = cadd(cmul(cscale(2.0, v), rad), cscale(2.0, cadd(cmul(hx, jx), cmul(hy, jy))));
+      BK(0) = sd;
+      BK(1) = sk;
+      break;
+    }
+    case ROW_PSI22: {  // spatial.py:370-380; banks: channel c at 8c..8c+7
+      cplx r[8];
+      for (int i = 0; i < 2; ++i) {
+        for (int j = 0; j < 2; ++j) {
+          const int o = 2 * (2 * i + j);
+          if (i >= chan_count || j >= chan_count) { r[o] = czero(); r[o + 1] = czero(); continue; }
+          const int L = 8 * i, R = 8 * j;
+          cplx sd = csub(csub(cadd(cmul(cscale(2.0, BK(L + 0)), BK(R + 2)), cmul(BK(L + 1), BK(R + 1))),
+                              cmul(BK(L + 3), BK(R + 3))),
+                         cmul(BK(L + 4), BK(R + 4)));
+          cplx sk = cadd(cmul(cscale(2.0, BK(L + 0)), BK(R + 5)),
+                         cscale(2.0, cadd(cmul(BK(L + 3), BK(R + 6)), cmul(BK(L + 4), BK(R + 7)))));
+          r[o] = sd;
+          r[o + 1] = sk;
+        }
+      }
+      for (int o = 0; o < 8; ++o) BK(o) = r[o];
+      break;
+    }
+    case ROW_CONTACT22: {  // spatial.py:303-306: 0.5 * eta11 * (-i ifft2(s nu))
+      cplx e = BK(0);
+      cplx pz = cmulmi(BK(1));
+      BK(0) = cmul(cscale(0.5, e), pz);
+      break;
+    }
+    case ROW_INNER: {  // _order3.py:228-233
+      cplx v = BK(0), v1 = BK(1), v2 = BK(2), v3 = BK(3), hx = BK(4), hy = BK(5), jx = BK(6),
+           jy = BK(7), rad = BK(8), qq = BK(9), njx = BK(10), njy = BK(11);
+      cplx v2x = cscale(2.0, v);
+      cplx sd = csub(csub(cadd(cmul(v2x, v2), csq(v1)), csq(hx)), csq(hy));
+      cplx sk = cadd(cmul(v2x, rad), cscale(2.0, cadd(cmul(hx, jx), cmul(hy, jy))));
+      cplx sdt = csub(csub(cadd(cmul(v2x, v3), cmul(cscale(4.0, v1), v2)), cmul(cscale(2.0, hx), jx)),
+                      cmul(cscale(2.0, hy), jy));
+      cplx skt = cadd(cscale(2.0, cadd(cmul(v1, rad), cmul(v, qq))),
+                      cscale(2.0, cadd(cadd(cadd(csq(jx), cmul(hx, njx)), csq(jy)), cmul(hy, njy))));
+      BK(0) = sd;
+      BK(1) = sk;
+      BK(2) = sdt;
+      BK(3) = skt;
+      break;
+    }
+    case ROW_OUTER: {  // _order3.py:76-102, 275-287
+      // first-order banks 0..11: eta etax etay phix phiy phiz phixz phiyz phizz phizzz phitz phitzz
+      // pair banks 12..20: eta etax etay phix phiy phiz phizz phitz eta_t
+      cplx fe = BK(0), fex = BK(1), fey = BK(2), fpx = BK(3), fpy = BK(4), fpz = BK(5),
+           fpxz = BK(6), fpyz = BK(7), fpzz = BK(8), fpzzz = BK(9), fptz = BK(10), fptzz = BK(11);
+      cplx pe = BK(12), pex = BK(13), pey = BK(14), ppx = BK(15), ppy = BK(16), ppz = BK(17),
+           ppzz = BK(18), pptz = BK(19), pet = BK(20);
+      // first-state aliases: eta_t = phiz, phiz_t = phitz, phizz_t = phitzz; pair phiz_t = phitz
+      cplx fe2 = csq(fe);
+      cplx k_pair = csub(csub(cadd(cadd(cadd(cmul(fpx, pex), cmul(fpy, pey)), cmul(ppx, fex)), cmul(ppy, fey)),
+                              cmul(fe, ppzz)),
+                         cmul(pe, fpzz));
+      cplx k_direct = csub(cmul(fe, cadd(cmul(fpxz, fex), cmul(fpyz, fey))), cmul(cscale(0.5, fe2), fpzzz));
+      cplx d_pair = cadd(cadd(cadd(cadd(cmul(fe, pptz), cmul(pe, fptz)), cmul(fpx, ppx)), cmul(fpy, ppy)),
+                         cmul(fpz, ppz));
+      cplx d_direct = cadd(cmul(cscale(0.5, fe2), fptzz),
+                           cmul(fe, cadd(cadd(cmul(fpx, fpxz), cmul(fpy, fpyz)), cmul(fpz, fpzz))));
+      cplx fk = cadd(cscale(0.25, k_direct), cscale(0.5, k_pair));
+      cplx fd = cadd(cscale(0.25, d_direct), cscale(0.5, d_pair));
+      cplx contact = cadd(cadd(cmul(cscale(0.5, fe), ppz), cmul(cscale(0.5, pe), fpz)),
+                          cmul(cscale(0.125, fe2), fpzz));
+      cplx contact_t =
+          cadd(cadd(cadd(cscale(0.5, cadd(cmul(fpz, ppz), cmul(fe, pptz))),
+                         cscale(0.5, cadd(cmul(pet, fpz), cmul(pe, fptz)))),
+                    cmul(cmul(cscale(0.25, fe), fpz), fpzz)),
+               cmul(cscale(0.125, fe2), fptzz));
+      BK(0) = fk;
+      BK(1) = fd;
+      BK(2) = contact;
+      BK(3) = contact_t;
+      break;
+    }
+  }
+#undef BK
+}
+
+__global__ void row_kernel(RowArgs a, const cplx* __restrict__ tw) {
+  extern __shared__ cplx smem[];
+  const int y = blockIdx.x;
+  const int job = blockIdx.y;
+  const int n = a.nx;
+  int nb = 0;
+  for (int g = 0; g < a.ngrp; ++g) nb += a.grp[g].nb;
+  cplx* banks = smem;                       // nb * n
+  cplx* tmp = smem + (size_t)nb * n;        // gmax * n
+  for (int t = threadIdx.x; t < nb * n; t += blockDim.x) banks[t] = czero();
+  __syncthreads();
+  int k0 = 0;
+  for (int g = 0; g < a.ngrp; ++g) {
+    const BankGroup G = a.grp[g];
+    const int cnt = G.nb * G.w;
+    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+      const int k = t / G.w, xi = t % G.w;
+      const cplx v = G.data[(((size_t)job * G.nb + k) * G.w + xi) * a.ny + y];
+      banks[(size_t)(k0 + k) * n + wrap(G.x0 + xi, n)] = v;
+    }
+    k0 += G.nb;
+  }
+  __syncthreads();
+  fft_rows<+1>(banks, tmp, n, a.log2nx, nb, a.gmax, tw);
+  const int chan_count = a.kind == ROW_PSI22 ? a.us[job / a.jobs_per_unit].chan_count : 0;
+  for (int p = threadIdx.x; p < n; p += blockDim.x) row_products(a.kind, banks, n, p, chan_count);
+  __syncthreads();
+  fft_rows<-1>(banks, tmp, n, a.log2nx, a.nout, a.gmax, tw);
+  for (int t = threadIdx.x; t < a.nout * a.out_w; t += blockDim.x) {
+    const int o = t / a.out_w, xo = t % a.out_w;
+    a.out[(((size_t)job * a.nout + o) * a.out_w + xo) * a.ny + y] =
+        banks[(size_t)o * n + wrap(a.out_x0 + xo, n)];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// column forward FFT + support mask + per-spectrum max
+// ---------------------------------------------------------------------------
+
+struct ColFftArgs {
+  const cplx* in;          // [js][out_w][n]
+  cplx* out;               // [js][box h][box w]
+  Box box;                 // output box (modes)
+  int n, log2n;            // compact grid along y
+  int nsrc;                // spectra per job
+  int jobs_per_unit;
+  const unsigned char* mask;   // [unit][h][w] or null
+  unsigned long long* maxslot; // [js] or null
+  double scale;            // (Nx Ny)/(Ncx Ncy)
+};
+
+__global__ void col_fft_kernel(ColFftArgs a, const cplx* __restrict__ tw, int cw) {
+  extern __shared__ cplx smem[];
+  const int js = blockIdx.y;
+  const int job = js / a.nsrc;
+  const int unit = job / a.jobs_per_unit;
+  const int x_first = blockIdx.x * cw;
+  const int ncol = min(cw, a.box.w - x_first);
+  const int n = a.n;
+  cplx* buf = smem;
+  cplx* tmp = smem + (size_t)cw * n;
+  const cplx* src = a.in + ((size_t)js * a.box.w + x_first) * n;
+  for (int t = threadIdx.x; t < ncol * n; t += blockDim.x) buf[t] = src[t];
+  __syncthreads();
+  fft_rows<-1>(buf, tmp, n, a.log2n, ncol, cw, tw);
+  const unsigned char* mask = a.mask ? a.mask + (size_t)unit * a.box.w * a.box.h : nullptr;
+  cplx* dst = a.out + (size_t)js * a.box.w * a.box.h;
+  double local = 0.0;
+  for (int t = threadIdx.x; t < ncol * a.box.h; t += blockDim.x) {
+    const int c = t % ncol, by = t / ncol;
+    const int bx = x_first + c;
+    const int i = by * a.box.w + bx;
+    cplx v = cscale(a.scale, buf[c * n + wrap(a.box.y0 + by, n)]);
+    if (mask && !mask[i]) v = czero();
+    dst[i] = v;
+    const double m = cabs_(v);
+    local = (m > local || m != m) ? m : local;
+  }
+  if (a.maxslot) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const double other = __shfl_xor_sync(0xffffffffu, local, o);
+      local = (other > local || other != other) ? other : local;
+    }
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(a.maxslot + js, local);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// accumulation kernels (elementwise over output boxes)
+// ---------------------------------------------------------------------------
+
+GL_D cplx floored(cplx v, double rel, unsigned long long peak_bits) {
+  return cabs_(v) < rel * as_double(peak_bits) ? czero() : v;
+}
+
+struct AccArgs {
+  const UnitScalars* us;
+  const double* geo;        // geometry planes of the output box
+  Box box;
+  const cplx* in;           // stage spectra
+  const unsigned long long* maxin;
+  cplx* out;
+  unsigned long long* maxout;
+  const unsigned char* mask;    // [unit][h][w]
+  const unsigned char* pmask;   // psi22 channel-pair masks [unit][3][h][w]
+  const cplx* extra;        // psi22 contact spectrum [unit][h][w]
+  const double* nodes;
+  const double* weights;
+  int nnodes;               // rank of the accumulated loop
+  int nsub;                 // outer loop count (order-3 inner acc: jobs per unit)
+  double floor_rel;
+};
+
+// eta22: sum_n coef_n (-A sh_n sd_n + ch_n sk_n)   (spatial.py:206-221)
+__global__ void acc_eta22_kernel(AccArgs a) {
+  const int unit = blockIdx.y;
+  const int plane = a.box.w * a.box.h;
+  const UnitScalars& u = a.us[unit];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
+    BinGeo g = load_geo(a.geo, plane, i);
+    cplx acc = czero();
+    for (int nn = 0; nn < a.nnodes; ++nn) {
+      const int js = unit * a.nnodes + nn;
+      const double x = a.nodes[nn], w = a.weights[nn];
+      const double tau = x / u.lam22;
+      const double coef = w * exp(x) / u.lam22 / 4.0 * exp(-2.0 * u.shift2 * tau);
+      const double sh = sinh_over_root(g.sqa, tau);
+      const double ch = cosh(g.sqa * tau);
+      cplx sd = floored(a.in[((size_t)js * 2 + 0) * plane + i], a.floor_rel, a.maxin[js * 2 + 0]);
+      cplx sk = floored(a.in[((size_t)js * 2 + 1) * plane + i], a.floor_rel, a.maxin[js * 2 + 1]);
+      cplx term = cadd(cscale(-g.a * sh, sd), cscale(ch, sk));
+      acc = cadd(acc, cscale(coef, term));
+    }
+    a.out[(size_t)unit * plane + i] = acc;
+  }
+}
+
+// psi22 dual-branch resolvent + Taylor contact, masked to the pair support
+// (spatial.py:276-308, 384-393).
+__global__ void acc_psi22_kernel(AccArgs a) {
+  const int unit = blockIdx.y;
+  const int plane = a.box.w * a.box.h;
+  const UnitScalars& u = a.us[unit];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
+    BinGeo g = load_geo(a.geo, plane, i);
+    cplx res = czero();
+    for (int branch = 0; branch < 2; ++branch) {
+      const double lam = branch == 0 ? u.lam_minus : u.lam_plus;
+      const double ksign = branch == 0 ? -1.0 : 1.0;
+      for (int nn = 0; nn < a.nnodes; ++nn) {
+        const double x = a.nodes[nn], w = a.weights[nn];
+        const double tau = x / lam;
+        const double coef = w * exp(x) / lam / 8.0;
+        const int js = (unit * 2 + branch) * a.nnodes + nn;
+        cplx resp = czero();
+        for (int ci = 0; ci < u.chan_count; ++ci) {
+          for (int cj = 0; cj < u.chan_count; ++cj) {
+            const int o = 2 * (2 * ci + cj);
+            const cplx sd = a.in[((size_t)js * 8 + o) * plane + i];
+            const cplx sk = a.in[((size_t)js * 8 + o + 1) * plane + i];
+            const double ssum = u.chan_shift[ci] + u.chan_shift[cj];
+            const double factor =
+                branch == 0 ? exp((g.sqa - ssum) * tau) : exp(-(g.sqa + ssum) * tau);
+            const cplx ks = cscale(ksign, sk);
+            const double sa = safe_nu(g.sqa);
+            cplx part = cscale(factor, cadd(sd, cmk(ks.x / sa, ks.y / sa)));
+            // pair support of the physical channel pair
+            const int pi = u.chan_id[ci] + u.chan_id[cj];  // 0: (0,0) 1: (0,1)/(1,0) 2: (1,1)
+            const int pidx = (u.chan_count == 1) ? (u.chan_id[0] == 0 ? 0 : 2) : pi;
+            if (!a.pmask[((size_t)unit * 3 + pidx) * plane + i]) part = czero();
+            resp = cadd(resp, part);
+          }
+        }
+        res = cadd(res, cmul(cmk(0.0, coef), resp));
+      }
+    }
+    cplx total = cadd(res, a.extra[(size_t)unit * plane + i]);
+    if (!a.mask[(size_t)unit * plane + i]) total = czero();
+    a.out[(size_t)unit * plane + i] = total;
+  }
+}
+
+// order-3 inner accumulation into the four pair spectra of each outer node
+// (_order3.py:240-259); the eta_t max feeds its floor in the outer stage.
+__global__ void acc_inner_kernel(AccArgs a) {
+  const int uj = blockIdx.y;  // unit * n_outer + j
+  const int unit = uj / a.nsub;
+  const int plane = a.box.w * a.box.h;
+  const UnitScalars& u = a.us[unit];
+  double local = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
+    BinGeo g = load_geo(a.geo, plane, i);
+    cplx e = czero(), et = czero(), p = czero(), pt = czero();
+    for (int ii = 0; ii < a.nnodes; ++ii) {
+      const int js = uj * a.nnodes + ii;
+      const double x = a.nodes[ii], w = a.weights[ii];
+      const double tau = x / u.lam2;
+      const double coef = w * exp(x) / u.lam2 * exp(-2.0 * u.shift2 * tau) / 4.0;
+      const double sh = sinh_over_root(g.sqa, tau);
+      const double ch = cosh(g.sqa * tau);
+      const cplx* src = a.in + (size_t)js * 4 * plane;
+      cplx sd = floored(src[i], a.floor_rel, a.maxin[js * 4 + 0]);
+      cplx sk = floored(src[plane + i], a.floor_rel, a.maxin[js * 4 + 1]);
+      cplx sdt = floored(src[2 * plane + i], a.floor_rel, a.maxin[js * 4 + 2]);
+      cplx skt = floored(src[3 * plane + i], a.floor_rel, a.maxin[js * 4 + 3]);
+      const double mash = -g.a * sh;
+      e = cadd(e, cscale(coef, cadd(cscale(mash, sd), cscale(ch, sk))));
+      et = csub(et, cmul(cmk(0.0, coef), cadd(cscale(mash, sdt), cscale(ch, skt))));
+      p = cadd(p, cmul(cmk(0.0, coef), csub(cscale(ch, sd), cscale(sh, sk))));
+      pt = cadd(pt, cscale(coef, csub(cscale(ch, sdt), cscale(sh, skt))));
+    }
+    if (!a.mask[(size_t)unit * plane + i]) { e = czero(); et = czero(); p = czero(); pt = czero(); }
+    cplx* dst = a.out + (size_t)uj * 4 * plane;
+    dst[i] = e;
+    dst[plane + i] = et;
+    dst[2 * plane + i] = p;
+    dst[3 * plane + i] = pt;
+    const double m = cabs_(et);
+    local = (m > local || m != m) ? m : local;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double other = __shfl_xor_sync(0xffffffffu, local, o);
+    local = (other > local || other != other) ? other : local;
+  }
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(a.maxout + uj, local);
+}
+
+// order-3 outer combine: floors of the four forcing spectra, then the psi
+// forcings fk + A c and fd - c_t with their own maxima (_order3.py:103-122).
+__global__ void acc_outer_combine_kernel(AccArgs a) {
+  const int uj = blockIdx.y;
+  const int plane = a.box.w * a.box.h;
+  cplx* src = const_cast<cplx*>(a.in) + (size_t)uj * 4 * plane;
+  double l0 = 0.0, l1 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
+    BinGeo g = load_geo(a.geo, plane, i);
+    cplx fk = floored(src[i], a.floor_rel, a.maxin[uj * 4 + 0]);
+    cplx fd = floored(src[plane + i], a.floor_rel, a.maxin[uj * 4 + 1]);
+    cplx c = floored(src[2 * plane + i], a.floor_rel, a.maxin[uj * 4 + 2]);
+    cplx ct = floored(src[3 * plane + i], a.floor_rel, a.maxin[uj * 4 + 3]);
+    src[i] = fk;
+    src[plane + i] = fd;
+    cplx kpsi = cadd(fk, cscale(g.a, c));
+    cplx dpsi = csub(fd, ct);
+    // both already vanish off the triple support (their inputs were masked)
+    cplx* dst = a.out + (size_t)uj * 2 * plane;
+    dst[i] = kpsi;
+    dst[plane + i] = dpsi;
+    const double m0 = cabs_(kpsi), m1 = cabs_(dpsi);
+    l0 = (m0 > l0 || m0 != m0) ? m0 : l0;
+    l1 = (m1 > l1 || m1 != m1) ? m1 : l1;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double o0 = __shfl_xor_sync(0xffffffffu, l0, o);
+    const double o1 = __shfl_xor_sync(0xffffffffu, l1, o);
+    l0 = (o0 > l0 || o0 != o0) ? o0 : l0;
+    l1 = (o1 > l1 || o1 != o1) ? o1 : l1;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_nonneg(a.maxout + uj * 2 + 0, l0);
+    atomic_max_nonneg(a.maxout + uj * 2 + 1, l1);
+  }
+}
+
+// order-3 outer accumulation into eta33 / psi33 spectra (_order3.py:124-138).
+// `extra` holds the psi forcings, `in` the floored fk, fd.
+__global__ void acc_outer_kernel(AccArgs a, const unsigned long long* maxpsi) {
+  const int unit = blockIdx.y;
+  const int plane = a.box.w * a.box.h;
+  const UnitScalars& u = a.us[unit];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
+    BinGeo g = load_geo(a.geo, plane, i);
+    cplx eta = czero(), psi = czero();
+    for (int j = 0; j < a.nnodes; ++j) {
+      const int uj = unit * a.nnodes + j;
+      const double x = a.nodes[j], w = a.weights[j];
+      const double tau = x / u.lam3;
+      const double sh = sinh_over_root(g.sqa, tau);
+      const double ch = cosh(g.sqa * tau);
+      const double coef = w * exp(x) / u.lam3 * exp(-3.0 * u.shift3 * tau);
+      const cplx* fsrc = a.in + (size_t)uj * 4 * plane;
+      const cplx fk = fsrc[i], fd = fsrc[plane + i];
+      const cplx* psrc = a.extra + (size_t)uj * 2 * plane;
+      const cplx kpsi = floored(psrc[i], a.floor_rel, maxpsi[uj * 2 + 0]);
+      const cplx dpsi = floored(psrc[plane + i], a.floor_rel, maxpsi[uj * 2 + 1]);
+      cplx te = csub(cscale(g.a * sh, fd), cmul(cmk(0.0, ch), fk));
+      cplx tp = csub(cmul(cmk(0.0, -ch), dpsi), cscale(sh, kpsi));
+      eta = cadd(eta, cscale(coef, te));
+      psi = cadd(psi, cscale(coef, tp));
+    }
+    if (!a.mask[(size_t)unit * plane + i]) { eta = czero(); psi = czero(); }
+    a.out[((size_t)unit * 2 + 0) * plane + i] = eta;
+    a.out[((size_t)unit * 2 + 1) * plane + i] = psi;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// final inverse FFT along x on the reference grid
+// ---------------------------------------------------------------------------
+
+struct OutArgs {
+  const cplx* in;       // [uc][w][ny]  (column-transformed box spectra)
+  int w, x0;            // box columns
+  int nx, log2nx, ny;
+  int ncomp;            // components per unit in this launch
+  int comp_offset;      // first component slot in the output
+  int out_ncomp;        // component slots per unit in the output
+  const double* comp_scale;   // physical scale per component of this launch
+  void* out;            // [unit][out_ncomp][ny][nx]
+  int real_only;        // write float64 real parts instead of complex
+  int rows;             // rows per block
+};
+
+__global__ void out_row_kernel(OutArgs a, const cplx* __restrict__ tw) {
+  extern __shared__ cplx smem[];
+  const int y0 = blockIdx.x * a.rows;
+  const int uc = blockIdx.y;
+  const int unit = uc / a.ncomp, comp = uc % a.ncomp;
+  const int n = a.nx;
+  const int rows = min(a.rows, a.ny - y0);
+  cplx* buf = smem;
+  cplx* tmp = smem + (size_t)a.rows * n;
+  for (int t = threadIdx.x; t < rows * n; t += blockDim.x) buf[t] = czero();
+  __syncthreads();
+  for (int t = threadIdx.x; t < rows * a.w; t += blockDim.x) {
+    const int r = t / a.w, xi = t % a.w;
+    buf[r * n + wrap(a.x0 + xi, n)] = a.in[((size_t)uc * a.w + xi) * a.ny + y0 + r];
+  }
+  __syncthreads();
+  fft_rows<+1>(buf, tmp, n, a.log2nx, rows, a.rows, tw);
+  const double s = a.comp_scale[comp];
+  const size_t plane = (size_t)a.ny * n;
+  const size_t base = ((size_t)unit * a.out_ncomp + a.comp_offset + comp) * plane + (size_t)y0 * n;
+  if (a.real_only) {
+    double* o = reinterpret_cast<double*>(a.out) + base;
+    for (int t = threadIdx.x; t < rows * n; t += blockDim.x) o[t] = s * buf[t].x;
+  } else {
+    cplx* o = reinterpret_cast<cplx*>(a.out) + base;
+    for (int t = threadIdx.x; t < rows * n; t += blockDim.x) o[t] = cscale(s, buf[t]);
+  }
+}
+
+}  // namespace gl

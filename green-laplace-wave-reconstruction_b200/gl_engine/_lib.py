@@ -1,0 +1,117 @@
+"""ctypes binding of the engine's C ABI (``include/gl_engine.h``).
+
+This is the same binding a maintainer of the reference's Python package would
+add: plain ``ctypes`` over ``libgl_b200.so``.  Loading fails loudly when the
+library has not been built; there is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_native" / "libgl_b200.so"
+
+GL_OK = 0
+STATUS_NAMES = {
+    0: "GL_OK", 1: "GL_ERR_INVALID_ARGUMENT", 2: "GL_ERR_UNSUPPORTED", 3: "GL_ERR_OPTIONS",
+    4: "GL_ERR_UNIFORM_CURRENT", 5: "GL_ERR_COMPONENT_SIZE", 6: "GL_ERR_COMPONENTS",
+    7: "GL_ERR_SUPPORT", 8: "GL_ERR_SECTOR", 9: "GL_ERR_ZERO_INPUT", 10: "GL_ERR_ORDER2_DOMAIN",
+    11: "GL_ERR_ORDER3_DOMAIN", 12: "GL_ERR_OFF_GRID", 13: "GL_ERR_NYQUIST", 14: "GL_ERR_ALIAS",
+    15: "GL_ERR_SCALE", 16: "GL_ERR_RANK", 17: "GL_ERR_EMPTY_SUPPORT", 18: "GL_ERR_OUTSIDE_PLAN",
+    19: "GL_ERR_NONFINITE", 20: "GL_ERR_WORKSPACE", 21: "GL_ERR_CUDA", 22: "GL_ERR_TIMEOUT",
+    23: "GL_ERR_COEFFICIENTS",
+}
+
+COMP_ETA11, COMP_PSI11, COMP_ETA22, COMP_PSI22, COMP_ETA33, COMP_PSI33 = 1, 2, 4, 8, 16, 32
+COMP_NAMES = {COMP_ETA11: "eta11", COMP_PSI11: "psi11", COMP_ETA22: "eta22",
+              COMP_PSI22: "psi22", COMP_ETA33: "eta33", COMP_PSI33: "psi33"}
+GRID_COMPACT, GRID_REFERENCE = 0, 1
+OUT_COMPLEX, OUT_REAL = 0, 1
+SPECTRA_FULL, SPECTRA_BOX = 0, 1
+
+
+class PlanDesc(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int),
+        ("lx", C.c_double), ("ly", C.c_double),
+        ("depth", C.c_double), ("gravity", C.c_double),
+        ("order", C.c_int), ("components", C.c_int),
+        ("eta22_rank", C.c_int), ("inner_rank", C.c_int), ("outer_rank", C.c_int),
+        ("allow_below_model_parent_domain", C.c_int),
+        ("box_x0", C.c_int), ("box_y0", C.c_int), ("box_w", C.c_int), ("box_h", C.c_int),
+        ("grid", C.c_int), ("max_units", C.c_int), ("output", C.c_int),
+    ]
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [
+        ("ncx", C.c_int), ("ncy", C.c_int),
+        ("box1", C.c_int * 4), ("box2", C.c_int * 4), ("box3", C.c_int * 4),
+        ("n_components", C.c_int), ("component_ids", C.c_int * 6),
+        ("transforms_per_unit", C.c_double),
+    ]
+
+
+# name -> (restype, argtypes); every symbol declared in include/gl_engine.h
+SIGNATURES = {
+    "gl_plan_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(PlanDesc)]),
+    "gl_plan_destroy": (None, [C.c_void_p]),
+    "gl_plan_get_info": (C.c_int, [C.c_void_p, C.POINTER(PlanInfo)]),
+    "gl_workspace_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
+    "gl_deposit_modes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "gl_execute": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                             C.c_size_t, C.c_void_p, C.c_void_p]),
+    "gl_fft2": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "gl_gauss_laguerre": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "gl_dispersion_solve": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.c_double, C.c_double,
+                                      C.POINTER(C.c_double)]),
+    "gl_get_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
+    "gl_version": (C.c_char_p, []),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load(path: Path | None = None) -> C.CDLL:
+    """Load (once) and type the engine library.  Raises if it is missing."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        p = Path(path) if path else LIB_PATH
+        if not p.exists():
+            raise RuntimeError(
+                f"GL engine library not built: {p} is missing "
+                "(run `python __graft_entry__.py build` or gl_engine.build.build())")
+        lib = C.CDLL(str(p))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def last_error() -> str:
+    lib = load()
+    buf = C.create_string_buffer(1024)
+    lib.gl_get_last_error(buf, len(buf))
+    return buf.value.decode("utf-8", "replace")
+
+
+class EngineError(RuntimeError):
+    """A C-ABI call returned a non-zero gl_status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+
+
+def check(status: int) -> None:
+    if status != GL_OK:
+        raise EngineError(status, last_error())

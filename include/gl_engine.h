@@ -1,0 +1,158 @@
+/*
+ * gl_engine.h -- C ABI of the B200 Green--Laplace (GL) bound-wave engine.
+ *
+ * The engine evaluates the reference's spatial GL graphs on the GPU:
+ * first order (eta11, psi11), the prescribed-rank eta22, the dual-branch
+ * psi22 and the nested no-Stokes eta33 + psi33.  Every entry point takes
+ * plain pointers and sizes; device buffers are owned by the caller and
+ * complex values are interleaved float64 pairs.
+ *
+ * Reference interfaces replaced (Xinyu01091002/green-laplace-wave-reconstruction):
+ *   gl_plan_create/gl_execute   src/gl_spectral_surface.m:1-103 (stage 2 of the
+ *                               two-stage API) and its executors
+ *                               src/internal/green_laplace_eta22.m:1-79,
+ *                               ...dual_branch_green_laplace_psi22.m:1-265,
+ *                               src/internal/gl_no_stokes_eta33.m:1-274;
+ *                               Python python/src/green_laplace/spatial.py:33-414
+ *                               and _order3.py:18-297
+ *   gl_deposit_modes            src/gl_spectral_surface.m:123-149 (deposit_analytic_input)
+ *   gl_gauss_laguerre           python/src/green_laplace/quadrature.py:11-31
+ *   gl_dispersion_solve         python/src/green_laplace/dispersion.py:19-42
+ *   gl_status codes             the MATLAB 'green_laplace:<Id>' identifiers of
+ *                               src/gl_spectral_coefficients.m:9-70 and
+ *                               src/gl_spectral_surface.m:135-141
+ */
+#ifndef GL_ENGINE_H
+#define GL_ENGINE_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gl_status {
+  GL_OK = 0,
+  GL_ERR_INVALID_ARGUMENT = 1,  /* null pointer, bad size or enum value          */
+  GL_ERR_UNSUPPORTED = 2,       /* grid size / layout this engine does not run    */
+  GL_ERR_OPTIONS = 3,           /* green_laplace:Options, UnknownOption           */
+  GL_ERR_UNIFORM_CURRENT = 4,   /* green_laplace:UniformCurrent                   */
+  GL_ERR_COMPONENT_SIZE = 5,    /* green_laplace:ComponentSize                    */
+  GL_ERR_COMPONENTS = 6,        /* green_laplace:Components                       */
+  GL_ERR_SUPPORT = 7,           /* green_laplace:Support (strict-forward kx>0)    */
+  GL_ERR_SECTOR = 8,            /* green_laplace:Sector                           */
+  GL_ERR_ZERO_INPUT = 9,        /* green_laplace:ZeroInput                        */
+  GL_ERR_ORDER2_DOMAIN = 10,    /* green_laplace:Order2Domain (kh >= 0.3)         */
+  GL_ERR_ORDER3_DOMAIN = 11,    /* green_laplace:Order3Domain (kh > 0.5)          */
+  GL_ERR_OFF_GRID = 12,         /* green_laplace:OffGridComponent                 */
+  GL_ERR_NYQUIST = 13,          /* green_laplace:Nyquist                          */
+  GL_ERR_ALIAS = 14,            /* quadratic/cubic output support reaches Nyquist */
+  GL_ERR_SCALE = 15,            /* invalid GL tail scale                          */
+  GL_ERR_RANK = 16,             /* unsupported quadrature rank                    */
+  GL_ERR_EMPTY_SUPPORT = 17,    /* empty analytic support                         */
+  GL_ERR_OUTSIDE_PLAN = 18,     /* spectrum support outside the plan's box        */
+  GL_ERR_NONFINITE = 19,        /* non-finite value in an output field            */
+  GL_ERR_WORKSPACE = 20,        /* workspace too small or misaligned              */
+  GL_ERR_CUDA = 21,             /* CUDA runtime error                             */
+  GL_ERR_TIMEOUT = 22,          /* a bounded device wait ran out                  */
+  GL_ERR_COEFFICIENTS = 23      /* green_laplace:Coefficients                     */
+} gl_status;
+
+/* component bits (output order follows the bit order) */
+#define GL_COMP_ETA11 0x01
+#define GL_COMP_PSI11 0x02
+#define GL_COMP_ETA22 0x04
+#define GL_COMP_PSI22 0x08
+#define GL_COMP_ETA33 0x10
+#define GL_COMP_PSI33 0x20
+
+#define GL_GRID_COMPACT 0   /* smallest alias-free power-of-two product grid */
+#define GL_GRID_REFERENCE 1 /* products on the reference's own Nx x Ny grid   */
+
+#define GL_OUT_COMPLEX 0    /* analytic "plus" fields, complex128            */
+#define GL_OUT_REAL 1       /* real parts only, float64                      */
+
+#define GL_SPECTRA_FULL 0   /* [unit][ny][nx] complex128, numpy fft2 layout  */
+#define GL_SPECTRA_BOX 1    /* [unit][box_h][box_w] complex128               */
+
+typedef struct gl_plan gl_plan;
+
+typedef struct gl_plan_desc {
+  int nx, ny;                 /* reference grid (powers of two, 16..4096)   */
+  double lx, ly;              /* periodic domain lengths                    */
+  double depth, gravity;      /* h, g                                       */
+  int order;                  /* 1, 2 or 3                                  */
+  int components;             /* GL_COMP_* mask (0 = all for the order)     */
+  int eta22_rank;             /* 1..16 (reference default 6)                */
+  int inner_rank;             /* order 3: 4,6,8,10,12 (default 4)           */
+  int outer_rank;             /* order 3: 3,4,6,8,10 (default 4)            */
+  int allow_below_model_parent_domain;
+  int box_x0, box_y0;         /* parent support box: signed mode numbers    */
+  int box_w, box_h;
+  int grid;                   /* GL_GRID_*                                   */
+  int max_units;              /* units processed per internal group (>=1)   */
+  int output;                 /* GL_OUT_*                                    */
+} gl_plan_desc;
+
+typedef struct gl_plan_info {
+  int ncx, ncy;               /* product grid actually used                 */
+  int box1[4], box2[4], box3[4];  /* x0, y0, w, h of parent/pair/triple boxes */
+  int n_components;           /* output planes per unit                     */
+  int component_ids[6];       /* GL_COMP_* of each plane, in order          */
+  double transforms_per_unit; /* 2-D transforms of the reference graph      */
+} gl_plan_info;
+
+/* Create a plan: validates the descriptor, picks the product grid, builds
+ * geometry tables, twiddles and GL node tables on the current device. */
+gl_status gl_plan_create(gl_plan** plan, const gl_plan_desc* desc);
+void gl_plan_destroy(gl_plan* plan);
+gl_status gl_plan_get_info(const gl_plan* plan, gl_plan_info* info);
+
+/* Device workspace bytes needed by gl_execute (independent of n_units). */
+gl_status gl_workspace_size(const gl_plan* plan, size_t* bytes);
+
+/* Deposit N^2 (a+ib)/h e^{-i omega t} for n_units time snapshots into box
+ * spectra [unit][box_h][box_w].  Modes are grouped by destination bin:
+ * segment s covers modes seg_offsets[s] .. seg_offsets[s+1]-1 (summed in
+ * that order) and lands on box bin seg_bins[s] (row-major box index).
+ * d_ab holds (a, b) pairs per mode, d_omega the frequencies, d_times the
+ * unit times.  The output is fully overwritten. */
+gl_status gl_deposit_modes(const gl_plan* plan, int n_units, int n_segments,
+                           const int* d_seg_offsets, const int* d_seg_bins, int n_modes,
+                           const double* d_ab, const double* d_omega, const double* d_times,
+                           void* d_box_spectra, void* stream);
+
+/* Evaluate the plan's components for n_units analytic spectra.  d_outputs
+ * receives [unit][n_components][ny][nx] (complex128 or float64 per the plan's
+ * output mode) in physical units (eta in metres, psi = phi(x, z=eta, t)).
+ * d_unit_status (n_units ints, may be null) receives a gl_status per unit;
+ * the call itself is asynchronous on `stream` (a cudaStream_t). */
+gl_status gl_execute(gl_plan* plan, int n_units, const void* d_spectra, int spectra_layout,
+                     void* d_outputs, void* d_workspace, size_t workspace_bytes,
+                     int* d_unit_status, void* stream);
+
+/* Batched 2-D complex FFT on [batch][ny][nx] complex128 with numpy's
+ * conventions: forward = fft2 (unnormalised), inverse = ifft2 (1/(nx ny)).
+ * In-place (d_in == d_out) is allowed.  Replaces the numpy.fft.fft2/ifft2
+ * calls of python/src/green_laplace/_spectral.py:29-37. */
+gl_status gl_fft2(int batch, int nx, int ny, const void* d_in, void* d_out, int inverse,
+                  void* stream);
+
+/* Host FP64 Gauss--Laguerre rule (Golub--Welsch with the moment gate). */
+gl_status gl_gauss_laguerre(int rank, double* nodes, double* weights);
+
+/* Host FP64 Newton solve of q tanh q = omega^2 h / g for n frequencies. */
+gl_status gl_dispersion_solve(int n, const double* omega, double depth, double gravity,
+                              double* q_out);
+
+/* Message of the last error raised on the calling thread. */
+size_t gl_get_last_error(char* buffer, size_t length);
+
+/* Library version string. */
+const char* gl_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GL_ENGINE_H */
