@@ -9,6 +9,8 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <atomic>
+#include <mutex>
 
 #include "../../include/gl_engine.h"
 #include "gl_kernels.cuh"
@@ -44,6 +46,89 @@ static gl_status fail(gl_status s, const char* fmt, ...) {
     if (e_ != cudaSuccess)                                                           \
       return fail(GL_ERR_CUDA, "launch of %s failed: %s", what, cudaGetErrorString(e_)); \
   } while (0)
+
+// ---------------------------------------------------------------------------
+// launch accounting: a launch counter and optional per-kernel event timing
+// ---------------------------------------------------------------------------
+
+static std::atomic<unsigned long long> g_launches{0};
+
+struct ProfRecord {
+  const char* name;
+  cudaEvent_t start, stop;
+  double bytes;
+};
+static std::mutex g_prof_mu;
+static bool g_prof_on = false;
+static std::vector<ProfRecord> g_prof;
+
+// Wraps one kernel launch: counts it and, while profiling, brackets it with
+// events on its own stream.  `bytes` is the launch's algorithmic traffic.
+struct LaunchScope {
+  const char* name;
+  cudaStream_t st;
+  double bytes;
+  cudaEvent_t a = nullptr, b = nullptr;
+  LaunchScope(const char* n, cudaStream_t s, double by) : name(n), st(s), bytes(by) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (g_prof_on) {
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, st);
+    }
+  }
+  ~LaunchScope() {
+    if (a) {
+      cudaEventRecord(b, st);
+      std::lock_guard<std::mutex> lk(g_prof_mu);
+      g_prof.push_back(ProfRecord{name, a, b, bytes});
+    }
+  }
+};
+
+extern "C" unsigned long long gl_launch_count(void) { return g_launches.load(); }
+
+extern "C" gl_status gl_profile_begin(void) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  for (auto& r : g_prof) {
+    cudaEventDestroy(r.start);
+    cudaEventDestroy(r.stop);
+  }
+  g_prof.clear();
+  g_prof_on = true;
+  return GL_OK;
+}
+
+extern "C" gl_status gl_profile_end(gl_kernel_stat* stats, int max_stats, int* n_stats) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof_on = false;
+  std::vector<gl_kernel_stat> agg;
+  for (auto& r : g_prof) {
+    float ms = 0.f;
+    cudaEventSynchronize(r.stop);
+    cudaEventElapsedTime(&ms, r.start, r.stop);
+    cudaEventDestroy(r.start);
+    cudaEventDestroy(r.stop);
+    gl_kernel_stat* hit = nullptr;
+    for (auto& a : agg)
+      if (std::strncmp(a.name, r.name, sizeof a.name) == 0) hit = &a;
+    if (!hit) {
+      gl_kernel_stat z;
+      std::memset(&z, 0, sizeof z);
+      std::strncpy(z.name, r.name, sizeof z.name - 1);
+      agg.push_back(z);
+      hit = &agg.back();
+    }
+    hit->launches += 1;
+    hit->ms_total += ms;
+    hit->bytes_total += r.bytes;
+  }
+  g_prof.clear();
+  const int n = std::min<int>((int)agg.size(), std::max(0, max_stats));
+  for (int i = 0; i < n && stats; ++i) stats[i] = agg[i];
+  if (n_stats) *n_stats = (int)agg.size();
+  return GL_OK;
+}
 
 // ---------------------------------------------------------------------------
 // analysis kernels
@@ -872,6 +957,9 @@ static gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, c
     attr = true;
   }
   dim3 grid((a.box.w + cw - 1) / cw, njobs);
+  const double bytes = (double)njobs * a.nbanks * a.box.w * a.n * sizeof(cplx) +
+                       (double)njobs * a.box.w * a.box.h * sizeof(cplx);
+  LaunchScope ls("col_ifft_kernel", st, bytes);
   col_ifft_kernel<<<grid, 256, smem, st>>>(a, tw, cw);
   LAUNCH_CHECK("col_ifft_kernel");
   return GL_OK;
@@ -887,6 +975,10 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
     attr = true;
   }
   dim3 grid(a.ny, njobs);
+  double bytes = (double)njobs * a.nout * a.out_w * a.ny * sizeof(cplx);
+  for (int g = 0; g < a.ngrp; ++g) bytes += (double)njobs * a.grp[g].nb * a.grp[g].w * a.ny * sizeof(cplx);
+  LaunchScope ls(a.kind == ROW_INNER ? "row_kernel[inner]" : a.kind == ROW_OUTER ? "row_kernel[outer]"
+                 : "row_kernel[order2]", st, bytes);
   row_kernel<<<grid, 256, smem, st>>>(a, tw);
   LAUNCH_CHECK("row_kernel");
   return GL_OK;
@@ -901,6 +993,8 @@ static gl_status launch_col_fft(const ColFftArgs& a, int njs, cudaStream_t st, c
     attr = true;
   }
   dim3 grid((a.box.w + cw - 1) / cw, njs);
+  const double bytes = (double)njs * a.box.w * (a.n + a.box.h) * sizeof(cplx);
+  LaunchScope ls("col_fft_kernel", st, bytes);
   col_fft_kernel<<<grid, 256, smem, st>>>(a, tw, cw);
   LAUNCH_CHECK("col_fft_kernel");
   return GL_OK;
@@ -916,6 +1010,9 @@ static gl_status launch_out_rows(const OutArgs& a0, int nuc, cudaStream_t st, co
     attr = true;
   }
   dim3 grid((a.ny + a.rows - 1) / a.rows, nuc);
+  const double bytes = (double)nuc * a.w * a.ny * sizeof(cplx) +
+                       (double)nuc * a.nx * a.ny * (a.real_only ? sizeof(double) : sizeof(cplx));
+  LaunchScope ls("out_row_kernel", st, bytes);
   out_row_kernel<<<grid, 256, smem, st>>>(a, tw);
   LAUNCH_CHECK("out_row_kernel");
   return GL_OK;
@@ -1027,53 +1124,83 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
   const double* dn = p->nodes;  // [k*MAX_RANK] nodes, [(4+k)*MAX_RANK] weights
   gl_status s;
 
-  slots_init_kernel<<<(gu + 63) / 64, 64, 0, st>>>(slots, gu);
+  {
+    LaunchScope ls_("slots_init_kernel", st, 0.0);
+    slots_init_kernel<<<(gu + 63) / 64, 64, 0, st>>>(slots, gu);
+  }
   LAUNCH_CHECK("slots_init_kernel");
   const cplx* spec = boxv;
   if (layout == GL_SPECTRA_FULL) {
     CUDA_TRY(cudaMemsetAsync(boxv, 0, sizeof(cplx) * (size_t)gu * pl1, st));
     dim3 g(grid_for((size_t)p->d.nx * p->d.ny, T, 1024), gu);
-    extract_kernel<<<g, T, 0, st>>>(reinterpret_cast<const cplx*>(spectra), boxv, B1, p->d.nx,
+    {
+      LaunchScope ls_("extract_kernel", st, 0.0);
+      extract_kernel<<<g, T, 0, st>>>(reinterpret_cast<const cplx*>(spectra), boxv, B1, p->d.nx,
                                     p->d.ny, slots);
+    }
     LAUNCH_CHECK("extract_kernel");
   } else {
     spec = reinterpret_cast<const cplx*>(spectra);
     dim3 g(grid_for(pl1, T, 64), gu);
-    box_max_kernel<<<g, T, 0, st>>>(spec, pl1, slots);
+    {
+      LaunchScope ls_("box_max_kernel", st, 0.0);
+      box_max_kernel<<<g, T, 0, st>>>(spec, pl1, slots);
+    }
     LAUNCH_CHECK("box_max_kernel");
   }
   {
     dim3 g(grid_for(pl1, T, 64), gu);
-    support_kernel<<<g, T, 0, st>>>(spec, p->geo1, B1, slots, s1);
+    {
+      LaunchScope ls_("support_kernel", st, 0.0);
+      support_kernel<<<g, T, 0, st>>>(spec, p->geo1, B1, slots, s1);
+    }
     LAUNCH_CHECK("support_kernel");
-    peak_kernel<<<g, T, 0, st>>>(spec, p->geo1, B1, p->d.nx, p->d.ny, slots, s1, ch,
+    {
+      LaunchScope ls_("peak_kernel", st, 0.0);
+      peak_kernel<<<g, T, 0, st>>>(spec, p->geo1, B1, p->d.nx, p->d.ny, slots, s1, ch,
                                  p->want_psi22 ? 1 : 0);
+    }
     LAUNCH_CHECK("peak_kernel");
   }
   const bool need_s2 = p->want_eta22 || p->want_psi22 || p->want_o3;
   if (need_s2) {
     dim3 g(grid_for(B1.h * p->ww1, T, 64), gu);
-    bitrows_kernel<<<g, T, 0, st>>>(s1, B1.h, B1.w, p->ww1, s1f, s1r);
+    {
+      LaunchScope ls_("bitrows_kernel", st, 0.0);
+      bitrows_kernel<<<g, T, 0, st>>>(s1, B1.h, B1.w, p->ww1, s1f, s1r);
+    }
     LAUNCH_CHECK("bitrows_kernel");
     MinkArgs m;
     mink_args(m, s1f, B1.h, B1.w, p->ww1, s1r, B1.h, B1.w, p->ww1, s2, p->geo2, slots, 2);
     dim3 g2(grid_for(pl2, T, 256), gu);
-    minkowski_kernel<<<g2, T, 0, st>>>(m);
+    {
+      LaunchScope ls_("minkowski_kernel", st, 0.0);
+      minkowski_kernel<<<g2, T, 0, st>>>(m);
+    }
     LAUNCH_CHECK("minkowski_kernel");
   }
   if (p->want_o3) {
     dim3 g(grid_for(B2.h * p->ww2, T, 64), gu);
-    bitrows_kernel<<<g, T, 0, st>>>(s2, B2.h, B2.w, p->ww2, s2f, s2r);
+    {
+      LaunchScope ls_("bitrows_kernel", st, 0.0);
+      bitrows_kernel<<<g, T, 0, st>>>(s2, B2.h, B2.w, p->ww2, s2f, s2r);
+    }
     LAUNCH_CHECK("bitrows_kernel");
     MinkArgs m;
     mink_args(m, s2f, B2.h, B2.w, p->ww2, s1r, B1.h, B1.w, p->ww1, s3, p->geo3, slots, 3);
     dim3 g3(grid_for(pl3, T, 512), gu);
-    minkowski_kernel<<<g3, T, 0, st>>>(m);
+    {
+      LaunchScope ls_("minkowski_kernel", st, 0.0);
+      minkowski_kernel<<<g3, T, 0, st>>>(m);
+    }
     LAUNCH_CHECK("minkowski_kernel");
   }
   if (p->want_psi22) {
     dim3 g(grid_for(B1.h * p->ww1, T, 64), gu * 2);
-    bitrows_kernel<<<g, T, 0, st>>>(ch, B1.h, B1.w, p->ww1, chf, chr);
+    {
+      LaunchScope ls_("bitrows_kernel", st, 0.0);
+      bitrows_kernel<<<g, T, 0, st>>>(ch, B1.h, B1.w, p->ww1, chf, chr);
+    }
     LAUNCH_CHECK("bitrows_kernel");
     const long long cstride = (long long)B1.h * p->ww1;
     const int pairs[3][2] = {{0, 0}, {0, 1}, {1, 1}};
@@ -1085,7 +1212,10 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       m.b_job_stride = 2 * cstride;
       m.c_job_stride = 3LL * pl2;
       dim3 g2(grid_for(pl2, T, 256), gu);
-      minkowski_kernel<<<g2, T, 0, st>>>(m);
+      {
+        LaunchScope ls_("minkowski_kernel", st, 0.0);
+        minkowski_kernel<<<g2, T, 0, st>>>(m);
+      }
       LAUNCH_CHECK("minkowski_kernel");
     }
   }
@@ -1103,7 +1233,10 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     a.want_o3 = p->want_o3;
     a.allow_below = p->d.allow_below_model_parent_domain;
     a.full_input = layout == GL_SPECTRA_FULL;
-    scalars_kernel<<<(gu + 63) / 64, 64, 0, st>>>(a, gu);
+    {
+      LaunchScope ls_("scalars_kernel", st, 0.0);
+      scalars_kernel<<<(gu + 63) / 64, 64, 0, st>>>(a, gu);
+    }
     LAUNCH_CHECK("scalars_kernel");
   }
   const double fwd_scale = ((double)p->d.nx * (double)p->d.ny) / ((double)p->ncx * (double)p->ncy);
@@ -1179,7 +1312,10 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     c.nnodes = J;
     c.floor_rel = p->floor_rel;
     dim3 g(grid_for(pl2, T, 256), gu);
-    acc_eta22_kernel<<<g, T, 0, st>>>(c);
+    {
+      LaunchScope ls_("acc_eta22_kernel", st, 0.0);
+      acc_eta22_kernel<<<g, T, 0, st>>>(c);
+    }
     LAUNCH_CHECK("acc_eta22_kernel");
   }
 
@@ -1299,7 +1435,10 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     c.weights = dn + 5 * MAX_RANK;
     c.nnodes = 2;
     dim3 g(grid_for(pl2, T, 256), gu);
-    acc_psi22_kernel<<<g, T, 0, st>>>(c);
+    {
+      LaunchScope ls_("acc_psi22_kernel", st, 0.0);
+      acc_psi22_kernel<<<g, T, 0, st>>>(c);
+    }
     LAUNCH_CHECK("acc_psi22_kernel");
   }
 
@@ -1389,7 +1528,10 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       c.nsub = J;
       c.floor_rel = p->floor_rel;
       dim3 g(grid_for(pl2, T, 128), nuj);
-      acc_inner_kernel<<<g, T, 0, st>>>(c);
+      {
+        LaunchScope ls_("acc_inner_kernel", st, 0.0);
+        acc_inner_kernel<<<g, T, 0, st>>>(c);
+      }
       LAUNCH_CHECK("acc_inner_kernel");
     }
     // outer stage buffers (reuse the inner region)
@@ -1485,7 +1627,10 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       c.floor_rel = p->floor_rel;
       c.nsub = J;
       dim3 g(grid_for(pl3, T, 128), nuj);
-      acc_outer_combine_kernel<<<g, T, 0, st>>>(c);
+      {
+        LaunchScope ls_("acc_outer_combine_kernel", st, 0.0);
+        acc_outer_combine_kernel<<<g, T, 0, st>>>(c);
+      }
       LAUNCH_CHECK("acc_outer_combine_kernel");
       c.out = out33;
       c.extra = FO;
@@ -1493,7 +1638,10 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       c.weights = dn + 7 * MAX_RANK;
       c.nnodes = J;
       dim3 g2(grid_for(pl3, T, 256), gu);
-      acc_outer_kernel<<<g2, T, 0, st>>>(c, maxF);
+      {
+        LaunchScope ls_("acc_outer_kernel", st, 0.0);
+        acc_outer_kernel<<<g2, T, 0, st>>>(c, maxF);
+      }
       LAUNCH_CHECK("acc_outer_kernel");
     }
   }
@@ -1543,11 +1691,17 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
   {
     const size_t per_unit = (size_t)p->ncomp * p->d.nx * p->d.ny;
     dim3 g(grid_for(per_unit, T, 256), gu);
-    nonfinite_kernel<<<g, T, 0, st>>>(outputs, per_unit, p->d.output == GL_OUT_REAL, us);
+    {
+      LaunchScope ls_("nonfinite_kernel", st, 0.0);
+      nonfinite_kernel<<<g, T, 0, st>>>(outputs, per_unit, p->d.output == GL_OUT_REAL, us);
+    }
     LAUNCH_CHECK("nonfinite_kernel");
   }
   if (status) {
-    status_kernel<<<(gu + 63) / 64, 64, 0, st>>>(us, gu, status);
+    {
+      LaunchScope ls_("status_kernel", st, 0.0);
+      status_kernel<<<(gu + 63) / 64, 64, 0, st>>>(us, gu, status);
+    }
     LAUNCH_CHECK("status_kernel");
   }
   return GL_OK;
@@ -1593,9 +1747,12 @@ extern "C" gl_status gl_deposit_modes(const gl_plan* p, int n_units, int n_seg, 
   CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(cplx) * (size_t)n_units * plane, st));
   if (n_seg == 0) return GL_OK;
   dim3 g(grid_for(n_seg, 128, 256), n_units);
-  deposit_kernel<<<g, 128, 0, st>>>(n_seg, seg_off, seg_bin, ab, omega, times,
+  {
+    LaunchScope ls_("deposit_kernel", st, 0.0);
+    deposit_kernel<<<g, 128, 0, st>>>(n_seg, seg_off, seg_bin, ab, omega, times,
                                     (double)p->d.nx * (double)p->d.ny, p->d.depth,
                                     reinterpret_cast<cplx*>(out), plane);
+  }
   LAUNCH_CHECK("deposit_kernel");
   return GL_OK;
 }

@@ -54,6 +54,11 @@ class PlanInfo(C.Structure):
     ]
 
 
+class KernelStat(C.Structure):
+    _fields_ = [("name", C.c_char * 40), ("launches", C.c_int), ("ms_total", C.c_double),
+                ("bytes_total", C.c_double)]
+
+
 # name -> (restype, argtypes); every symbol declared in include/gl_engine.h
 SIGNATURES = {
     "gl_plan_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(PlanDesc)]),
@@ -69,6 +74,9 @@ SIGNATURES = {
     "gl_dispersion_solve": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.c_double, C.c_double,
                                       C.POINTER(C.c_double)]),
     "gl_get_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
+    "gl_launch_count": (C.c_ulonglong, []),
+    "gl_profile_begin": (C.c_int, []),
+    "gl_profile_end": (C.c_int, [C.POINTER(KernelStat), C.c_int, C.POINTER(C.c_int)]),
     "gl_version": (C.c_char_p, []),
 }
 
@@ -115,3 +123,22 @@ class EngineError(RuntimeError):
 def check(status: int) -> None:
     if status != GL_OK:
         raise EngineError(status, last_error())
+
+
+def launch_count() -> int:
+    return int(load().gl_launch_count())
+
+
+def profile_begin() -> None:
+    check(load().gl_profile_begin())
+
+
+def profile_end() -> list[dict]:
+    """Per-kernel {name, launches, ms_total, bytes_total} since profile_begin()."""
+    lib = load()
+    stats = (KernelStat * 64)()
+    n = C.c_int()
+    check(lib.gl_profile_end(stats, 64, C.byref(n)))
+    return [{"name": stats[i].name.decode(), "launches": stats[i].launches,
+             "ms_total": stats[i].ms_total, "bytes_total": stats[i].bytes_total}
+            for i in range(min(n.value, 64))]

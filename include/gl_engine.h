@@ -145,6 +145,22 @@ gl_status gl_gauss_laguerre(int rank, double* nodes, double* weights);
 gl_status gl_dispersion_solve(int n, const double* omega, double depth, double gravity,
                               double* q_out);
 
+/* Launch accounting (no reference counterpart: measurement support).
+ * gl_launch_count: kernels launched by this library since load.
+ * gl_profile_begin / gl_profile_end: while enabled, every launch is bracketed
+ * by CUDA events on its own stream; gl_profile_end synchronises them and
+ * returns per-kernel launches, total milliseconds and algorithmic bytes. */
+typedef struct gl_kernel_stat {
+  char name[40];
+  int launches;
+  double ms_total;
+  double bytes_total;
+} gl_kernel_stat;
+
+unsigned long long gl_launch_count(void);
+gl_status gl_profile_begin(void);
+gl_status gl_profile_end(gl_kernel_stat* stats, int max_stats, int* n_stats);
+
 /* Message of the last error raised on the calling thread. */
 size_t gl_get_last_error(char* buffer, size_t length);
 

@@ -426,10 +426,12 @@ def _cubic_forcing(f: dict, p: dict):
 
 
 def order3(spectrum: np.ndarray, qx: np.ndarray, qy: np.ndarray, *,
-           inner_rank: int = 4, outer_rank: int = 4):
+           inner_rank: int = 4, outer_rank: int = 4, outer_subset=None):
     """Nested no-Stokes GL eta33 + psi33 (``_order3.py:18-148``; MATLAB ``gl_no_stokes_eta33.m``).
 
     Returns (eta33/h, psi33/(h sqrt(gh)), audit), complex physical fields.
+    ``outer_subset`` (bench sampling only) restricts the outer GL loop to the
+    listed node indices, i.e. evaluates that fraction of the graph.
     """
     if inner_rank not in INNER_RANKS or outer_rank not in OUTER_RANKS:
         raise ValueError("unsupported inner or outer third-order GL rank")
@@ -454,7 +456,9 @@ def order3(spectrum: np.ndarray, qx: np.ndarray, qy: np.ndarray, *,
     onodes, oweights = gauss_laguerre(outer_rank)
     eta_hat = np.zeros_like(spectrum)
     psi_hat = np.zeros_like(spectrum)
-    for x, w in zip(onodes, oweights):
+    for j, (x, w) in enumerate(zip(onodes, oweights)):
+        if outer_subset is not None and j not in outer_subset:
+            continue
         tau = x / lam3
         damped = spectrum * np.exp(-tau * (g.nu - shift3))
         first = _first_state(damped, g)

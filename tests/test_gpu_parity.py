@@ -203,3 +203,36 @@ def test_config2_order3_matches_oracle():
     emax = float(np.max(np.abs(got[0] - st.depth * e33)) / np.max(np.abs(st.depth * e33)))
     print(f"config2 eta33 rel L2 {ee:.3e} max {emax:.3e}; psi33 rel L2 {pe:.3e}")
     assert ee < 1e-6 and pe < 1e-6
+
+
+def test_config2_deviation_is_within_oracle_roundoff_sensitivity():
+    """The FP64 oracle itself moves when only its FFT roundoff changes (the
+    roundoff floor of _spectral.py:52-64 then zeroes different bins).  The
+    engine's deviation from the oracle must stay within 3x of that spread,
+    measured here by re-running the oracle with its 2-D FFTs taken in the
+    other axis order."""
+    import numpy.fft as F
+
+    st = seastate.config2(0)
+    kxg, kyg = O.fft_wavenumber_grid(st.lx, st.ly, st.nx, st.ny)
+    oc = O.spectral_coefficients(3, st.gravity, st.depth, st.a, st.b, st.kx, st.ky)
+    s = O.deposit_modes(oc["a"], oc["b"], oc["kx"], oc["ky"], oc["omega"], st.depth, st.lx,
+                        st.ly, st.nx, st.ny, 0.0)
+    qx, qy = st.depth * kxg, st.depth * kyg
+    e0, p0, _ = O.order3(s, qx, qy)
+    f2, i2 = F.fft2, F.ifft2
+    try:
+        F.fft2 = lambda a: F.fft(F.fft(a, axis=0), axis=1)
+        F.ifft2 = lambda a: F.ifft(F.ifft(a, axis=0), axis=1)
+        e1, p1, _ = O.order3(s, qx, qy)
+    finally:
+        F.fft2, F.ifft2 = f2, i2
+    c = gl_engine.gl_spectral_coefficients(3, st.gravity, st.depth, st.a, st.b, st.kx, st.ky)
+    got = api.surface_batch_device(c, st.lx, st.ly, st.nx, st.ny, [0.0],
+                                   components=["eta33", "psi33"]).fields[0].cpu().numpy()
+    pscale = st.depth * np.sqrt(st.gravity * st.depth)
+    spread_e, spread_p = rel(e1, e0), rel(p1, p0)
+    dev_e, dev_p = rel(got[0], st.depth * e0), rel(got[1], pscale * p0)
+    print(f"oracle self-spread eta33 {spread_e:.3e} psi33 {spread_p:.3e}; "
+          f"engine deviation eta33 {dev_e:.3e} psi33 {dev_p:.3e}")
+    assert dev_e < 3 * spread_e and dev_p < 3 * spread_p
