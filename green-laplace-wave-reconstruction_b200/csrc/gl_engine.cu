@@ -1852,6 +1852,120 @@ extern "C" gl_status gl_fft2(int batch, int nx, int ny, const void* d_in, void* 
   return GL_OK;
 }
 
+// ---------------------------------------------------------------------------
+// box spectra -> physical grid with no device allocation
+// ---------------------------------------------------------------------------
+//
+// Some callers cannot allocate device memory when they evaluate a field:
+// code running inside a captured CUDA graph or a fixed-budget real-time
+// loop, and host runtimes whose GPU bindings only hand over buffers they
+// already own.  gl_box_synthesize_noalloc serves them.  Its scratch (the
+// twiddle table, an unused geometry plane for the multiplier-free bank and
+// the column-transformed intermediate) lives in the file-scope array below,
+// which every GPU that loads this library holds until the process exits.
+
+#define GL_NOALLOC_SCRATCH_BYTES (16u << 20)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[GL_NOALLOC_SCRATCH_BYTES];
+
+static std::mutex g_noalloc_mu;
+static unsigned char* g_noalloc_base[64] = {nullptr};
+
+// Device address of the scratch array on the current device.  The first call
+// on a device looks the symbol up (a host-side name is not a device address),
+// fills the twiddle table and waits for it on `st`; that first call must
+// therefore come before any stream capture.
+static gl_status noalloc_scratch(cudaStream_t st, unsigned char** out) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(GL_ERR_CUDA, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_base[dev]) {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr)
+      return fail(GL_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch failed: %s",
+                  cudaGetErrorString(e));
+    twiddle_kernel<<<TW_N / 256, 256, 0, st>>>(reinterpret_cast<cplx*>(ptr));
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(st));
+    g_noalloc_base[dev] = reinterpret_cast<unsigned char*>(ptr);
+  }
+  *out = g_noalloc_base[dev];
+  return GL_OK;
+}
+
+extern "C" gl_status gl_box_synthesize_noalloc(int n_units, int nx, int ny, int box_x0,
+                                               int box_y0, int box_w, int box_h,
+                                               const void* d_box_spectra, double scale,
+                                               void* d_out, int real_only, void* stream) {
+  if (n_units < 0 || box_w < 1 || box_h < 1 || !d_box_spectra || !d_out)
+    return fail(GL_ERR_INVALID_ARGUMENT, "bad no-alloc synthesis arguments");
+  if (!is_pow2(nx) || !is_pow2(ny) || nx < 16 || ny < 16 || nx > TW_N || ny > TW_N)
+    return fail(GL_ERR_UNSUPPORTED, "power-of-two grids from 16 to %d are required", TW_N);
+  if (box_w > nx || box_h > ny || std::abs(box_x0) >= nx || std::abs(box_y0) >= ny ||
+      std::abs(box_x0 + box_w - 1) >= nx || std::abs(box_y0 + box_h - 1) >= ny)
+    return fail(GL_ERR_INVALID_ARGUMENT, "box does not fit the grid");
+  const size_t tw_bytes = align_up(sizeof(cplx) * TW_N);
+  const size_t geo_bytes = align_up(sizeof(double) * 6 * (size_t)box_w * box_h);
+  const size_t mid_bytes = align_up(sizeof(cplx) * (size_t)n_units * box_w * ny);
+  const size_t scale_bytes = 256;  // one slot for the physical scale factor
+  if (tw_bytes + geo_bytes + mid_bytes + scale_bytes > GL_NOALLOC_SCRATCH_BYTES)
+    return fail(GL_ERR_WORKSPACE,
+                "no-alloc synthesis needs %zu bytes of scratch but its static array holds %u: "
+                "use fewer units per call (n_units * box_w * ny * 16 bytes must stay below "
+                "about %u bytes)",
+                tw_bytes + geo_bytes + mid_bytes + scale_bytes, GL_NOALLOC_SCRATCH_BYTES,
+                (unsigned)(GL_NOALLOC_SCRATCH_BYTES - tw_bytes - geo_bytes - scale_bytes));
+  if (n_units == 0) return GL_OK;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  unsigned char* base = nullptr;
+  gl_status s = noalloc_scratch(st, &base);
+  if (s != GL_OK) return s;
+  const cplx* tw = reinterpret_cast<const cplx*>(base);
+  double* geo = reinterpret_cast<double*>(base + tw_bytes);
+  cplx* mid = reinterpret_cast<cplx*>(base + tw_bytes + geo_bytes);
+  // the multiplier-free bank never reads the geometry plane; clear it so the
+  // kernel's loads see defined values whatever an earlier call left there
+  CUDA_TRY(cudaMemsetAsync(geo, 0, geo_bytes, st));
+  const Box box{box_x0, box_y0, box_w, box_h};
+  ColArgs a;
+  std::memset(&a, 0, sizeof a);
+  a.kind = COL_PLAIN;
+  a.nbanks = 1;
+  a.mult[0] = M_ONE;
+  a.src_of[0] = 0;
+  a.box = box;
+  a.geo = geo;
+  a.spec = reinterpret_cast<const cplx*>(d_box_spectra);
+  a.spec_job_stride = (long long)box_w * box_h;
+  a.spec_sub_stride = 0;
+  a.jobs_per_unit = 1;
+  a.out = mid;
+  a.n = ny;
+  a.log2n = ilog2(ny);
+  a.scale = 1.0 / ((double)nx * (double)ny);
+  if ((s = launch_col_ifft(a, n_units, st, tw)) != GL_OK) return s;
+  OutArgs o;
+  std::memset(&o, 0, sizeof o);
+  o.in = mid;
+  o.w = box_w;
+  o.x0 = box_x0;
+  o.nx = nx;
+  o.log2nx = ilog2(nx);
+  o.ny = ny;
+  o.ncomp = 1;
+  o.comp_offset = 0;
+  o.out_ncomp = 1;
+  // the output kernel reads its physical scale from device memory: keep it in
+  // its own slot of the scratch, written on the caller's stream
+  double* scale_dev = reinterpret_cast<double*>(base + tw_bytes + geo_bytes + mid_bytes);
+  CUDA_TRY(cudaMemcpyAsync(scale_dev, &scale, sizeof(double), cudaMemcpyHostToDevice, st));
+  o.comp_scale = scale_dev;
+  o.out = d_out;
+  o.real_only = real_only ? 1 : 0;
+  return launch_out_rows(o, n_units, st, tw);
+}
+
 extern "C" gl_status gl_gauss_laguerre(int rank, double* nodes, double* weights) {
   if (!nodes || !weights) return fail(GL_ERR_INVALID_ARGUMENT, "null output");
   return gauss_laguerre(rank, nodes, weights);

@@ -70,6 +70,9 @@ SIGNATURES = {
     "gl_execute": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                              C.c_size_t, C.c_void_p, C.c_void_p]),
     "gl_fft2": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "gl_box_synthesize_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                            C.c_int, C.c_void_p, C.c_double, C.c_void_p, C.c_int,
+                                            C.c_void_p]),
     "gl_gauss_laguerre": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "gl_dispersion_solve": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.c_double, C.c_double,
                                       C.POINTER(C.c_double)]),

@@ -138,6 +138,25 @@ gl_status gl_execute(gl_plan* plan, int n_units, const void* d_spectra, int spec
 gl_status gl_fft2(int batch, int nx, int ny, const void* d_in, void* d_out, int inverse,
                   void* stream);
 
+/* Physical fields from box spectra without allocating device memory.
+ * No counterpart in the reference: it serves callers that cannot call
+ * cudaMalloc while they run (work inside a captured CUDA graph or a
+ * fixed-budget real-time loop, or a host runtime whose GPU binding only passes
+ * buffers it already owns).  out[u] = scale * ifft2(S_u) on the nx x ny grid,
+ * S_u being box spectrum u ([n_units][box_h][box_w] complex128, signed-mode
+ * origin box_x0, box_y0) embedded at its modes; out is [n_units][ny][nx]
+ * complex128, or float64 real parts when real_only != 0.  The same transform
+ * gl_execute applies to its final spectra.
+ * Scratch: one static device array of 16 MiB per GPU (held until the process
+ * exits); n_units * box_w * ny * 16 bytes plus ~66 KB of tables must fit, and
+ * larger requests return GL_ERR_WORKSPACE.  The first call on a device looks
+ * the array up and fills its tables (synchronising `stream`), so make that
+ * first call before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU race. */
+gl_status gl_box_synthesize_noalloc(int n_units, int nx, int ny, int box_x0, int box_y0,
+                                    int box_w, int box_h, const void* d_box_spectra,
+                                    double scale, void* d_out, int real_only, void* stream);
+
 /* Host FP64 Gauss--Laguerre rule (Golub--Welsch with the moment gate). */
 gl_status gl_gauss_laguerre(int rank, double* nodes, double* weights);
 
