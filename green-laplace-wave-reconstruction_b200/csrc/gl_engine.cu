@@ -660,7 +660,7 @@ static const int ROW_GMAX = 4;
 static const size_t SMEM_LIMIT = 227 * 1024;
 
 static size_t row_smem(int nbanks, int ncx) {
-  return (size_t)(nbanks + ROW_GMAX) * ncx * sizeof(cplx);
+  return (size_t)nbanks * padded_len(ncx) * sizeof(cplx);
 }
 
 // Scratch bytes of each stage, for `g` units.
@@ -948,9 +948,14 @@ static int grid_for(size_t n, int threads, int cap = 4096) {
   return (int)b;
 }
 
+static int fft_cols_per_block(int n, int w) {
+  const int T = n / 16;
+  return std::max(1, std::min(256 / T, w));
+}
+
 static gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
-  const int cw = std::max(1, 2048 / a.n);
-  const size_t smem = (size_t)3 * cw * a.n * sizeof(cplx);
+  const int cw = fft_cols_per_block(a.n, a.box.w);
+  const size_t smem = ((size_t)cw * padded_len(a.n) + (size_t)cw * a.box.h) * sizeof(cplx);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(col_ifft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
@@ -985,8 +990,8 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
 }
 
 static gl_status launch_col_fft(const ColFftArgs& a, int njs, cudaStream_t st, const cplx* tw) {
-  const int cw = std::max(1, 2048 / a.n);
-  const size_t smem = (size_t)2 * cw * a.n * sizeof(cplx);
+  const int cw = fft_cols_per_block(a.n, a.box.w);
+  const size_t smem = (size_t)cw * padded_len(a.n) * sizeof(cplx);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(col_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
@@ -1002,14 +1007,15 @@ static gl_status launch_col_fft(const ColFftArgs& a, int njs, cudaStream_t st, c
 
 static gl_status launch_out_rows(const OutArgs& a0, int nuc, cudaStream_t st, const cplx* tw) {
   OutArgs a = a0;
-  a.rows = std::max(1, 2048 / a.nx);
-  const size_t smem = (size_t)2 * a.rows * a.nx * sizeof(cplx);
+  const int G = 256 / (a.nx / 16);
+  a.rows = G;
+  const size_t smem = (size_t)G * padded_len(a.nx) * sizeof(cplx);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(out_row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
     attr = true;
   }
-  dim3 grid((a.ny + a.rows - 1) / a.rows, nuc);
+  dim3 grid((a.ny + G - 1) / G, nuc);
   const double bytes = (double)nuc * a.w * a.ny * sizeof(cplx) +
                        (double)nuc * a.nx * a.ny * (a.real_only ? sizeof(double) : sizeof(cplx));
   LaunchScope ls("out_row_kernel", st, bytes);

@@ -20,6 +20,7 @@
 #pragma once
 #include "gl_analysis.cuh"
 #include "gl_fft.cuh"
+#include "gl_fftreg.cuh"
 
 namespace gl {
 
@@ -70,34 +71,46 @@ GL_D BinGeo load_geo(const double* geo, int plane, int i) {
   return g;
 }
 
+// Geometry planes of a box: qx, qy, q, nu, A, sqrt(A) at i, plane, 2 plane, ...
+struct GeoRef {
+  const double* g;
+  int plane, i;
+  GL_D double qx() const { return __ldg(g + i); }
+  GL_D double qy() const { return __ldg(g + plane + i); }
+  GL_D double q() const { return __ldg(g + 2 * plane + i); }
+  GL_D double nu() const { return __ldg(g + 3 * plane + i); }
+  GL_D double a() const { return __ldg(g + 4 * plane + i); }
+};
+
 // value = multiplier(bin) * s, in the evaluation order of the reference's
-// NumPy expressions (_order3.py:151-193, spatial.py:196-203).
-GL_D cplx apply_mult(int m, const BinGeo& g, cplx s) {
+// NumPy expressions (_order3.py:151-193, spatial.py:196-203); only the
+// geometry planes a multiplier needs are read.
+GL_D cplx apply_mult(int m, const GeoRef& g, cplx s) {
   switch (m) {
     case M_ONE: return s;
-    case M_NU: return cscale(g.nu, s);
-    case M_NU2: return cscale(g.nu * g.nu, s);
-    case M_NU3: return cscale(g.nu * g.nu * g.nu, s);
-    case M_QX_SNU: return cscale(g.qx / safe_nu(g.nu), s);
-    case M_QY_SNU: return cscale(g.qy / safe_nu(g.nu), s);
-    case M_Q2_SNU: return cscale((g.q * g.q) / safe_nu(g.nu), s);
-    case M_QX: return cscale(g.qx, s);
-    case M_QY: return cscale(g.qy, s);
-    case M_Q2: return cscale(g.q * g.q, s);
-    case M_NUQX: return cscale(g.nu * g.qx, s);
-    case M_NUQY: return cscale(g.nu * g.qy, s);
-    case M_IQX: return cmuli(cscale(g.qx, s));
-    case M_IQY: return cmuli(cscale(g.qy, s));
-    case M_MI_NU: return cmulmi(cscale(g.nu, s));
-    case M_MI_Q2_SNU: return cmulmi(cscale((g.q * g.q) / safe_nu(g.nu), s));
-    case M_MI_Q2NU: return cmulmi(cscale((g.q * g.q) * g.nu, s));
-    case M_MINUS_A: return cscale(-g.a, s);
-    case M_MINUS_Q2: return cscale(-(g.q * g.q), s);
-    case M_A: return cscale(g.a, s);
-    case M_PSI11: return g.nu > 0.0 ? cmk(s.y / g.nu, -s.x / g.nu) : czero();
-    case M_QX_DIVNU: { const cplx t = cscale(g.qx, s); const double sn = safe_nu(g.nu); return cmk(t.x / sn, t.y / sn); }
-    case M_QY_DIVNU: { const cplx t = cscale(g.qy, s); const double sn = safe_nu(g.nu); return cmk(t.x / sn, t.y / sn); }
-    case M_Q2_DIVNU: { const cplx t = cscale(g.q * g.q, s); const double sn = safe_nu(g.nu); return cmk(t.x / sn, t.y / sn); }
+    case M_NU: return cscale(g.nu(), s);
+    case M_NU2: { const double nu = g.nu(); return cscale(nu * nu, s); }
+    case M_NU3: { const double nu = g.nu(); return cscale(nu * nu * nu, s); }
+    case M_QX_SNU: return cscale(g.qx() / safe_nu(g.nu()), s);
+    case M_QY_SNU: return cscale(g.qy() / safe_nu(g.nu()), s);
+    case M_Q2_SNU: { const double q = g.q(); return cscale((q * q) / safe_nu(g.nu()), s); }
+    case M_QX: return cscale(g.qx(), s);
+    case M_QY: return cscale(g.qy(), s);
+    case M_Q2: { const double q = g.q(); return cscale(q * q, s); }
+    case M_NUQX: return cscale(g.nu() * g.qx(), s);
+    case M_NUQY: return cscale(g.nu() * g.qy(), s);
+    case M_IQX: return cmuli(cscale(g.qx(), s));
+    case M_IQY: return cmuli(cscale(g.qy(), s));
+    case M_MI_NU: return cmulmi(cscale(g.nu(), s));
+    case M_MI_Q2_SNU: { const double q = g.q(); return cmulmi(cscale((q * q) / safe_nu(g.nu()), s)); }
+    case M_MI_Q2NU: { const double q = g.q(); return cmulmi(cscale((q * q) * g.nu(), s)); }
+    case M_MINUS_A: return cscale(-g.a(), s);
+    case M_MINUS_Q2: { const double q = g.q(); return cscale(-(q * q), s); }
+    case M_A: return cscale(g.a(), s);
+    case M_PSI11: { const double nu = g.nu(); return nu > 0.0 ? cmk(s.y / nu, -s.x / nu) : czero(); }
+    case M_QX_DIVNU: { const cplx t = cscale(g.qx(), s); const double sn = safe_nu(g.nu()); return cmk(t.x / sn, t.y / sn); }
+    case M_QY_DIVNU: { const cplx t = cscale(g.qy(), s); const double sn = safe_nu(g.nu()); return cmk(t.x / sn, t.y / sn); }
+    case M_Q2_DIVNU: { const double q = g.q(); const cplx t = cscale(q * q, s); const double sn = safe_nu(g.nu()); return cmk(t.x / sn, t.y / sn); }
   }
   return czero();
 }
@@ -144,7 +157,7 @@ struct ColArgs {
 };
 
 // Damping base value of the job at box bin i (COL_ETA22/PSI22/INNER/OUTER1).
-GL_D cplx col_base(const ColArgs& a, int job, int i, const BinGeo& g, int by, int bx) {
+GL_D cplx col_base(const ColArgs& a, int job, int i, double nu) {
   const int unit = job / a.jobs_per_unit;
   const int sub = job % a.jobs_per_unit;
   const UnitScalars& u = a.us[unit];
@@ -153,7 +166,7 @@ GL_D cplx col_base(const ColArgs& a, int job, int i, const BinGeo& g, int by, in
   switch (a.kind) {
     case COL_ETA22: {
       const double tau = a.nodes[sub] / u.lam22;
-      return cscale(exp(-tau * (g.nu - u.shift2)), v);
+      return cscale(exp(-tau * (nu - u.shift2)), v);
     }
     case COL_PSI22: {
       // sub = (branch * n_inner + node) * chan_count + channel
@@ -168,77 +181,85 @@ GL_D cplx col_base(const ColArgs& a, int job, int i, const BinGeo& g, int by, in
       const unsigned char m =
           a.chan_mask[((size_t)unit * 2 + cid) * a.box.w * a.box.h + i];
       cplx sm = m ? v : cscale(0.0, v);
-      return cscale(exp(-tau * (g.nu - u.chan_shift[chan])), sm);
+      return cscale(exp(-tau * (nu - u.chan_shift[chan])), sm);
     }
     case COL_INNER: {
       const int jo = sub / a.n_inner;
       const int ii = sub % a.n_inner;
       const double tau3 = a.nodes[jo] / u.lam3;
       const double tau2 = a.nodes2[ii] / u.lam2;
-      cplx d3 = cscale(exp(-tau3 * (g.nu - u.shift3)), v);
-      return cscale(exp(-tau2 * (g.nu - u.shift2)), d3);
+      cplx d3 = cscale(exp(-tau3 * (nu - u.shift3)), v);
+      return cscale(exp(-tau2 * (nu - u.shift2)), d3);
     }
     case COL_OUTER1: {
       const double tau3 = a.nodes[sub] / u.lam3;
-      return cscale(exp(-tau3 * (g.nu - u.shift3)), v);
+      return cscale(exp(-tau3 * (nu - u.shift3)), v);
     }
   }
   return v;
 }
 
-__global__ void col_ifft_kernel(ColArgs a, const cplx* __restrict__ tw, int cw) {
+// One block: `cw` box columns of one job.  Each column is one length-n
+// inverse transform along y run by a group of n/16 threads; the damped base
+// spectrum of the columns is computed once and every bank applies its
+// multiplier while the first FFT pass reads it.  Output layout
+// [job][bank][y][column] (rows contiguous for the row kernel).
+__global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx* __restrict__ tw, int cw) {
   extern __shared__ cplx smem[];
   const int job = blockIdx.y;
   const int x_first = blockIdx.x * cw;
   const int ncol = min(cw, a.box.w - x_first);
   const int n = a.n;
-  cplx* base = smem;                 // cw * h
-  cplx* buf = smem + (size_t)cw * n;  // cw * n
-  cplx* tmp = buf + (size_t)cw * n;   // cw * n
+  const int L = padded_len(n);
   const int h = a.box.h;
   const int plane = a.box.w * a.box.h;
+  cplx* bufs = smem;                   // cw * L
+  cplx* base = smem + (size_t)cw * L;  // cw * h
   const bool shared_base = a.kind != COL_PLAIN && a.kind != COL_OUTER2;
   if (shared_base) {
     for (int t = threadIdx.x; t < ncol * h; t += blockDim.x) {
       const int c = t / h, by = t % h;
-      const int bx = x_first + c;
-      const int i = by * a.box.w + bx;
-      BinGeo g = load_geo(a.geo, plane, i);
-      base[c * h + by] = col_base(a, job, i, g, by, bx);
+      const int i = by * a.box.w + x_first + c;
+      base[c * h + by] = col_base(a, job, i, __ldg(a.geo + 3 * plane + i));
     }
   }
-  const int unit = job / a.jobs_per_unit;
+  __syncthreads();
+  int g, G;
+  const FftGroup f = fft_group(n, a.log2n, g, G);
+  const int iters = (ncol + G - 1) / G;
   for (int k = 0; k < a.nbanks; ++k) {
-    for (int t = threadIdx.x; t < ncol * n; t += blockDim.x) buf[t] = czero();
-    __syncthreads();
-    for (int t = threadIdx.x; t < ncol * h; t += blockDim.x) {
-      const int c = t / h, by = t % h;
-      const int bx = x_first + c;
-      const int i = by * a.box.w + bx;
-      BinGeo g = load_geo(a.geo, plane, i);
-      cplx v;
-      if (shared_base) {
-        v = base[c * h + by];
-      } else {
-        const cplx* s = a.spec + (long long)job * a.spec_job_stride +
-                        (long long)a.src_of[k] * a.spec_sub_stride;
-        v = s[i];
-        if (a.kind == COL_OUTER2 && a.src_of[k] == 1 && a.floor_max) {
-          const double pk = as_double(a.floor_max[job]);
-          if (cabs_(v) < a.floor_rel * pk) v = czero();
+    const int mult = a.mult[k];
+    const cplx* sk = a.spec + (long long)job * a.spec_job_stride + (long long)a.src_of[k] * a.spec_sub_stride;
+    const bool floor_it = a.kind == COL_OUTER2 && a.src_of[k] == 1 && a.floor_max;
+    const double floor_abs = floor_it ? a.floor_rel * as_double(a.floor_max[job]) : 0.0;
+    for (int it = 0; it < iters; ++it) {
+      const int c = it * G + g;
+      const bool active = c < ncol;
+      cplx* buf = bufs + (size_t)(active ? c : 0) * L;
+      auto load = [&](int yb) -> cplx {
+        const int by = wrap(yb - a.box.y0, n);
+        if (by >= h) return czero();
+        const int i = by * a.box.w + x_first + c;
+        cplx v;
+        if (shared_base) {
+          v = base[c * h + by];
+        } else {
+          v = sk[i];
+          if (floor_it && cabs_(v) < floor_abs) v = czero();
         }
-      }
-      v = apply_mult(a.mult[k], g, v);
-      const int my = a.box.y0 + by;
-      buf[c * n + wrap(my, n)] = v;
+        return apply_mult(mult, GeoRef{a.geo, plane, i}, v);
+      };
+      auto store = [&](int yb, cplx v) { buf[phys(yb)] = v; };
+      fft_row<+1>(buf, f, active, tw, load, store);
     }
     __syncthreads();
-    fft_rows<+1>(buf, tmp, n, a.log2n, ncol, cw, tw);
-    cplx* dst = a.out + (((size_t)job * a.nbanks + k) * a.box.w + x_first) * n;
-    for (int t = threadIdx.x; t < ncol * n; t += blockDim.x) dst[t] = cscale(a.scale, buf[t]);
+    cplx* dst = a.out + ((size_t)job * a.nbanks + k) * n * a.box.w + x_first;
+    for (int t = threadIdx.x; t < n * ncol; t += blockDim.x) {
+      const int y = t / ncol, c = t % ncol;
+      dst[(size_t)y * a.box.w + c] = cscale(a.scale, bufs[(size_t)c * L + phys(y)]);
+    }
     __syncthreads();
   }
-  (void)unit;
 }
 
 // ---------------------------------------------------------------------------
@@ -269,8 +290,8 @@ struct RowArgs {
 
 // Pointwise products of each stage; `b` points at the bank rows (bank k at
 // b + k*n), outputs overwrite the first rows at the same point.
-GL_D void row_products(int kind, cplx* b, int n, int p, int chan_count) {
-#define BK(k) b[(k) * n + p]
+GL_D void row_products(int kind, cplx* b, int L, int p, int chan_count) {
+#define BK(k) b[(k) * L + p]
   switch (kind) {
     case ROW_ETA22: {  // spatial.py:204-205
       cplx v = BK(0), v1 = BK(1), v2 = BK(2), hx = BK(3), hy = BK(4), rad = BK(5), jx = BK(6),
@@ -287,12 +308,12 @@ GL_D void row_products(int kind, cplx* b, int n, int p, int chan_count) {
         for (int j = 0; j < 2; ++j) {
           const int o = 2 * (2 * i + j);
           if (i >= chan_count || j >= chan_count) { r[o] = czero(); r[o + 1] = czero(); continue; }
-          const int L = 8 * i, R = 8 * j;
-          cplx sd = csub(csub(cadd(cmul(cscale(2.0, BK(L + 0)), BK(R + 2)), cmul(BK(L + 1), BK(R + 1))),
-                              cmul(BK(L + 3), BK(R + 3))),
-                         cmul(BK(L + 4), BK(R + 4)));
-          cplx sk = cadd(cmul(cscale(2.0, BK(L + 0)), BK(R + 5)),
-                         cscale(2.0, cadd(cmul(BK(L + 3), BK(R + 6)), cmul(BK(L + 4), BK(R + 7)))));
+          const int li = 8 * i, ri = 8 * j;
+          cplx sd = csub(csub(cadd(cmul(cscale(2.0, BK(li + 0)), BK(ri + 2)), cmul(BK(li + 1), BK(ri + 1))),
+                              cmul(BK(li + 3), BK(ri + 3))),
+                         cmul(BK(li + 4), BK(ri + 4)));
+          cplx sk = cadd(cmul(cscale(2.0, BK(li + 0)), BK(ri + 5)),
+                         cscale(2.0, cadd(cmul(BK(li + 3), BK(ri + 6)), cmul(BK(li + 4), BK(ri + 7)))));
           r[o] = sd;
           r[o + 1] = sk;
         }
@@ -358,38 +379,51 @@ GL_D void row_products(int kind, cplx* b, int n, int p, int chan_count) {
 #undef BK
 }
 
-__global__ void row_kernel(RowArgs a, const cplx* __restrict__ tw) {
+// One block per (row y, job): inverse transforms along x of every bank
+// (inputs read straight from the column-transformed rows, zero outside the
+// bank's box columns), the stage's products, forward transforms of the
+// outputs, and only the output box's columns are written: [job][out][y][col].
+__global__ void __launch_bounds__(256, 2) row_kernel(RowArgs a, const cplx* __restrict__ tw) {
   extern __shared__ cplx smem[];
   const int y = blockIdx.x;
   const int job = blockIdx.y;
   const int n = a.nx;
+  const int L = padded_len(n);
   int nb = 0;
-  for (int g = 0; g < a.ngrp; ++g) nb += a.grp[g].nb;
-  cplx* banks = smem;                       // nb * n
-  cplx* tmp = smem + (size_t)nb * n;        // gmax * n
-  for (int t = threadIdx.x; t < nb * n; t += blockDim.x) banks[t] = czero();
-  __syncthreads();
-  int k0 = 0;
-  for (int g = 0; g < a.ngrp; ++g) {
-    const BankGroup G = a.grp[g];
-    const int cnt = G.nb * G.w;
-    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
-      const int k = t / G.w, xi = t % G.w;
-      const cplx v = G.data[(((size_t)job * G.nb + k) * G.w + xi) * a.ny + y];
-      banks[(size_t)(k0 + k) * n + wrap(G.x0 + xi, n)] = v;
-    }
-    k0 += G.nb;
+  for (int q = 0; q < a.ngrp; ++q) nb += a.grp[q].nb;
+  cplx* banks = smem;  // nb * L
+  int g, G;
+  const FftGroup f = fft_group(n, a.log2nx, g, G);
+  for (int it = 0; it < (nb + G - 1) / G; ++it) {
+    const int k = it * G + g;
+    const bool active = k < nb;
+    int q = 0, kk = active ? k : 0;
+    while (q + 1 < a.ngrp && kk >= a.grp[q].nb) kk -= a.grp[q++].nb;
+    const BankGroup B = a.grp[q];
+    const cplx* row = B.data + (((size_t)job * B.nb + kk) * a.ny + y) * B.w;
+    cplx* buf = banks + (size_t)(active ? k : 0) * L;
+    auto load = [&](int xb) -> cplx {
+      const int xi = wrap(xb - B.x0, n);
+      return xi < B.w ? row[xi] : czero();
+    };
+    auto store = [&](int xb, cplx v) { buf[phys(xb)] = v; };
+    fft_row<+1>(buf, f, active, tw, load, store);
   }
   __syncthreads();
-  fft_rows<+1>(banks, tmp, n, a.log2nx, nb, a.gmax, tw);
   const int chan_count = a.kind == ROW_PSI22 ? a.us[job / a.jobs_per_unit].chan_count : 0;
-  for (int p = threadIdx.x; p < n; p += blockDim.x) row_products(a.kind, banks, n, p, chan_count);
+  for (int p = threadIdx.x; p < n; p += blockDim.x) row_products(a.kind, banks, L, phys(p), chan_count);
   __syncthreads();
-  fft_rows<-1>(banks, tmp, n, a.log2nx, a.nout, a.gmax, tw);
-  for (int t = threadIdx.x; t < a.nout * a.out_w; t += blockDim.x) {
-    const int o = t / a.out_w, xo = t % a.out_w;
-    a.out[(((size_t)job * a.nout + o) * a.out_w + xo) * a.ny + y] =
-        banks[(size_t)o * n + wrap(a.out_x0 + xo, n)];
+  for (int it = 0; it < (a.nout + G - 1) / G; ++it) {
+    const int o = it * G + g;
+    const bool active = o < a.nout;
+    cplx* buf = banks + (size_t)(active ? o : 0) * L;
+    cplx* orow = a.out + (((size_t)job * a.nout + (active ? o : 0)) * a.ny + y) * a.out_w;
+    auto load = [&](int xb) -> cplx { return buf[phys(xb)]; };
+    auto store = [&](int xb, cplx v) {
+      const int xo = wrap(xb - a.out_x0, n);
+      if (xo < a.out_w) orow[xo] = v;
+    };
+    fft_row<-1>(buf, f, active, tw, load, store);
   }
 }
 
@@ -409,7 +443,11 @@ struct ColFftArgs {
   double scale;            // (Nx Ny)/(Ncx Ncy)
 };
 
-__global__ void col_fft_kernel(ColFftArgs a, const cplx* __restrict__ tw, int cw) {
+// One block: `cw` kept columns of one (job, source) spectrum.  Rows of the
+// input ([js][y][col]) are staged with coalesced loads, each column is one
+// forward transform along y, and only the output box's rows are written
+// (support-masked), with the spectrum's max |.| folded into maxslot.
+__global__ void __launch_bounds__(256, 2) col_fft_kernel(ColFftArgs a, const cplx* __restrict__ tw, int cw) {
   extern __shared__ cplx smem[];
   const int js = blockIdx.y;
   const int job = js / a.nsrc;
@@ -417,20 +455,32 @@ __global__ void col_fft_kernel(ColFftArgs a, const cplx* __restrict__ tw, int cw
   const int x_first = blockIdx.x * cw;
   const int ncol = min(cw, a.box.w - x_first);
   const int n = a.n;
-  cplx* buf = smem;
-  cplx* tmp = smem + (size_t)cw * n;
-  const cplx* src = a.in + ((size_t)js * a.box.w + x_first) * n;
-  for (int t = threadIdx.x; t < ncol * n; t += blockDim.x) buf[t] = src[t];
+  const int L = padded_len(n);
+  cplx* bufs = smem;  // cw * L
+  const cplx* src = a.in + (size_t)js * n * a.box.w + x_first;
+  for (int t = threadIdx.x; t < n * ncol; t += blockDim.x) {
+    const int y = t / ncol, c = t % ncol;
+    bufs[(size_t)c * L + phys(y)] = src[(size_t)y * a.box.w + c];
+  }
   __syncthreads();
-  fft_rows<-1>(buf, tmp, n, a.log2n, ncol, cw, tw);
+  int g, G;
+  const FftGroup f = fft_group(n, a.log2n, g, G);
+  for (int it = 0; it < (ncol + G - 1) / G; ++it) {
+    const int c = it * G + g;
+    const bool active = c < ncol;
+    cplx* buf = bufs + (size_t)(active ? c : 0) * L;
+    auto load = [&](int yb) -> cplx { return buf[phys(yb)]; };
+    auto store = [&](int yb, cplx v) { buf[phys(yb)] = v; };
+    fft_row<-1>(buf, f, active, tw, load, store);
+  }
+  __syncthreads();
   const unsigned char* mask = a.mask ? a.mask + (size_t)unit * a.box.w * a.box.h : nullptr;
   cplx* dst = a.out + (size_t)js * a.box.w * a.box.h;
   double local = 0.0;
   for (int t = threadIdx.x; t < ncol * a.box.h; t += blockDim.x) {
     const int c = t % ncol, by = t / ncol;
-    const int bx = x_first + c;
-    const int i = by * a.box.w + bx;
-    cplx v = cscale(a.scale, buf[c * n + wrap(a.box.y0 + by, n)]);
+    const int i = by * a.box.w + x_first + c;
+    cplx v = cscale(a.scale, bufs[(size_t)c * L + phys(wrap(a.box.y0 + by, n))]);
     if (mask && !mask[i]) v = czero();
     dst[i] = v;
     const double m = cabs_(v);
@@ -671,32 +721,37 @@ struct OutArgs {
   int rows;             // rows per block
 };
 
-__global__ void out_row_kernel(OutArgs a, const cplx* __restrict__ tw) {
+// Final inverse transform along x on the reference grid: each group of n/16
+// threads takes one output row (inputs [uc][y][col], zero outside the box
+// columns) and writes scaled complex values or real parts.
+__global__ void __launch_bounds__(256, 2) out_row_kernel(OutArgs a, const cplx* __restrict__ tw) {
   extern __shared__ cplx smem[];
-  const int y0 = blockIdx.x * a.rows;
+  const int n = a.nx;
+  const int L = padded_len(n);
+  int g, G;
+  const FftGroup f = fft_group(n, a.log2nx, g, G);
+  const int y = blockIdx.x * G + g;
   const int uc = blockIdx.y;
   const int unit = uc / a.ncomp, comp = uc % a.ncomp;
-  const int n = a.nx;
-  const int rows = min(a.rows, a.ny - y0);
-  cplx* buf = smem;
-  cplx* tmp = smem + (size_t)a.rows * n;
-  for (int t = threadIdx.x; t < rows * n; t += blockDim.x) buf[t] = czero();
-  __syncthreads();
-  for (int t = threadIdx.x; t < rows * a.w; t += blockDim.x) {
-    const int r = t / a.w, xi = t % a.w;
-    buf[r * n + wrap(a.x0 + xi, n)] = a.in[((size_t)uc * a.w + xi) * a.ny + y0 + r];
-  }
-  __syncthreads();
-  fft_rows<+1>(buf, tmp, n, a.log2nx, rows, a.rows, tw);
+  const bool active = y < a.ny;
+  const int yy = active ? y : 0;
+  cplx* buf = smem + (size_t)g * L;
+  const cplx* row = a.in + ((size_t)uc * a.ny + yy) * a.w;
   const double s = a.comp_scale[comp];
-  const size_t plane = (size_t)a.ny * n;
-  const size_t base = ((size_t)unit * a.out_ncomp + a.comp_offset + comp) * plane + (size_t)y0 * n;
+  const size_t base = ((size_t)unit * a.out_ncomp + a.comp_offset + comp) * (size_t)a.ny * n +
+                      (size_t)yy * n;
+  auto load = [&](int xb) -> cplx {
+    const int xi = wrap(xb - a.x0, n);
+    return xi < a.w ? row[xi] : czero();
+  };
   if (a.real_only) {
     double* o = reinterpret_cast<double*>(a.out) + base;
-    for (int t = threadIdx.x; t < rows * n; t += blockDim.x) o[t] = s * buf[t].x;
+    auto store = [&](int xb, cplx v) { o[xb] = s * v.x; };
+    fft_row<+1>(buf, f, active, tw, load, store);
   } else {
     cplx* o = reinterpret_cast<cplx*>(a.out) + base;
-    for (int t = threadIdx.x; t < rows * n; t += blockDim.x) o[t] = cscale(s, buf[t]);
+    auto store = [&](int xb, cplx v) { o[xb] = cscale(s, v); };
+    fft_row<+1>(buf, f, active, tw, load, store);
   }
 }
 
