@@ -14,6 +14,7 @@
 
 #include "../../include/gl_engine.h"
 #include "gl_kernels.cuh"
+#include "gl_wit.cuh"
 
 using namespace gl;
 
@@ -961,11 +962,12 @@ static gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, c
     cudaFuncSetAttribute(col_ifft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
     attr = true;
   }
-  dim3 grid((a.box.w + cw - 1) / cw, njobs);
+  const int bpb = std::min(a.nbanks, 4);  // banks per block: grid.z spreads the rest
+  dim3 grid((a.box.w + cw - 1) / cw, njobs, (a.nbanks + bpb - 1) / bpb);
   const double bytes = (double)njobs * a.nbanks * a.box.w * a.n * sizeof(cplx) +
                        (double)njobs * a.box.w * a.box.h * sizeof(cplx);
   LaunchScope ls("col_ifft_kernel", st, bytes);
-  col_ifft_kernel<<<grid, 256, smem, st>>>(a, tw, cw);
+  col_ifft_kernel<<<grid, 256, smem, st>>>(a, tw, cw, bpb);
   LAUNCH_CHECK("col_ifft_kernel");
   return GL_OK;
 }
@@ -980,11 +982,15 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
     attr = true;
   }
   dim3 grid(a.ny, njobs);
+  // 8 transform groups per block (n/16 threads each) when the row has at
+  // most 12 banks (4 blocks fit per SM by shared memory), 16 for the wider
+  // outer stage (2 blocks per SM); at least one warp
+  const int threads = std::max(32, std::min(256, (nb <= 12 ? 8 : 16) * (a.nx / 16)));
   double bytes = (double)njobs * a.nout * a.out_w * a.ny * sizeof(cplx);
   for (int g = 0; g < a.ngrp; ++g) bytes += (double)njobs * a.grp[g].nb * a.grp[g].w * a.ny * sizeof(cplx);
   LaunchScope ls(a.kind == ROW_INNER ? "row_kernel[inner]" : a.kind == ROW_OUTER ? "row_kernel[outer]"
                  : "row_kernel[order2]", st, bytes);
-  row_kernel<<<grid, 256, smem, st>>>(a, tw);
+  row_kernel<<<grid, threads, smem, st>>>(a, tw);
   LAUNCH_CHECK("row_kernel");
   return GL_OK;
 }
@@ -1970,6 +1976,142 @@ extern "C" gl_status gl_box_synthesize_noalloc(int n_units, int nx, int ny, int 
   o.out = d_out;
   o.real_only = real_only ? 1 : 0;
   return launch_out_rows(o, n_units, st, tw);
+}
+
+// ---------------------------------------------------------------------------
+// WIT fourth-order quartet sum (sector 44)
+// ---------------------------------------------------------------------------
+
+static std::mutex g_wit_mu;
+static bool g_wit_tables[64] = {false};
+
+// Set partitions of every subset mask, enumerated like
+// directional_eta4_openmp.cpp:60-89 (assignment codes counted up with the
+// mask's slots as base-b digits, least significant first; surjective only).
+static gl_status wit_upload_tables() {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_wit_mu);
+  if (dev >= 0 && dev < 64 && g_wit_tables[dev]) return GL_OK;
+  unsigned int parts[160];
+  unsigned char off[16][5], cnt[16][5];
+  std::memset(off, 0, sizeof off);
+  std::memset(cnt, 0, sizeof cnt);
+  int n = 0;
+  for (int mask = 1; mask < 16; ++mask) {
+    int slots[4], k = 0;
+    for (int sl = 0; sl < 4; ++sl)
+      if (mask & (1 << sl)) slots[k++] = sl;
+    for (int b = 1; b <= 4; ++b) {
+      off[mask][b] = (unsigned char)n;
+      int total = 1;
+      for (int i = 0; i < k; ++i) total *= b;
+      for (int code = 0; code < total; ++code) {
+        int cur = code, seen = 0;
+        unsigned int blocks[4] = {0, 0, 0, 0};
+        for (int i = 0; i < k; ++i) {
+          const int as = cur % b;
+          cur /= b;
+          seen |= 1 << as;
+          blocks[as] |= 1u << slots[i];
+        }
+        if (seen == (1 << b) - 1) {
+          if (n >= 160) return fail(GL_ERR_CUDA, "partition table overflow");
+          parts[n++] = blocks[0] | (blocks[1] << 8) | (blocks[2] << 16) | (blocks[3] << 24);
+          cnt[mask][b] += 1;
+        }
+      }
+    }
+  }
+  CUDA_TRY(cudaMemcpyToSymbol(c_wit_parts, parts, sizeof parts));
+  CUDA_TRY(cudaMemcpyToSymbol(c_wit_off, off, sizeof off));
+  CUDA_TRY(cudaMemcpyToSymbol(c_wit_cnt, cnt, sizeof cnt));
+  if (dev >= 0 && dev < 64) g_wit_tables[dev] = true;
+  return GL_OK;
+}
+
+static size_t wit_binom_stride(int n_modes) { return (size_t)n_modes + 4; }
+
+extern "C" size_t gl_wit_workspace_size(int n_modes) {
+  if (n_modes < 1) return 0;
+  return align_up(sizeof(WitStats)) + 5 * wit_binom_stride(n_modes) * sizeof(unsigned long long);
+}
+
+extern "C" gl_status gl_wit_eta44(int n_modes, const int* d_modes, int n_cases, const void* d_amp,
+                                  int nx, int ny, double gravity, double depth, double dkx,
+                                  double dky, double threshold, void* d_out, void* d_work,
+                                  size_t work_bytes, void* stream) {
+  if (n_modes < 1 || n_modes > 65535 || n_cases < 1 || !d_modes || !d_amp || !d_out || !d_work)
+    return fail(GL_ERR_INVALID_ARGUMENT, "bad WIT arguments (modes 1..65535, cases >= 1, non-null buffers)");
+  if (nx < 2 || ny < 2 || (nx % 2) || (ny % 2))
+    return fail(GL_ERR_INVALID_ARGUMENT, "WIT grid sizes must be positive and even");
+  if (!(gravity > 0) || !(depth > 0) || !(dkx > 0) || !(dky > 0) || !(threshold > 0))
+    return fail(GL_ERR_INVALID_ARGUMENT, "gravity, depth, dk and the resonance threshold must be positive");
+  if (work_bytes < gl_wit_workspace_size(n_modes))
+    return fail(GL_ERR_WORKSPACE, "WIT workspace needs %zu bytes", gl_wit_workspace_size(n_modes));
+  gl_status s = wit_upload_tables();
+  if (s != GL_OK) return s;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const size_t stride = wit_binom_stride(n_modes);
+  std::vector<unsigned long long> binom(5 * stride, 0ull);
+  for (size_t v = 0; v < stride; ++v) {
+    binom[v] = 1;
+    for (int r = 1; r <= 4; ++r)
+      binom[r * stride + v] = v == 0 ? 0ull : binom[r * stride + v - 1] + binom[(r - 1) * stride + v - 1];
+  }
+  WitStats init;
+  std::memset(&init, 0, sizeof init);
+  init.min_detuning = BITS_POS_INF;
+  char* work = reinterpret_cast<char*>(d_work);
+  unsigned long long* d_binom = reinterpret_cast<unsigned long long*>(work + align_up(sizeof(WitStats)));
+  CUDA_TRY(cudaMemcpyAsync(work, &init, sizeof init, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(d_binom, binom.data(), binom.size() * sizeof(unsigned long long),
+                           cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemsetAsync(d_out, 0, sizeof(cplx) * 5 * (size_t)n_cases * nx * ny, st));
+  CUDA_TRY(cudaStreamSynchronize(st));  // host staging buffers above go out of scope
+  WitArgs a;
+  a.n_modes = n_modes;
+  a.modes = d_modes;
+  a.n_cases = n_cases;
+  a.amp = reinterpret_cast<const cplx*>(d_amp);
+  a.nx = nx;
+  a.ny = ny;
+  a.dkx = dkx;
+  a.dky = dky;
+  a.thr = threshold;
+  a.M = WitModel{gravity, depth};
+  a.out = reinterpret_cast<cplx*>(d_out);
+  a.stats = reinterpret_cast<WitStats*>(work);
+  a.n_quartets = binom[4 * stride + n_modes + 3];
+  a.binom = d_binom;
+  a.binom_stride = (int)stride;
+  const int blocks = (int)std::min<unsigned long long>((a.n_quartets + 127) / 128, 148ull * 32);
+  {
+    LaunchScope ls("wit44_kernel", st, 0.0);
+    wit44_kernel<<<blocks, 128, 0, st>>>(a);
+  }
+  LAUNCH_CHECK("wit44_kernel");
+  return GL_OK;
+}
+
+extern "C" gl_status gl_wit_read_stats(const void* d_work, int n_modes, gl_wit_stats* out) {
+  if (!d_work || !out || n_modes < 1) return fail(GL_ERR_INVALID_ARGUMENT, "bad WIT stats arguments");
+  WitStats w;
+  CUDA_TRY(cudaMemcpy(&w, d_work, sizeof w, cudaMemcpyDeviceToHost));
+  const unsigned long long n = (unsigned long long)n_modes;
+  out->candidates = n * (n + 1) * (n + 2) * (n + 3) / 24;
+  out->kept = w.kept;
+  out->near = w.near;
+  out->strict_zero_output = w.strict_zero_output;
+  out->strict_zero_intermediate = w.strict_zero_intermediate;
+  double t;
+  std::memcpy(&t, &w.max_residual, sizeof t);
+  out->max_residual = t;
+  std::memcpy(&t, &w.min_detuning, sizeof t);
+  out->min_detuning = t;
+  std::memcpy(&t, &w.max_strict_src, sizeof t);
+  out->max_strict_zero_source = t;
+  return GL_OK;
 }
 
 extern "C" gl_status gl_gauss_laguerre(int rank, double* nodes, double* weights) {

@@ -204,11 +204,14 @@ GL_D cplx col_base(const ColArgs& a, int job, int i, double nu) {
 // spectrum of the columns is computed once and every bank applies its
 // multiplier while the first FFT pass reads it.  Output layout
 // [job][bank][y][column] (rows contiguous for the row kernel).
-__global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx* __restrict__ tw, int cw) {
+__global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx* __restrict__ tw,
+                                                         int cw, int banks_per_block) {
   extern __shared__ cplx smem[];
   const int job = blockIdx.y;
   const int x_first = blockIdx.x * cw;
   const int ncol = min(cw, a.box.w - x_first);
+  const int k_first = blockIdx.z * banks_per_block;
+  const int k_last = min(a.nbanks, k_first + banks_per_block);
   const int n = a.n;
   const int L = padded_len(n);
   const int h = a.box.h;
@@ -227,7 +230,7 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
   int g, G;
   const FftGroup f = fft_group(n, a.log2n, g, G);
   const int iters = (ncol + G - 1) / G;
-  for (int k = 0; k < a.nbanks; ++k) {
+  for (int k = k_first; k < k_last; ++k) {
     const int mult = a.mult[k];
     const cplx* sk = a.spec + (long long)job * a.spec_job_stride + (long long)a.src_of[k] * a.spec_sub_stride;
     const bool floor_it = a.kind == COL_OUTER2 && a.src_of[k] == 1 && a.floor_max;
@@ -392,20 +395,32 @@ __global__ void __launch_bounds__(256, 2) row_kernel(RowArgs a, const cplx* __re
   int nb = 0;
   for (int q = 0; q < a.ngrp; ++q) nb += a.grp[q].nb;
   cplx* banks = smem;  // nb * L
+  // stage 0: zero the rows and gather every bank's box columns with
+  // coalesced loads (all loads in flight at once)
+  for (int t = threadIdx.x; t < nb * L; t += blockDim.x) banks[t] = czero();
+  __syncthreads();
+  {
+    int k0 = 0;
+    for (int q = 0; q < a.ngrp; ++q) {
+      const BankGroup B = a.grp[q];
+      const int cnt = B.nb * B.w;
+      const cplx* src = B.data + ((size_t)job * B.nb * a.ny + y) * B.w;
+      for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+        const int kk = t / B.w, xi = t % B.w;
+        banks[(size_t)(k0 + kk) * L + phys(wrap(B.x0 + xi, n))] =
+            src[(size_t)kk * a.ny * B.w + xi];
+      }
+      k0 += B.nb;
+    }
+  }
+  __syncthreads();
   int g, G;
   const FftGroup f = fft_group(n, a.log2nx, g, G);
   for (int it = 0; it < (nb + G - 1) / G; ++it) {
     const int k = it * G + g;
     const bool active = k < nb;
-    int q = 0, kk = active ? k : 0;
-    while (q + 1 < a.ngrp && kk >= a.grp[q].nb) kk -= a.grp[q++].nb;
-    const BankGroup B = a.grp[q];
-    const cplx* row = B.data + (((size_t)job * B.nb + kk) * a.ny + y) * B.w;
     cplx* buf = banks + (size_t)(active ? k : 0) * L;
-    auto load = [&](int xb) -> cplx {
-      const int xi = wrap(xb - B.x0, n);
-      return xi < B.w ? row[xi] : czero();
-    };
+    auto load = [&](int xb) -> cplx { return buf[phys(xb)]; };
     auto store = [&](int xb, cplx v) { buf[phys(xb)] = v; };
     fft_row<+1>(buf, f, active, tw, load, store);
   }

@@ -59,6 +59,13 @@ class KernelStat(C.Structure):
                 ("bytes_total", C.c_double)]
 
 
+class WitStats(C.Structure):
+    _fields_ = [("candidates", C.c_ulonglong), ("kept", C.c_ulonglong), ("near", C.c_ulonglong),
+                ("strict_zero_output", C.c_ulonglong), ("strict_zero_intermediate", C.c_ulonglong),
+                ("max_residual", C.c_double), ("min_detuning", C.c_double),
+                ("max_strict_zero_source", C.c_double)]
+
+
 # name -> (restype, argtypes); every symbol declared in include/gl_engine.h
 SIGNATURES = {
     "gl_plan_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(PlanDesc)]),
@@ -73,6 +80,11 @@ SIGNATURES = {
     "gl_box_synthesize_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                             C.c_int, C.c_void_p, C.c_double, C.c_void_p, C.c_int,
                                             C.c_void_p]),
+    "gl_wit_workspace_size": (C.c_size_t, [C.c_int]),
+    "gl_wit_eta44": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                               C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                               C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
+    "gl_wit_read_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(WitStats)]),
     "gl_gauss_laguerre": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "gl_dispersion_solve": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.c_double, C.c_double,
                                       C.POINTER(C.c_double)]),

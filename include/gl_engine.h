@@ -157,6 +157,25 @@ gl_status gl_box_synthesize_noalloc(int n_units, int nx, int ny, int box_x0, int
                                     int box_w, int box_h, const void* d_box_spectra,
                                     double scale, void* d_out, int real_only, void* stream);
 
+/* Fourth-order WIT direct sum, sector 44 (all four parents on the + branch).
+ * Replaces the sector-44 path of paper/order4/cpp/directional_eta4_openmp.cpp
+ * (DirectionalKernel::evaluate :157-453, quartet loop :690-734, output
+ * :747-773).  d_modes: (mx, my) int32 pairs; d_amp: [case][mode] complex128;
+ * d_out: 5 planes [field][case][ny][nx] complex128 (eta, psi, etaCoordinate,
+ * psiCoordinate, retained), zeroed and accumulated by the call; d_work:
+ * gl_wit_workspace_size(n_modes) device bytes (statistics + binomial table). */
+typedef struct gl_wit_stats {
+  unsigned long long candidates, kept, near, strict_zero_output, strict_zero_intermediate;
+  double max_residual, min_detuning, max_strict_zero_source;
+} gl_wit_stats;
+
+size_t gl_wit_workspace_size(int n_modes);
+gl_status gl_wit_eta44(int n_modes, const int* d_modes, int n_cases, const void* d_amp, int nx,
+                       int ny, double gravity, double depth, double dkx, double dky,
+                       double threshold, void* d_out, void* d_work, size_t work_bytes,
+                       void* stream);
+gl_status gl_wit_read_stats(const void* d_work, int n_modes, gl_wit_stats* out);
+
 /* Host FP64 Gauss--Laguerre rule (Golub--Welsch with the moment gate). */
 gl_status gl_gauss_laguerre(int rank, double* nodes, double* weights);
 
