@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(128) wit44_kernel(WitArgs a) {
       }
     }
     for (int v = 2; v <= run; ++v) rep *= v;
-    const int ix = wrap(tx, a.nx), iy = wrap(ty, a.ny);
+    const int ix = ((tx % a.nx) + a.nx) % a.nx, iy = ((ty % a.ny) + a.ny) % a.ny;  // any even size
     const size_t plane = (size_t)a.nx * a.ny;
     const size_t field = plane * a.n_cases;
     for (int cs = 0; cs < a.n_cases; ++cs) {
