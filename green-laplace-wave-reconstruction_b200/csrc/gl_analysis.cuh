@@ -29,7 +29,7 @@ struct UnitSlots {
   unsigned long long chan_max[2];
   unsigned long long count;      // support size
   unsigned long long nonfinite;  // set when a non-finite value is met
-  unsigned long long pad[3];
+  unsigned long long pad[3];   // [0] min q over S, [1] max |s| outside the box, [2] max sqrt(A) over the quartic support
 };
 
 constexpr int MAX_RANK = 16;
@@ -47,7 +47,7 @@ struct UnitScalars {
   int chan_id[2];           // physical channel index of each compacted channel
   int chan_count;
   int status;               // 0 ok, else GL_ERR_* code
-  double pad;
+  double lam4, shift4;      // order-4 (eta44) outer scale and balance shift
 };
 
 constexpr unsigned long long BITS_POS_INF = 0x7ff0000000000000ull;

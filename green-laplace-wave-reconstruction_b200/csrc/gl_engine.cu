@@ -15,6 +15,7 @@
 #include "../../include/gl_engine.h"
 #include "gl_kernels.cuh"
 #include "gl_wit.cuh"
+#include "gl_eta44.cuh"
 
 using namespace gl;
 
@@ -137,8 +138,10 @@ extern "C" gl_status gl_profile_end(gl_kernel_stat* stats, int max_stats, int* n
 
 // Geometry planes of a box on the reference grid.  kx follows numpy's
 // 2*pi*fftfreq(nx, d=lx/nx) evaluation order (_spectral.py:9-16).
+// dk > 0 selects the order-4 convention qx = (depth dk) mx of
+// gl_eta44_fftw.cpp:91-93 instead of numpy's fftfreq evaluation.
 __global__ void geo_kernel(double* geo, Box box, int nx, int ny, double lx, double ly,
-                           double depth) {
+                           double depth, double dk) {
   const int plane = box.w * box.h;
   const double valx = 1.0 / ((double)nx * (lx / (double)nx));
   const double valy = 1.0 / ((double)ny * (ly / (double)ny));
@@ -146,9 +149,14 @@ __global__ void geo_kernel(double* geo, Box box, int nx, int ny, double lx, doub
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
     const int mx = box.x0 + i % box.w;
     const int my = box.y0 + i / box.w;
-    const double kx = two_pi * ((double)mx * valx);
-    const double ky = two_pi * ((double)my * valy);
-    const double qx = depth * kx, qy = depth * ky;
+    double qx, qy;
+    if (dk > 0.0) {
+      qx = depth * dk * (double)mx;
+      qy = depth * dk * (double)my;
+    } else {
+      qx = depth * (two_pi * ((double)mx * valx));
+      qy = depth * (two_pi * ((double)my * valy));
+    }
     const double q = hypot(qx, qy);
     const double a = q * tanh(q);
     geo[i] = qx;
@@ -394,7 +402,8 @@ __global__ void minkowski_kernel(MinkArgs m) {
   if (m.which) {
     for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
     if ((threadIdx.x & 31) == 0)
-      atomic_max_nonneg(m.which == 2 ? &m.slots[job].sqa_max2 : &m.slots[job].sqa_max3, lmax);
+      atomic_max_nonneg(m.which == 2 ? &m.slots[job].sqa_max2
+                        : m.which == 3 ? &m.slots[job].sqa_max3 : &m.slots[job].pad[2], lmax);
   }
 }
 
@@ -408,6 +417,8 @@ struct ScalarArgs {
   int want_eta22, want_psi22, want_o3;
   int allow_below;
   int full_input;
+  int want_e44;
+  double fixed_peak;  // > 0: peak depth supplied by the caller (order 4)
 };
 
 // Scales, shifts and status per unit (spatial.py:179-189, 246-268;
@@ -437,7 +448,7 @@ __global__ void scalars_kernel(ScalarArgs a, int n) {
     const int mx = ix < a.nx / 2 ? ix : ix - a.nx;
     const int my = iy < a.ny / 2 ? iy : iy - a.ny;
     const int i = (my - a.box.y0) * a.box.w + (mx - a.box.x0);
-    const double qp = a.geo1[2 * a.box.w * a.box.h + i];
+    const double qp = a.fixed_peak > 0.0 ? a.fixed_peak : a.geo1[2 * a.box.w * a.box.h + i];
     r.peak_q = qp;
     const double pnu = sqrt(qp * tanh(qp));
     const double sqa2 = as_double(s.sqa_max2);
@@ -472,6 +483,15 @@ __global__ void scalars_kernel(ScalarArgs a, int n) {
       r.lam2 = 2.0 * pnu - sqrt(2.0 * qp * tanh(2.0 * qp));
       r.lam3 = 3.0 * pnu - sqrt(3.0 * qp * tanh(3.0 * qp));
       if (!(r.lam2 > 0.0) || !(r.lam3 > 0.0)) status = GL_ERR_SCALE;
+    }
+    if (a.want_e44) {  // gl_eta44_fftw.cpp:121-128
+      const double sqa3 = as_double(s.sqa_max3), sqa4 = as_double(s.pad[2]);
+      r.shift3 = 0.5 * (r.nu_min + sqa3 / 3.0);
+      r.shift4 = 0.5 * (r.nu_min + sqa4 / 4.0);
+      r.lam2 = 2.0 * pnu - sqrt(2.0 * qp * tanh(2.0 * qp));
+      r.lam3 = 3.0 * pnu - sqrt(3.0 * qp * tanh(3.0 * qp));
+      r.lam4 = 4.0 * pnu - sqrt(4.0 * qp * tanh(4.0 * qp));
+      if (!(r.lam2 > 0.0) || !(r.lam3 > 0.0) || !(r.lam4 > 0.0)) status = GL_ERR_SCALE;
     }
   }
   r.status = status;
@@ -633,6 +653,14 @@ struct gl_plan {
   size_t o_slots, o_us, o_box, o_s1, o_s1f, o_s1r, o_s2, o_s2f, o_s2r, o_s3, o_ch, o_chf, o_chr,
       o_pm, o_out22, o_outp22, o_out33, o_scratch;
   size_t scratch_bytes;
+  // fourth-order eta44 plans (gl_eta44_plan_create)
+  bool e44 = false;
+  int R44 = 0;
+  double dk44 = 0.0, peak44 = 0.0;
+  Box b4;
+  int ww3 = 0;
+  double* geo4 = nullptr;
+  size_t o_s3f = 0, o_s3r = 0, o_s4 = 0, o_e44 = 0;
 };
 
 static int ilog2(int v) {
@@ -723,6 +751,7 @@ static size_t stage_scratch(const gl_plan* p, int g) {
 
 static void plan_free(gl_plan* p) {
   if (!p) return;
+  cudaFree(p->geo4);
   cudaFree(p->geo1);
   cudaFree(p->geo2);
   cudaFree(p->geo3);
@@ -845,7 +874,7 @@ extern "C" gl_status gl_plan_create(gl_plan** out, const gl_plan_desc* desc) {
     if (e == cudaSuccess) e = cudaMalloc(g, sizeof(double) * 6 * b.w * b.h);
     if (e == cudaSuccess) {
       const int plane = b.w * b.h;
-      geo_kernel<<<std::min(1024, (plane + 255) / 256), 256>>>(*g, b, d.nx, d.ny, d.lx, d.ly, d.depth);
+      geo_kernel<<<std::min(1024, (plane + 255) / 256), 256>>>(*g, b, d.nx, d.ny, d.lx, d.ly, d.depth, 0.0);
       e = cudaGetLastError();
     }
   };
@@ -928,6 +957,11 @@ extern "C" gl_status gl_plan_get_info(const gl_plan* p, gl_plan_info* info) {
   if (p->want_eta22) t += 10.0 * p->ranks[0] + 3;
   if (p->want_psi22) t += 108;
   if (p->want_o3) t += p->ranks[3] * (25.0 + 16.0 * p->ranks[2]) + 5;
+  if (p->e44) {  // gl_eta44_fftw.cpp: third level, first/pair at order 4, forcing, final
+    const double R = p->R44;
+    const double pair = R * (16 + 6) + 18;
+    t = R * (R * (16 + (R * (16 + 6) + 15) + 4) + 8 + 19 + pair + 2) + 1;
+  }
   info->transforms_per_unit = t;
   return GL_OK;
 }
@@ -1110,8 +1144,12 @@ static int comp_slot(const gl_plan* p, int id) {
 // one group of units
 // ---------------------------------------------------------------------------
 
+static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int layout,
+                                 void* outputs, void* ws, int* status, cudaStream_t st);
+
 static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, void* outputs,
                            void* ws, int* status, cudaStream_t st) {
+  if (p->e44) return run_group_eta44(p, gu, spectra, layout, outputs, ws, status, st);
   const int T = 256;
   const Box B1 = p->b1, B2 = p->b2, B3 = p->b3;
   const int pl1 = B1.w * B1.h, pl2 = B2.w * B2.h, pl3 = B3.w * B3.h;
@@ -1245,6 +1283,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     a.want_o3 = p->want_o3;
     a.allow_below = p->d.allow_below_model_parent_domain;
     a.full_input = layout == GL_SPECTRA_FULL;
+    a.want_e44 = 0;
+    a.fixed_peak = 0.0;
     {
       LaunchScope ls_("scalars_kernel", st, 0.0);
       scalars_kernel<<<(gu + 63) / 64, 64, 0, st>>>(a, gu);
@@ -1702,6 +1742,583 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
   }
   {
     const size_t per_unit = (size_t)p->ncomp * p->d.nx * p->d.ny;
+    dim3 g(grid_for(per_unit, T, 256), gu);
+    {
+      LaunchScope ls_("nonfinite_kernel", st, 0.0);
+      nonfinite_kernel<<<g, T, 0, st>>>(outputs, per_unit, p->d.output == GL_OUT_REAL, us);
+    }
+    LAUNCH_CHECK("nonfinite_kernel");
+  }
+  if (status) {
+    {
+      LaunchScope ls_("status_kernel", st, 0.0);
+      status_kernel<<<(gu + 63) / 64, 64, 0, st>>>(us, gu, status);
+    }
+    LAUNCH_CHECK("status_kernel");
+  }
+  return GL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// fourth-order eta44 (paper/order4/cpp/gl_eta44_fftw.cpp)
+// ---------------------------------------------------------------------------
+
+// Bank tables of the eta44 graph (multiplier, source spectrum).
+static const int E44_FIRST_MULT[19] = {
+    M_ONE, M_IQX, M_IQY, M_QX_SNU, M_QY_SNU, M_MI_NU, M_NUQX, M_NUQY, M_MI_Q2_SNU, M_MI_Q2NU,
+    M_MINUS_A, M_MINUS_Q2, M_MI_NU2QX, M_MI_NU2QY, M_MINUS_Q2A, M_I_ANU,
+    M_PHI_IQXQ2, M_PHI_IQYQ2, M_PHI_Q4};
+static const int E44_PAIR_MULT[16] = {M_ONE, M_NU, M_NU2, M_NU3, M_NU4, M_QX_SNU, M_QY_SNU, M_QX,
+                                      M_QY, M_Q2_SNU, M_Q2, M_Q2NU, M_NUQX, M_NUQY, M_NU2QX, M_NU2QY};
+// pair outputs from (es, ets, ps, pts, ptts) = sources 0..4
+static const int E44_POUT_MULT[18] = {M_ONE, M_IQX, M_IQY, M_ONE, M_IQX, M_IQY, M_IQX, M_IQY, M_A,
+                                      M_Q2, M_A, M_IQX, M_IQY, M_Q2, M_A, M_IQXA, M_IQYA, M_Q2A};
+static const int E44_POUT_SRC[18] = {0, 0, 0, 1, 1, 1, 2, 2, 2, 2, 3, 3, 3, 3, 4, 2, 2, 2};
+// third outputs from (es, ps, pts) = sources 0..2
+static const int E44_TOUT_MULT[8] = {M_ONE, M_IQX, M_IQY, M_IQX, M_IQY, M_A, M_Q2, M_A};
+static const int E44_TOUT_SRC[8] = {0, 0, 0, 1, 1, 1, 1, 2};
+
+struct E44Layout {
+  size_t E, maxE, T, maxT, OUT, maxOUT, transient;
+  size_t total;
+};
+
+static E44Layout e44_layout(const gl_plan* p, int g) {
+  const size_t c = sizeof(cplx), R = p->R44, ncy = p->ncy;
+  const size_t b2 = (size_t)p->b2.w * p->b2.h, b3 = (size_t)p->b3.w * p->b3.h,
+               b4 = (size_t)p->b4.w * p->b4.h;
+  const size_t JP = R * R * R + R * R, GP = R * R + R;
+  E44Layout L;
+  Bump b;
+  L.E = b.take(g * GP * 5 * b2 * c);
+  L.maxE = b.take(g * GP * 5 * 8);
+  L.T = b.take(g * R * 3 * b3 * c);
+  L.maxT = b.take(g * R * 3 * 8);
+  L.OUT = b.take(g * b4 * c);
+  L.maxOUT = b.take(g * 8);
+  L.transient = b.off;
+  size_t need = 0;
+  {  // pair stage
+    Bump t;
+    t.take(g * JP * 16 * p->b1.w * ncy * c);
+    t.take(g * JP * 6 * p->b2.w * ncy * c);
+    t.take(g * JP * 6 * b2 * c);
+    t.take(g * JP * 6 * 8);
+    need = std::max(need, t.off);
+  }
+  {  // third stage
+    Bump t;
+    t.take(g * R * R * 16 * p->b1.w * ncy * c);
+    t.take(g * R * R * 15 * p->b2.w * ncy * c);
+    t.take(g * R * R * 4 * p->b3.w * ncy * c);
+    t.take(g * R * R * 4 * b3 * c);
+    t.take(g * R * R * 4 * 8);
+    need = std::max(need, t.off);
+  }
+  {  // order-4 stage
+    Bump t;
+    t.take(g * R * 19 * p->b1.w * ncy * c);
+    t.take(g * R * 18 * p->b2.w * ncy * c);
+    t.take(g * R * 8 * p->b3.w * ncy * c);
+    t.take(g * R * 2 * p->b4.w * ncy * c);
+    t.take(g * R * 2 * b4 * c);
+    t.take(g * R * 2 * 8);
+    need = std::max(need, t.off);
+  }
+  need = std::max(need, (size_t)g * p->b4.w * p->d.ny * c);  // final column transforms
+  L.total = L.transient + need;
+  return L;
+}
+
+extern "C" gl_status gl_eta44_plan_create(gl_plan** out, const gl_eta44_desc* desc) {
+  if (!out || !desc) return fail(GL_ERR_INVALID_ARGUMENT, "null plan or descriptor");
+  *out = nullptr;
+  const gl_eta44_desc& e = *desc;
+  if (!is_pow2(e.n) || e.n < 16 || e.n > TW_N)
+    return fail(GL_ERR_UNSUPPORTED, "the GPU engine runs power-of-two grids from 16 to %d (got %d)", TW_N, e.n);
+  if (!(e.dk > 0) || !(e.depth > 0) || !(e.peak_depth > 0))
+    return fail(GL_ERR_INVALID_ARGUMENT, "dk, depth and peak_depth must be positive");
+  if (e.rank < 1 || e.rank > MAX_RANK) return fail(GL_ERR_RANK, "rank must be an integer from 1 to %d", MAX_RANK);
+  if (e.max_units < 1) return fail(GL_ERR_INVALID_ARGUMENT, "max_units must be >= 1");
+  if (e.output != GL_OUT_COMPLEX && e.output != GL_OUT_REAL)
+    return fail(GL_ERR_INVALID_ARGUMENT, "unknown output mode");
+  if (e.box_w < 1 || e.box_h < 1) return fail(GL_ERR_INVALID_ARGUMENT, "empty parent box");
+  if (e.box_x0 < 1) return fail(GL_ERR_SUPPORT, "strict-forward nonzero analytic eta1 support is required");
+  const int xmax = e.box_x0 + e.box_w - 1;
+  const int ymax = std::max(std::abs(e.box_y0), std::abs(e.box_y0 + e.box_h - 1));
+  if (4 * xmax >= e.n / 2 || 4 * ymax >= e.n / 2)
+    return fail(GL_ERR_ALIAS, "quartic output support reaches a Nyquist boundary");
+  gl_plan* p = new gl_plan();
+  std::memset(&p->d, 0, sizeof p->d);
+  p->d.nx = p->d.ny = e.n;
+  p->d.lx = p->d.ly = 6.283185307179586 / e.dk;
+  p->d.depth = e.depth;
+  p->d.gravity = 1.0;
+  p->d.order = 4;
+  p->d.max_units = e.max_units;
+  p->d.output = e.output;
+  p->d.box_x0 = e.box_x0;
+  p->d.box_y0 = e.box_y0;
+  p->d.box_w = e.box_w;
+  p->d.box_h = e.box_h;
+  p->e44 = true;
+  p->R44 = e.rank;
+  p->dk44 = e.dk;
+  p->peak44 = e.peak_depth;
+  p->comps = 0;
+  p->ncomp = 1;
+  p->comp_ids[0] = GL_COMP_ETA44;
+  p->b1 = Box{e.box_x0, e.box_y0, e.box_w, e.box_h};
+  p->b2 = Box{2 * e.box_x0, 2 * e.box_y0, 2 * (e.box_w - 1) + 1, 2 * (e.box_h - 1) + 1};
+  p->b3 = Box{3 * e.box_x0, 3 * e.box_y0, 3 * (e.box_w - 1) + 1, 3 * (e.box_h - 1) + 1};
+  p->b4 = Box{4 * e.box_x0, 4 * e.box_y0, 4 * (e.box_w - 1) + 1, 4 * (e.box_h - 1) + 1};
+  p->ww1 = (p->b1.w + 63) / 64;
+  p->ww2 = (p->b2.w + 63) / 64;
+  p->ww3 = (p->b3.w + 63) / 64;
+  p->ncx = std::min(e.n, std::max(16, next_pow2(p->b4.w)));
+  p->ncy = std::min(e.n, std::max(16, next_pow2(p->b4.h)));
+  p->lncx = ilog2(p->ncx);
+  p->lncy = ilog2(p->ncy);
+  p->lnx = p->lny = ilog2(e.n);
+  if (row_smem(45, p->ncx) > SMEM_LIMIT) {
+    plan_free(p);
+    return fail(GL_ERR_UNSUPPORTED,
+                "eta44 product grid width %d exceeds the shared-memory row budget (45 banks)", p->ncx);
+  }
+  p->floor_rel = 16.0 * 2.220446049250313e-16 * std::max(1.0, std::log2((double)e.n * (double)e.n));
+  if (e.nodes && e.weights) {
+    for (int k = 0; k < e.rank; ++k) {
+      p->h_nodes[0][k] = e.nodes[k];
+      p->h_weights[0][k] = e.weights[k];
+    }
+  } else {
+    gl_status st = gauss_laguerre(e.rank, p->h_nodes[0], p->h_weights[0]);
+    if (st != GL_OK) {
+      plan_free(p);
+      return st;
+    }
+  }
+  p->h_comp_scale[0] = e.depth;
+  cudaError_t err = cudaSuccess;
+  auto geo_alloc = [&](double** g, const Box& b) {
+    if (err == cudaSuccess) err = cudaMalloc(g, sizeof(double) * 6 * b.w * b.h);
+    if (err == cudaSuccess) {
+      const int plane = b.w * b.h;
+      geo_kernel<<<std::min(1024, (plane + 255) / 256), 256>>>(*g, b, e.n, e.n, p->d.lx, p->d.ly, e.depth, e.dk);
+      err = cudaGetLastError();
+    }
+  };
+  geo_alloc(&p->geo1, p->b1);
+  geo_alloc(&p->geo2, p->b2);
+  geo_alloc(&p->geo3, p->b3);
+  geo_alloc(&p->geo4, p->b4);
+  if (err == cudaSuccess) err = cudaMalloc(&p->tw, sizeof(cplx) * TW_N);
+  if (err == cudaSuccess) {
+    twiddle_kernel<<<TW_N / 256, 256>>>(p->tw);
+    err = cudaGetLastError();
+  }
+  if (err == cudaSuccess) err = cudaMalloc(&p->nodes, sizeof(double) * 2 * MAX_RANK);
+  if (err == cudaSuccess) {
+    double host[2 * MAX_RANK] = {0};
+    std::memcpy(host, p->h_nodes[0], sizeof(double) * MAX_RANK);
+    std::memcpy(host + MAX_RANK, p->h_weights[0], sizeof(double) * MAX_RANK);
+    err = cudaMemcpy(p->nodes, host, sizeof host, cudaMemcpyHostToDevice);
+  }
+  if (err == cudaSuccess) err = cudaMalloc(&p->comp_scale, sizeof(double) * 6);
+  if (err == cudaSuccess) err = cudaMemcpy(p->comp_scale, p->h_comp_scale, sizeof(double) * 6, cudaMemcpyHostToDevice);
+  if (err == cudaSuccess) err = cudaDeviceSynchronize();
+  if (err != cudaSuccess) {
+    plan_free(p);
+    return fail(GL_ERR_CUDA, "eta44 plan set-up failed: %s", cudaGetErrorString(err));
+  }
+  const int g = e.max_units;
+  p->group = g;
+  const size_t c = sizeof(cplx);
+  const size_t b1 = (size_t)p->b1.w * p->b1.h, b2 = (size_t)p->b2.w * p->b2.h,
+               b3 = (size_t)p->b3.w * p->b3.h, b4 = (size_t)p->b4.w * p->b4.h;
+  Bump b;
+  p->o_slots = b.take(g * sizeof(UnitSlots));
+  p->o_us = b.take(g * sizeof(UnitScalars));
+  p->o_box = b.take(g * b1 * c);
+  p->o_s1 = b.take(g * b1);
+  p->o_s1f = b.take((size_t)g * p->b1.h * p->ww1 * 8);
+  p->o_s1r = b.take((size_t)g * p->b1.h * p->ww1 * 8);
+  p->o_s2 = b.take(g * b2);
+  p->o_s2f = b.take((size_t)g * p->b2.h * p->ww2 * 8);
+  p->o_s2r = b.take((size_t)g * p->b2.h * p->ww2 * 8);
+  p->o_s3 = b.take(g * b3);
+  p->o_s3f = b.take((size_t)g * p->b3.h * p->ww3 * 8);
+  p->o_s3r = b.take((size_t)g * p->b3.h * p->ww3 * 8);
+  p->o_s4 = b.take(g * b4);
+  const E44Layout L = e44_layout(p, g);
+  p->o_e44 = b.take(L.total);
+  p->ws_total = b.off;
+  *out = p;
+  return GL_OK;
+}
+
+static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int layout,
+                                 void* outputs, void* ws, int* status, cudaStream_t st) {
+  const int T = 256, R = p->R44;
+  const Box B1 = p->b1, B2 = p->b2, B3 = p->b3, B4 = p->b4;
+  const int pl1 = B1.w * B1.h, pl2 = B2.w * B2.h, pl3 = B3.w * B3.h, pl4 = B4.w * B4.h;
+  UnitSlots* slots = at<UnitSlots>(ws, p->o_slots);
+  UnitScalars* us = at<UnitScalars>(ws, p->o_us);
+  cplx* boxv = at<cplx>(ws, p->o_box);
+  unsigned char* s1 = at<unsigned char>(ws, p->o_s1);
+  unsigned long long* s1f = at<unsigned long long>(ws, p->o_s1f);
+  unsigned long long* s1r = at<unsigned long long>(ws, p->o_s1r);
+  unsigned char* s2 = at<unsigned char>(ws, p->o_s2);
+  unsigned long long* s2f = at<unsigned long long>(ws, p->o_s2f);
+  unsigned long long* s2r = at<unsigned long long>(ws, p->o_s2r);
+  unsigned char* s3 = at<unsigned char>(ws, p->o_s3);
+  unsigned long long* s3f = at<unsigned long long>(ws, p->o_s3f);
+  unsigned long long* s3r = at<unsigned long long>(ws, p->o_s3r);
+  unsigned char* s4 = at<unsigned char>(ws, p->o_s4);
+  char* e44 = at<char>(ws, p->o_e44);
+  const E44Layout L = e44_layout(p, p->group);
+  cplx* E = reinterpret_cast<cplx*>(e44 + L.E);
+  unsigned long long* maxE = reinterpret_cast<unsigned long long*>(e44 + L.maxE);
+  cplx* TS = reinterpret_cast<cplx*>(e44 + L.T);
+  unsigned long long* maxT = reinterpret_cast<unsigned long long*>(e44 + L.maxT);
+  cplx* OUT = reinterpret_cast<cplx*>(e44 + L.OUT);
+  unsigned long long* maxOUT = reinterpret_cast<unsigned long long*>(e44 + L.maxOUT);
+  char* tr = e44 + L.transient;
+  const double* dn = p->nodes;  // nodes, then weights at +MAX_RANK
+  gl_status s;
+
+  // ---- analysis: support, S2..S4, shifts, scales
+  {
+    LaunchScope ls_("slots_init_kernel", st, 0.0);
+    slots_init_kernel<<<(gu + 63) / 64, 64, 0, st>>>(slots, gu);
+  }
+  LAUNCH_CHECK("slots_init_kernel");
+  const cplx* spec = boxv;
+  if (layout == GL_SPECTRA_FULL) {
+    CUDA_TRY(cudaMemsetAsync(boxv, 0, sizeof(cplx) * (size_t)gu * pl1, st));
+    dim3 g(grid_for((size_t)p->d.nx * p->d.ny, T, 1024), gu);
+    {
+      LaunchScope ls_("extract_kernel", st, 0.0);
+      extract_kernel<<<g, T, 0, st>>>(reinterpret_cast<const cplx*>(spectra), boxv, B1, p->d.nx, p->d.ny, slots);
+    }
+    LAUNCH_CHECK("extract_kernel");
+  } else {
+    spec = reinterpret_cast<const cplx*>(spectra);
+    dim3 g(grid_for(pl1, T, 64), gu);
+    {
+      LaunchScope ls_("box_max_kernel", st, 0.0);
+      box_max_kernel<<<g, T, 0, st>>>(spec, pl1, slots);
+    }
+    LAUNCH_CHECK("box_max_kernel");
+  }
+  {
+    dim3 g(grid_for(pl1, T, 64), gu);
+    {
+      LaunchScope ls_("support_kernel", st, 0.0);
+      support_kernel<<<g, T, 0, st>>>(spec, p->geo1, B1, slots, s1);
+    }
+    LAUNCH_CHECK("support_kernel");
+    {
+      LaunchScope ls_("peak_kernel", st, 0.0);
+      peak_kernel<<<g, T, 0, st>>>(spec, p->geo1, B1, p->d.nx, p->d.ny, slots, s1, nullptr, 0);
+    }
+    LAUNCH_CHECK("peak_kernel");
+    dim3 gb(grid_for(B1.h * p->ww1, T, 64), gu);
+    {
+      LaunchScope ls_("bitrows_kernel", st, 0.0);
+      bitrows_kernel<<<gb, T, 0, st>>>(s1, B1.h, B1.w, p->ww1, s1f, s1r);
+    }
+    LAUNCH_CHECK("bitrows_kernel");
+  }
+  {
+    MinkArgs m;
+    mink_args(m, s1f, B1.h, B1.w, p->ww1, s1r, B1.h, B1.w, p->ww1, s2, p->geo2, slots, 2);
+    dim3 g2(grid_for(pl2, T, 256), gu);
+    {
+      LaunchScope ls_("minkowski_kernel", st, 0.0);
+      minkowski_kernel<<<g2, T, 0, st>>>(m);
+    }
+    LAUNCH_CHECK("minkowski_kernel");
+    dim3 gb(grid_for(B2.h * p->ww2, T, 64), gu);
+    {
+      LaunchScope ls_("bitrows_kernel", st, 0.0);
+      bitrows_kernel<<<gb, T, 0, st>>>(s2, B2.h, B2.w, p->ww2, s2f, s2r);
+    }
+    LAUNCH_CHECK("bitrows_kernel");
+    mink_args(m, s2f, B2.h, B2.w, p->ww2, s1r, B1.h, B1.w, p->ww1, s3, p->geo3, slots, 3);
+    dim3 g3(grid_for(pl3, T, 512), gu);
+    {
+      LaunchScope ls_("minkowski_kernel", st, 0.0);
+      minkowski_kernel<<<g3, T, 0, st>>>(m);
+    }
+    LAUNCH_CHECK("minkowski_kernel");
+    dim3 gb3(grid_for(B3.h * p->ww3, T, 64), gu);
+    {
+      LaunchScope ls_("bitrows_kernel", st, 0.0);
+      bitrows_kernel<<<gb3, T, 0, st>>>(s3, B3.h, B3.w, p->ww3, s3f, s3r);
+    }
+    LAUNCH_CHECK("bitrows_kernel");
+    mink_args(m, s3f, B3.h, B3.w, p->ww3, s1r, B1.h, B1.w, p->ww1, s4, p->geo4, slots, 4);
+    dim3 g4(grid_for(pl4, T, 512), gu);
+    {
+      LaunchScope ls_("minkowski_kernel", st, 0.0);
+      minkowski_kernel<<<g4, T, 0, st>>>(m);
+    }
+    LAUNCH_CHECK("minkowski_kernel");
+  }
+  {
+    ScalarArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.slots = slots;
+    a.us = us;
+    a.geo1 = p->geo1;
+    a.box = B1;
+    a.nx = p->d.nx;
+    a.ny = p->d.ny;
+    a.order = 4;
+    a.full_input = layout == GL_SPECTRA_FULL;
+    a.want_e44 = 1;
+    a.fixed_peak = p->peak44;
+    {
+      LaunchScope ls_("scalars_kernel", st, 0.0);
+      scalars_kernel<<<(gu + 63) / 64, 64, 0, st>>>(a, gu);
+    }
+    LAUNCH_CHECK("scalars_kernel");
+  }
+  const double fwd_scale = ((double)p->d.nx * (double)p->d.ny) / ((double)p->ncx * (double)p->ncy);
+  const double inv_scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
+  const int ncy = p->ncy;
+  const int JP = R * R * R + R * R, GP = R * R + R;
+  CUDA_TRY(cudaMemsetAsync(maxE, 0, (size_t)gu * GP * 5 * 8, st));
+  CUDA_TRY(cudaMemsetAsync(maxT, 0, (size_t)gu * R * 3 * 8, st));
+  CUDA_TRY(cudaMemsetAsync(maxOUT, 0, (size_t)gu * 8, st));
+
+  auto colargs = [&](int kind, int nb, const int* mults, const int* srcs, const Box& box,
+                     const double* geo, const cplx* sp, long long job_stride, long long sub_stride,
+                     int jobs_per_unit, cplx* outp) {
+    ColArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.kind = kind;
+    a.nbanks = nb;
+    for (int k = 0; k < nb; ++k) {
+      a.mult[k] = mults[k];
+      a.src_of[k] = srcs ? srcs[k] : 0;
+    }
+    a.box = box;
+    a.geo = geo;
+    a.spec = sp;
+    a.spec_job_stride = job_stride;
+    a.spec_sub_stride = sub_stride;
+    a.jobs_per_unit = jobs_per_unit;
+    a.us = us;
+    a.nodes = dn;
+    a.n_inner = R;
+    a.floor_rel = p->floor_rel;
+    a.out = outp;
+    a.n = ncy;
+    a.log2n = p->lncy;
+    a.scale = inv_scale;
+    return a;
+  };
+  auto rowargs = [&](int kind, int nout, const Box& outbox, cplx* outp) {
+    RowArgs r;
+    std::memset(&r, 0, sizeof r);
+    r.kind = kind;
+    r.nout = nout;
+    r.out_x0 = outbox.x0;
+    r.out_w = outbox.w;
+    r.out = outp;
+    r.nx = p->ncx;
+    r.log2nx = p->lncx;
+    r.ny = ncy;
+    r.us = us;
+    r.jobs_per_unit = 1;
+    r.gmax = ROW_GMAX;
+    return r;
+  };
+  auto colfft = [&](const cplx* in, cplx* outp, const Box& box, int nsrc, const unsigned char* mask,
+                    unsigned long long* mx, int jobs_per_unit, int njs) {
+    ColFftArgs f;
+    f.in = in;
+    f.out = outp;
+    f.box = box;
+    f.n = ncy;
+    f.log2n = p->lncy;
+    f.nsrc = nsrc;
+    f.jobs_per_unit = jobs_per_unit;
+    f.mask = mask;
+    f.maxslot = mx;
+    f.scale = fwd_scale;
+    return launch_col_fft(f, njs, st, p->tw);
+  };
+
+  // ---- stage 1: every pair level (R^3 third-level + R^2 order-4 pair jobs)
+  {
+    const int nj = gu * JP;
+    Bump b;
+    cplx* P = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 16 * B1.w * ncy * sizeof(cplx)));
+    cplx* Q = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 6 * B2.w * ncy * sizeof(cplx)));
+    cplx* RP = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 6 * pl2 * sizeof(cplx)));
+    unsigned long long* mRP = reinterpret_cast<unsigned long long*>(tr + b.take((size_t)nj * 6 * 8));
+    CUDA_TRY(cudaMemsetAsync(mRP, 0, (size_t)nj * 6 * 8, st));
+    ColArgs a = colargs(COL_E44_PAIR, 16, E44_PAIR_MULT, nullptr, B1, p->geo1, spec, pl1, 0, JP, P);
+    if ((s = launch_col_ifft(a, nj, st, p->tw)) != GL_OK) return s;
+    RowArgs r = rowargs(ROW_E44_PAIR, 6, B2, Q);
+    r.grp[0] = BankGroup{P, 16, B1.x0, B1.w};
+    r.ngrp = 1;
+    if ((s = launch_row(r, nj, st, p->tw)) != GL_OK) return s;
+    if ((s = colfft(Q, RP, B2, 6, s2, mRP, JP, nj * 6)) != GL_OK) return s;
+    E44Acc c;
+    std::memset(&c, 0, sizeof c);
+    c.us = us;
+    c.geo = p->geo2;
+    c.box = B2;
+    c.in = RP;
+    c.maxin = mRP;
+    c.out = E;
+    c.maxout = maxE;
+    c.nodes = dn;
+    c.weights = dn + MAX_RANK;
+    c.R = R;
+    c.groups_per_unit = GP;
+    c.floor_rel = p->floor_rel;
+    dim3 g(grid_for(pl2, T, 64), gu * GP);
+    {
+      LaunchScope ls_("acc_e44_pair_kernel", st, 0.0);
+      acc_e44_pair_kernel<<<g, T, 0, st>>>(c);
+    }
+    LAUNCH_CHECK("acc_e44_pair_kernel");
+  }
+  // ---- stage 2: third level (R^2 jobs per unit)
+  {
+    const int nj = gu * R * R;
+    Bump b;
+    cplx* PF = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 16 * B1.w * ncy * sizeof(cplx)));
+    cplx* PP = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 15 * B2.w * ncy * sizeof(cplx)));
+    cplx* Q = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 4 * B3.w * ncy * sizeof(cplx)));
+    cplx* R3 = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 4 * pl3 * sizeof(cplx)));
+    unsigned long long* mR3 = reinterpret_cast<unsigned long long*>(tr + b.take((size_t)nj * 4 * 8));
+    CUDA_TRY(cudaMemsetAsync(mR3, 0, (size_t)nj * 4 * 8, st));
+    ColArgs a = colargs(COL_E44_FIRST3, 16, E44_FIRST_MULT, nullptr, B1, p->geo1, spec, pl1, 0, R * R, PF);
+    if ((s = launch_col_ifft(a, nj, st, p->tw)) != GL_OK) return s;
+    // pair outputs of third-level groups: group g = o R + t of unit u sits at E[u GP + g]
+    // and job (u, o, t) = u R^2 + o R + t, so job -> group index u GP + (job mod R^2).
+    for (int u = 0; u < gu; ++u) {
+      ColArgs a2 = colargs(COL_FLOORED, 15, E44_POUT_MULT, E44_POUT_SRC, B2, p->geo2,
+                           E + (size_t)u * GP * 5 * pl2, 5LL * pl2, pl2, R * R,
+                           PP + (size_t)u * R * R * 15 * B2.w * ncy);
+      a2.floor_max = maxE + (size_t)u * GP * 5;
+      a2.floor_nsrc = 5;
+      if ((s = launch_col_ifft(a2, R * R, st, p->tw)) != GL_OK) return s;
+    }
+    RowArgs r = rowargs(ROW_E44_THIRD, 4, B3, Q);
+    r.grp[0] = BankGroup{PF, 16, B1.x0, B1.w};
+    r.grp[1] = BankGroup{PP, 15, B2.x0, B2.w};
+    r.ngrp = 2;
+    if ((s = launch_row(r, nj, st, p->tw)) != GL_OK) return s;
+    if ((s = colfft(Q, R3, B3, 4, s3, mR3, R * R, nj * 4)) != GL_OK) return s;
+    E44Acc c;
+    std::memset(&c, 0, sizeof c);
+    c.us = us;
+    c.geo = p->geo3;
+    c.box = B3;
+    c.in = R3;
+    c.maxin = mR3;
+    c.out = TS;
+    c.maxout = maxT;
+    c.nodes = dn;
+    c.weights = dn + MAX_RANK;
+    c.R = R;
+    c.groups_per_unit = R;
+    c.floor_rel = p->floor_rel;
+    dim3 g(grid_for(pl3, T, 64), gu * R);
+    {
+      LaunchScope ls_("acc_e44_third_kernel", st, 0.0);
+      acc_e44_third_kernel<<<g, T, 0, st>>>(c);
+    }
+    LAUNCH_CHECK("acc_e44_third_kernel");
+  }
+  // ---- stage 3: order-4 forcing (R jobs per unit)
+  {
+    const int nj = gu * R;
+    Bump b;
+    cplx* PF = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 19 * B1.w * ncy * sizeof(cplx)));
+    cplx* PP = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 18 * B2.w * ncy * sizeof(cplx)));
+    cplx* PT = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 8 * B3.w * ncy * sizeof(cplx)));
+    cplx* Q = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 2 * B4.w * ncy * sizeof(cplx)));
+    cplx* R4 = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 2 * pl4 * sizeof(cplx)));
+    unsigned long long* mR4 = reinterpret_cast<unsigned long long*>(tr + b.take((size_t)nj * 2 * 8));
+    CUDA_TRY(cudaMemsetAsync(mR4, 0, (size_t)nj * 2 * 8, st));
+    ColArgs a = colargs(COL_E44_FIRST4, 19, E44_FIRST_MULT, nullptr, B1, p->geo1, spec, pl1, 0, R, PF);
+    if ((s = launch_col_ifft(a, nj, st, p->tw)) != GL_OK) return s;
+    for (int u = 0; u < gu; ++u) {
+      ColArgs a2 = colargs(COL_FLOORED, 18, E44_POUT_MULT, E44_POUT_SRC, B2, p->geo2,
+                           E + ((size_t)u * GP + R * R) * 5 * pl2, 5LL * pl2, pl2, R,
+                           PP + (size_t)u * R * 18 * B2.w * ncy);
+      a2.floor_max = maxE + ((size_t)u * GP + R * R) * 5;
+      a2.floor_nsrc = 5;
+      if ((s = launch_col_ifft(a2, R, st, p->tw)) != GL_OK) return s;
+    }
+    ColArgs a3 = colargs(COL_FLOORED, 8, E44_TOUT_MULT, E44_TOUT_SRC, B3, p->geo3, TS, 3LL * pl3, pl3,
+                         R, PT);
+    a3.floor_max = maxT;
+    a3.floor_nsrc = 3;
+    if ((s = launch_col_ifft(a3, nj, st, p->tw)) != GL_OK) return s;
+    RowArgs r = rowargs(ROW_E44_ORDER4, 2, B4, Q);
+    r.grp[0] = BankGroup{PF, 19, B1.x0, B1.w};
+    r.grp[1] = BankGroup{PP, 18, B2.x0, B2.w};
+    r.grp[2] = BankGroup{PT, 8, B3.x0, B3.w};
+    r.ngrp = 3;
+    if ((s = launch_row(r, nj, st, p->tw)) != GL_OK) return s;
+    if ((s = colfft(Q, R4, B4, 2, s4, mR4, R, nj * 2)) != GL_OK) return s;
+    E44Acc c;
+    std::memset(&c, 0, sizeof c);
+    c.us = us;
+    c.geo = p->geo4;
+    c.box = B4;
+    c.in = R4;
+    c.maxin = mR4;
+    c.out = OUT;
+    c.maxout = maxOUT;
+    c.nodes = dn;
+    c.weights = dn + MAX_RANK;
+    c.R = R;
+    c.groups_per_unit = 1;
+    c.floor_rel = p->floor_rel;
+    dim3 g(grid_for(pl4, T, 64), gu);
+    {
+      LaunchScope ls_("acc_e44_order4_kernel", st, 0.0);
+      acc_e44_order4_kernel<<<g, T, 0, st>>>(c);
+    }
+    LAUNCH_CHECK("acc_e44_order4_kernel");
+  }
+  // ---- final transform on the reference grid, with the last roundoff floor
+  {
+    const int m1[1] = {M_ONE}, z1[1] = {0};
+    ColArgs a = colargs(COL_FLOORED, 1, m1, z1, B4, p->geo4, OUT, pl4, 0, 1, reinterpret_cast<cplx*>(tr));
+    a.floor_max = maxOUT;
+    a.floor_nsrc = 1;
+    a.n = p->d.ny;
+    a.log2n = p->lny;
+    if ((s = launch_col_ifft(a, gu, st, p->tw)) != GL_OK) return s;
+    OutArgs o;
+    std::memset(&o, 0, sizeof o);
+    o.in = reinterpret_cast<cplx*>(tr);
+    o.w = B4.w;
+    o.x0 = B4.x0;
+    o.nx = p->d.nx;
+    o.log2nx = p->lnx;
+    o.ny = p->d.ny;
+    o.ncomp = 1;
+    o.comp_offset = 0;
+    o.out_ncomp = 1;
+    o.comp_scale = p->comp_scale;
+    o.out = outputs;
+    o.real_only = p->d.output == GL_OUT_REAL;
+    if ((s = launch_out_rows(o, gu, st, p->tw)) != GL_OK) return s;
+  }
+  {
+    const size_t per_unit = (size_t)p->d.nx * p->d.ny;
     dim3 g(grid_for(per_unit, T, 256), gu);
     {
       LaunchScope ls_("nonfinite_kernel", st, 0.0);

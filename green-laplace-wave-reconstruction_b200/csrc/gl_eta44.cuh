@@ -1,0 +1,151 @@
+// Accumulation kernels of the fourth-order GL eta44 graph
+// (paper/order4/cpp/gl_eta44_fftw.cpp).  One GL rule of rank R serves the
+// three nested levels: outer4 node o, third node t, pair node p.
+//
+// Job numbering per unit:
+//   pair jobs      (o, t, p) -> (o R + t) R + p            for third-level pairs,
+//                  (o, p)    -> R^3 + o R + p              for order-4 pairs;
+//   pair groups    g = o R + t (third) or R^2 + o (order 4); group g's
+//                  jobs are g R + p, p = 0..R-1;
+//   third jobs     (o, t) -> o R + t;   outer jobs o.
+#pragma once
+#include "gl_kernels.cuh"
+
+namespace gl {
+
+struct E44Acc {
+  const UnitScalars* us;
+  const double* geo;        // geometry planes of the output box
+  Box box;
+  const cplx* in;
+  const unsigned long long* maxin;
+  cplx* out;
+  unsigned long long* maxout;
+  const double* nodes;
+  const double* weights;
+  int R;
+  int groups_per_unit;      // pair stage: R^2 + R; third stage: R
+  double floor_rel;
+};
+
+GL_D void e44_max_reduce(double* v, int n, unsigned long long* slots) {
+  for (int k = 0; k < n; ++k) {
+    double l = v[k];
+    for (int o = 16; o > 0; o >>= 1) {
+      const double other = __shfl_xor_sync(0xffffffffu, l, o);
+      l = (other > l || other != other) ? other : l;
+    }
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(slots + k, l);
+  }
+}
+
+GL_D double e44_keep_max(double cur, cplx v) {
+  const double m = cabs_(v);
+  return (m > cur || m != m) ? m : cur;
+}
+
+// Pair level: the five pair spectra of one group (gl_eta44_fftw.cpp:383-402).
+__global__ void acc_e44_pair_kernel(E44Acc a) {
+  const int grp = blockIdx.y;                 // unit * groups + g
+  const int unit = grp / a.groups_per_unit;
+  const int g = grp % a.groups_per_unit;
+  const int R = a.R;
+  const int jobs_per_unit = R * R * R + R * R;
+  const int plane = a.box.w * a.box.h;
+  const UnitScalars& u = a.us[unit];
+  double lm[5] = {0, 0, 0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
+    const GeoRef G{a.geo, plane, i};
+    const double A = G.a(), sqa = __ldg(a.geo + 5 * plane + i);
+    cplx es = czero(), ets = czero(), ps = czero(), pts = czero(), ptts = czero();
+    for (int p = 0; p < R; ++p) {
+      const int job = unit * jobs_per_unit + g * R + p;
+      const double x = a.nodes[p], w = a.weights[p];
+      const double t = x / u.lam2;
+      const double co = w * exp(x) / u.lam2 * exp(-2.0 * u.shift2 * t) / 4.0;
+      const double sh = sinh_over_root(sqa, t), ch = cosh(sqa * t);
+      const cplx* src = a.in + (size_t)job * 6 * plane;
+      cplx s[6];
+      for (int k = 0; k < 6; ++k) s[k] = floored(src[(size_t)k * plane + i], a.floor_rel, a.maxin[job * 6 + k]);
+      const double mash = -A * sh;
+      es = cadd(es, cscale(co, cadd(cscale(mash, s[0]), cscale(ch, s[1]))));
+      ets = csub(ets, cmul(cmk(0.0, co), cadd(cscale(mash, s[2]), cscale(ch, s[3]))));
+      ps = cadd(ps, cmul(cmk(0.0, co), csub(cscale(ch, s[0]), cscale(sh, s[1]))));
+      pts = cadd(pts, cscale(co, csub(cscale(ch, s[2]), cscale(sh, s[3]))));
+      ptts = csub(ptts, cmul(cmk(0.0, co), csub(cscale(ch, s[4]), cscale(sh, s[5]))));
+    }
+    cplx* dst = a.out + (size_t)grp * 5 * plane;
+    const cplx r[5] = {es, ets, ps, pts, ptts};
+    for (int k = 0; k < 5; ++k) {
+      dst[(size_t)k * plane + i] = r[k];
+      lm[k] = e44_keep_max(lm[k], r[k]);
+    }
+  }
+  e44_max_reduce(lm, 5, a.maxout + (size_t)grp * 5);
+}
+
+// Third level: es, ps, pts of one outer node (gl_eta44_fftw.cpp:571-584).
+__global__ void acc_e44_third_kernel(E44Acc a) {
+  const int uo = blockIdx.y;  // unit * R + o
+  const int unit = uo / a.R;
+  const int R = a.R;
+  const int plane = a.box.w * a.box.h;
+  const UnitScalars& u = a.us[unit];
+  double lm[3] = {0, 0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
+    const GeoRef G{a.geo, plane, i};
+    const double A = G.a(), sqa = __ldg(a.geo + 5 * plane + i);
+    cplx es = czero(), ps = czero(), pts = czero();
+    for (int t = 0; t < R; ++t) {
+      const int job = uo * R + t;
+      const double x = a.nodes[t], w = a.weights[t];
+      const double tt = x / u.lam3;
+      const double co = w * exp(x) / u.lam3 * exp(-3.0 * u.shift3 * tt);
+      const double sh = sinh_over_root(sqa, tt), ch = cosh(sqa * tt);
+      const cplx* src = a.in + (size_t)job * 4 * plane;
+      cplx s[4];
+      for (int k = 0; k < 4; ++k) s[k] = floored(src[(size_t)k * plane + i], a.floor_rel, a.maxin[job * 4 + k]);
+      // s = fk, fd, fkt, fdt
+      es = cadd(es, cscale(co, csub(cscale(A * sh, s[1]), cmul(cmk(0.0, ch), s[0]))));
+      ps = cadd(ps, cscale(co, csub(cmul(cmk(0.0, -ch), s[1]), cscale(sh, s[0]))));
+      pts = cadd(pts, cscale(co, csub(cmul(cmk(0.0, -ch), s[3]), cscale(sh, s[2]))));
+    }
+    cplx* dst = a.out + (size_t)uo * 3 * plane;
+    const cplx r[3] = {es, ps, pts};
+    for (int k = 0; k < 3; ++k) {
+      dst[(size_t)k * plane + i] = r[k];
+      lm[k] = e44_keep_max(lm[k], r[k]);
+    }
+  }
+  e44_max_reduce(lm, 3, a.maxout + (size_t)uo * 3);
+}
+
+// Order 4: the eta44 spectrum of one unit (gl_eta44_fftw.cpp:736-748).
+__global__ void acc_e44_order4_kernel(E44Acc a) {
+  const int unit = blockIdx.y;
+  const int R = a.R;
+  const int plane = a.box.w * a.box.h;
+  const UnitScalars& u = a.us[unit];
+  double lm[1] = {0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
+    const GeoRef G{a.geo, plane, i};
+    const double A = G.a(), sqa = __ldg(a.geo + 5 * plane + i);
+    cplx acc = czero();
+    for (int o = 0; o < R; ++o) {
+      const int job = unit * R + o;
+      const double x = a.nodes[o], w = a.weights[o];
+      const double tm = x / u.lam4;
+      const double co = w * exp(x) / u.lam4 * exp(-4.0 * u.shift4 * tm);
+      const double sh = sinh_over_root(sqa, tm), ch = cosh(sqa * tm);
+      const cplx* src = a.in + (size_t)job * 2 * plane;
+      const cplx fk = floored(src[i], a.floor_rel, a.maxin[job * 2 + 0]);
+      const cplx fd = floored(src[plane + i], a.floor_rel, a.maxin[job * 2 + 1]);
+      acc = cadd(acc, cscale(co, csub(cscale(A * sh, fd), cmul(cmk(0.0, ch), fk))));
+    }
+    a.out[(size_t)unit * plane + i] = acc;
+    lm[0] = e44_keep_max(lm[0], acc);
+  }
+  e44_max_reduce(lm, 1, a.maxout + unit);
+}
+
+}  // namespace gl

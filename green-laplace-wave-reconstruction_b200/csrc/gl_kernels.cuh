@@ -53,7 +53,10 @@ enum Mult : int {
   M_NUQX, M_NUQY, M_IQX, M_IQY, M_MI_NU, M_MI_Q2_SNU, M_MI_Q2NU, M_MINUS_A, M_MINUS_Q2,
   M_A, M_PSI11,
   // order-2 banks divide after the multiply: (s * qx) / safe_nu (spatial.py:199-201)
-  M_QX_DIVNU, M_QY_DIVNU, M_Q2_DIVNU
+  M_QX_DIVNU, M_QY_DIVNU, M_Q2_DIVNU,
+  // order-4 banks (paper/order4/cpp/gl_eta44_fftw.cpp:188-290, 299-529)
+  M_MI_NU2QX, M_MI_NU2QY, M_MINUS_Q2A, M_I_ANU, M_PHI_IQXQ2, M_PHI_IQYQ2, M_PHI_Q4, M_NU4,
+  M_Q2NU, M_NU2QX, M_NU2QY, M_IQXA, M_IQYA, M_Q2A
 };
 
 struct BinGeo {
@@ -111,6 +114,26 @@ GL_D cplx apply_mult(int m, const GeoRef& g, cplx s) {
     case M_QX_DIVNU: { const cplx t = cscale(g.qx(), s); const double sn = safe_nu(g.nu()); return cmk(t.x / sn, t.y / sn); }
     case M_QY_DIVNU: { const cplx t = cscale(g.qy(), s); const double sn = safe_nu(g.nu()); return cmk(t.x / sn, t.y / sn); }
     case M_Q2_DIVNU: { const double q = g.q(); const cplx t = cscale(q * q, s); const double sn = safe_nu(g.nu()); return cmk(t.x / sn, t.y / sn); }
+    case M_MI_NU2QX: { const double nu = g.nu(); return cmulmi(cscale(nu * nu * g.qx(), s)); }
+    case M_MI_NU2QY: { const double nu = g.nu(); return cmulmi(cscale(nu * nu * g.qy(), s)); }
+    case M_MINUS_Q2A: { const double q = g.q(); return cscale(-(q * q * g.a()), s); }
+    case M_I_ANU: return cmuli(cscale(g.a() * g.nu(), s));
+    case M_PHI_IQXQ2: case M_PHI_IQYQ2: case M_PHI_Q4: {
+      // phi = (-i s)/nu where nu > 0, then the vertical-derivative multiplier
+      const double nu = g.nu();
+      if (!(nu > 0.0)) return czero();
+      const cplx phi = cmk(s.y / nu, -s.x / nu);
+      const double q = g.q();
+      if (m == M_PHI_Q4) return cscale(q * q * q * q, phi);
+      return cmuli(cscale((m == M_PHI_IQXQ2 ? g.qx() : g.qy()) * q * q, phi));
+    }
+    case M_NU4: { const double nu = g.nu(); return cscale(nu * nu * nu * nu, s); }
+    case M_Q2NU: { const double q = g.q(); return cscale(q * q * g.nu(), s); }
+    case M_NU2QX: { const double nu = g.nu(); return cscale(nu * nu * g.qx(), s); }
+    case M_NU2QY: { const double nu = g.nu(); return cscale(nu * nu * g.qy(), s); }
+    case M_IQXA: return cmuli(cscale(g.qx() * g.a(), s));
+    case M_IQYA: return cmuli(cscale(g.qy() * g.a(), s));
+    case M_Q2A: { const double q = g.q(); return cscale(q * q * g.a(), s); }
   }
   return czero();
 }
@@ -126,6 +149,10 @@ enum ColKind : int {
   COL_INNER,       // (s e^{-tau3 (nu - shift3)}) e^{-tau2 (nu - shift2)}
   COL_OUTER1,      // s e^{-tau3 (nu - shift3)}
   COL_OUTER2,      // pair spectra E (eta, eta_t floored, phi, phi_t)
+  COL_E44_PAIR,    // order 4: ((s e4) e3) e2 for third-level pairs, (s e4) e2 for order-4 pairs
+  COL_E44_FIRST3,  // order 4: (s e4) e3
+  COL_E44_FIRST4,  // order 4: s e4
+  COL_FLOORED,     // bank k reads spectrum src_of[k] of the job with its own roundoff floor
 };
 
 constexpr int MAX_BANKS = 24;
@@ -149,6 +176,7 @@ struct ColArgs {
   int n_outer;
   const unsigned char* chan_mask;  // [unit][2][h][w] (COL_PSI22)
   const unsigned long long* floor_max;  // per-job max for floored spectra
+  int floor_nsrc;          // COL_FLOORED: maxima per job (indexed job * floor_nsrc + src)
   double floor_rel;
   // output
   cplx* out;               // [job][bank][w][n]
@@ -195,6 +223,30 @@ GL_D cplx col_base(const ColArgs& a, int job, int i, double nu) {
       const double tau3 = a.nodes[sub] / u.lam3;
       return cscale(exp(-tau3 * (nu - u.shift3)), v);
     }
+    case COL_E44_PAIR: {
+      const int R = a.n_inner;
+      const int r3 = R * R * R;
+      int o, t = -1, pn;
+      if (sub < r3) {
+        o = sub / (R * R);
+        t = (sub / R) % R;
+        pn = sub % R;
+      } else {
+        o = (sub - r3) / R;
+        pn = (sub - r3) % R;
+      }
+      cplx d = cscale(exp(-(a.nodes[o] / u.lam4) * (nu - u.shift4)), v);
+      if (t >= 0) d = cscale(exp(-(a.nodes[t] / u.lam3) * (nu - u.shift3)), d);
+      return cscale(exp(-(a.nodes[pn] / u.lam2) * (nu - u.shift2)), d);
+    }
+    case COL_E44_FIRST3: {
+      const int R = a.n_inner;
+      const int o = sub / R, t = sub % R;
+      const cplx d = cscale(exp(-(a.nodes[o] / u.lam4) * (nu - u.shift4)), v);
+      return cscale(exp(-(a.nodes[t] / u.lam3) * (nu - u.shift3)), d);
+    }
+    case COL_E44_FIRST4:
+      return cscale(exp(-(a.nodes[sub] / u.lam4) * (nu - u.shift4)), v);
   }
   return v;
 }
@@ -218,7 +270,7 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
   const int plane = a.box.w * a.box.h;
   cplx* bufs = smem;                   // cw * L
   cplx* base = smem + (size_t)cw * L;  // cw * h
-  const bool shared_base = a.kind != COL_PLAIN && a.kind != COL_OUTER2;
+  const bool shared_base = a.kind != COL_PLAIN && a.kind != COL_OUTER2 && a.kind != COL_FLOORED;
   if (shared_base) {
     for (int t = threadIdx.x; t < ncol * h; t += blockDim.x) {
       const int c = t / h, by = t % h;
@@ -233,8 +285,11 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
   for (int k = k_first; k < k_last; ++k) {
     const int mult = a.mult[k];
     const cplx* sk = a.spec + (long long)job * a.spec_job_stride + (long long)a.src_of[k] * a.spec_sub_stride;
-    const bool floor_it = a.kind == COL_OUTER2 && a.src_of[k] == 1 && a.floor_max;
-    const double floor_abs = floor_it ? a.floor_rel * as_double(a.floor_max[job]) : 0.0;
+    const bool floor_it = a.floor_max && ((a.kind == COL_OUTER2 && a.src_of[k] == 1) || a.kind == COL_FLOORED);
+    const double floor_abs =
+        !floor_it ? 0.0
+                  : a.floor_rel * as_double(a.kind == COL_FLOORED ? a.floor_max[(size_t)job * a.floor_nsrc + a.src_of[k]]
+                                                                  : a.floor_max[job]);
     for (int it = 0; it < iters; ++it) {
       const int c = it * G + g;
       const bool active = c < ncol;
@@ -269,7 +324,8 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
 // row kernel: inverse FFT along x, products, forward FFT along x
 // ---------------------------------------------------------------------------
 
-enum RowKind : int { ROW_ETA22 = 0, ROW_PSI22, ROW_CONTACT22, ROW_INNER, ROW_OUTER };
+enum RowKind : int { ROW_ETA22 = 0, ROW_PSI22, ROW_CONTACT22, ROW_INNER, ROW_OUTER,
+                     ROW_E44_PAIR, ROW_E44_THIRD, ROW_E44_ORDER4 };
 
 struct BankGroup {
   const cplx* data;  // [job][nb][w][n_y]
@@ -279,7 +335,7 @@ struct BankGroup {
 
 struct RowArgs {
   int kind;
-  BankGroup grp[2];
+  BankGroup grp[3];
   int ngrp;
   int nout;
   int out_x0, out_w;       // kept output columns (modes)
@@ -344,6 +400,136 @@ GL_D void row_products(int kind, cplx* b, int L, int p, int chan_count) {
       BK(1) = sk;
       BK(2) = sdt;
       BK(3) = skt;
+      break;
+    }
+    case ROW_E44_PAIR: {  // gl_eta44_fftw.cpp:375-381: six pair sources from 16 banks
+      const cplx v = BK(0), vn = BK(1), vn2 = BK(2), vn3 = BK(3), vn4 = BK(4), hx = BK(5),
+                 hy = BK(6), jx = BK(7), jy = BK(8), ro = BK(9), qq = BK(10), q2n = BK(11),
+                 njx = BK(12), njy = BK(13), n2jx = BK(14), n2jy = BK(15);
+      const cplx v2 = cscale(2.0, v);
+      const cplx sd = csub(csub(cadd(cmul(v2, vn2), cmul(vn, vn)), cmul(hx, hx)), cmul(hy, hy));
+      const cplx sk = cadd(cmul(v2, ro), cscale(2.0, cadd(cmul(hx, jx), cmul(hy, jy))));
+      const cplx sds = csub(csub(cadd(cmul(v2, vn3), cmul(cscale(4.0, vn), vn2)), cmul(cscale(2.0, hx), jx)),
+                            cmul(cscale(2.0, hy), jy));
+      const cplx jj = cadd(cadd(cadd(cmul(jx, jx), cmul(hx, njx)), cmul(jy, jy)), cmul(hy, njy));
+      const cplx sks = cadd(cscale(2.0, cadd(cmul(vn, ro), cmul(v, qq))), cscale(2.0, jj));
+      const cplx sdss = csub(cadd(cadd(cmul(v2, vn4), cmul(cscale(6.0, vn), vn3)), cmul(cscale(4.0, vn2), vn2)),
+                             cscale(2.0, jj));
+      const cplx skss = cadd(cadd(cscale(2.0, cadd(cadd(cmul(vn2, ro), cmul(cscale(2.0, vn), qq)), cmul(v, q2n))),
+                                  cscale(6.0, cadd(cmul(jx, njx), cmul(jy, njy)))),
+                             cscale(2.0, cadd(cmul(hx, n2jx), cmul(hy, n2jy))));
+      BK(0) = sd;
+      BK(1) = sk;
+      BK(2) = sds;
+      BK(3) = sks;
+      BK(4) = sdss;
+      BK(5) = skss;
+      break;
+    }
+    case ROW_E44_THIRD: {  // gl_eta44_fftw.cpp:548-566: cubic forcing and its time derivative
+      // first banks 0..15: eta ex ey px py pz pxz pyz pzz pzzz ptz ptzz pxz_t pyz_t pzzz_t ptz_t
+      // pair banks 16..30: eta ex ey eta_t ex_t ey_t px py pz pzz ptz px_t py_t pzz_t ptz_t
+      const cplx fe = BK(0), fex = BK(1), fey = BK(2), fpx = BK(3), fpy = BK(4), fpz = BK(5), fpxz = BK(6),
+                 fpyz = BK(7), fpzz = BK(8), fpzzz = BK(9), fptz = BK(10), fptzz = BK(11), fpxzt = BK(12),
+                 fpyzt = BK(13), fpzzzt = BK(14), fptzt = BK(15);
+      const cplx pe = BK(16), pex = BK(17), pey = BK(18), pet = BK(19), pext = BK(20), peyt = BK(21),
+                 ppx = BK(22), ppy = BK(23), ppz = BK(24), ppzz = BK(25), pptz = BK(26), ppxt = BK(27),
+                 ppyt = BK(28), ppzzt = BK(29), pptzt = BK(30);
+      const cplx hfe = cscale(0.5, fe);
+      const cplx kp = csub(csub(cadd(cadd(cadd(cmul(fpx, pex), cmul(fpy, pey)), cmul(ppx, fex)), cmul(ppy, fey)),
+                                cmul(fe, ppzz)), cmul(pe, fpzz));
+      const cplx kd = csub(cmul(fe, cadd(cmul(fpxz, fex), cmul(fpyz, fey))), cmul(cmul(hfe, fe), fpzzz));
+      const cplx dp = cadd(cadd(cadd(cadd(cmul(fe, pptz), cmul(pe, fptz)), cmul(fpx, ppx)), cmul(fpy, ppy)),
+                           cmul(fpz, ppz));
+      const cplx dd = cadd(cmul(cmul(hfe, fe), fptzz),
+                           cmul(fe, cadd(cadd(cmul(fpx, fpxz), cmul(fpy, fpyz)), cmul(fpz, fpzz))));
+      cplx kpt = cmul(cmk(-fex.x, -fex.y), pex);
+      kpt = cadd(kpt, cmul(fpx, pext));
+      kpt = csub(kpt, cmul(fey, pey));
+      kpt = cadd(kpt, cmul(fpy, peyt));
+      kpt = cadd(kpt, cmul(ppxt, fex));
+      kpt = cadd(kpt, cmul(ppx, fpxz));
+      kpt = cadd(kpt, cmul(ppyt, fey));
+      kpt = cadd(kpt, cmul(ppy, fpyz));
+      kpt = csub(kpt, cmul(fpz, ppzz));
+      kpt = csub(kpt, cmul(fe, ppzzt));
+      kpt = csub(kpt, cmul(pet, fpzz));
+      kpt = csub(kpt, cmul(pe, fptzz));
+      const cplx kdt = csub(csub(cadd(cmul(fpz, cadd(cmul(fpxz, fex), cmul(fpyz, fey))),
+                                      cmul(fe, cadd(cadd(cadd(cmul(fpxzt, fex), cmul(fpxz, fpxz)), cmul(fpyzt, fey)),
+                                                    cmul(fpyz, fpyz)))),
+                                 cmul(cmul(fe, fpz), fpzzz)),
+                            cmul(cmul(hfe, fe), fpzzzt));
+      cplx dpt = cmul(fpz, pptz);
+      dpt = cadd(dpt, cmul(fe, pptzt));
+      dpt = cadd(dpt, cmul(pet, fptz));
+      dpt = cadd(dpt, cmul(pe, fptzt));
+      dpt = csub(dpt, cmul(fex, ppx));
+      dpt = cadd(dpt, cmul(fpx, ppxt));
+      dpt = csub(dpt, cmul(fey, ppy));
+      dpt = cadd(dpt, cmul(fpy, ppyt));
+      dpt = cadd(dpt, cmul(fptz, ppz));
+      dpt = cadd(dpt, cmul(fpz, pptz));
+      cplx inner = cmul(cmk(-fex.x, -fex.y), fpxz);
+      inner = cadd(inner, cmul(fpx, fpxzt));
+      inner = csub(inner, cmul(fey, fpyz));
+      inner = cadd(inner, cmul(fpy, fpyzt));
+      inner = cadd(inner, cmul(fptz, fpzz));
+      inner = cadd(inner, cmul(fpz, fptzz));
+      const cplx ddt = cadd(cadd(csub(cmul(cmul(fe, fpz), fptzz), cmul(cmul(hfe, fe), fpzzz)),
+                                 cmul(fpz, cadd(cadd(cmul(fpx, fpxz), cmul(fpy, fpyz)), cmul(fpz, fpzz)))),
+                            cmul(fe, inner));
+      BK(0) = cadd(cscale(0.25, kd), cscale(0.5, kp));
+      BK(1) = cadd(cscale(0.25, dd), cscale(0.5, dp));
+      BK(2) = cadd(cscale(0.25, kdt), cscale(0.5, kpt));
+      BK(3) = cadd(cscale(0.25, ddt), cscale(0.5, dpt));
+      break;
+    }
+    case ROW_E44_ORDER4: {  // gl_eta44_fftw.cpp:712-735: partitions 31, 22, 211, 1111
+      // first4 banks 0..18: eta ex ey px py pz pxz pyz pzz pzzz ptz ptzz pxz_t pyz_t pzzz_t ptz_t pxzz pyzz pzzzz
+      // pair4 banks 19..36: eta ex ey eta_t ex_t ey_t px py pz pzz ptz px_t py_t pzz_t ptz_t pxz pyz pzzz
+      // third banks 37..44: eta ex ey px py pz pzz pzt
+      const cplx fe = BK(0), fex = BK(1), fey = BK(2), fpx = BK(3), fpy = BK(4), fpz = BK(5), fpxz = BK(6),
+                 fpyz = BK(7), fpzz = BK(8), fpzzz = BK(9), fptz = BK(10), fptzz = BK(11),
+                 fpzzzt = BK(14), fpxzz = BK(16), fpyzz = BK(17), fpzzzz = BK(18);
+      const cplx pe = BK(19), pex = BK(20), pey = BK(21), ppx = BK(25), ppy = BK(26), ppz = BK(27),
+                 ppzz = BK(28), pptz = BK(29), ppzzt = BK(32), ppxz = BK(34), ppyz = BK(35), ppzzz = BK(36);
+      const cplx te = BK(37), tex = BK(38), tey = BK(39), tpx = BK(40), tpy = BK(41), tpz = BK(42),
+                 tpzz = BK(43), tpzt = BK(44);
+      const cplx hfe = cscale(0.5, fe);
+      const cplx k31 = csub(csub(cadd(cadd(cadd(cmul(fpx, tex), cmul(fpy, tey)), cmul(tpx, fex)), cmul(tpy, fey)),
+                                 cmul(fe, tpzz)), cmul(te, fpzz));
+      const cplx d31 = cadd(cadd(cadd(cadd(cmul(fe, tpzt), cmul(te, fptz)), cmul(fpx, tpx)), cmul(fpy, tpy)),
+                            cmul(fpz, tpz));
+      const cplx k22 = csub(cadd(cmul(ppx, pex), cmul(ppy, pey)), cmul(pe, ppzz));
+      const cplx d22 = cadd(cmul(pe, pptz), cscale(0.5, cadd(cadd(cmul(ppx, ppx), cmul(ppy, ppy)), cmul(ppz, ppz))));
+      const cplx mx_ = cadd(cmul(fe, ppxz), cmul(pe, fpxz));
+      const cplx my_ = cadd(cmul(fe, ppyz), cmul(pe, fpyz));
+      const cplx mz_ = cadd(cmul(fe, ppzz), cmul(pe, fpzz));
+      const cplx k211 = csub(csub(cadd(cadd(cmul(fe, cadd(cmul(fpxz, pex), cmul(fpyz, pey))), cmul(mx_, fex)),
+                                       cmul(my_, fey)),
+                                  cmul(cmul(hfe, fe), ppzzz)),
+                             cmul(cmul(fe, pe), fpzzz));
+      cplx d211 = cmul(cmul(hfe, fe), ppzzt);
+      d211 = cadd(d211, cmul(cmul(fe, pe), fptzz));
+      d211 = cadd(d211, cmul(fpx, mx_));
+      d211 = cadd(d211, cmul(fpy, my_));
+      d211 = cadd(d211, cmul(fpz, mz_));
+      d211 = cadd(d211, cmul(ppx, cmul(fe, fpxz)));
+      d211 = cadd(d211, cmul(ppy, cmul(fe, fpyz)));
+      d211 = cadd(d211, cmul(ppz, cmul(fe, fpzz)));
+      const cplx hfe2 = cmul(hfe, fe);
+      const cplx fe3 = cmul(cmul(fe, fe), fe);
+      const cplx k3v = cmul(fe3, fpzzzz);
+      const cplx k1111 = csub(cmul(hfe2, cadd(cmul(fpxzz, fex), cmul(fpyzz, fey))), cmk(k3v.x / 6.0, k3v.y / 6.0));
+      const cplx d3v = cmul(fe3, fpzzzt);
+      const cplx d1111 = cadd(cadd(cmk(d3v.x / 6.0, d3v.y / 6.0),
+                                   cmul(hfe2, cadd(cadd(cmul(fpx, fpxzz), cmul(fpy, fpyzz)), cmul(fpz, fpzzz)))),
+                              cmul(hfe2, cadd(cadd(cmul(fpxz, fpxz), cmul(fpyz, fpyz)), cmul(fpzz, fpzz))));
+      const cplx kb = cadd(cadd(cscale(0.125, k1111), cscale(0.25, k211)), cscale(0.5, k22));
+      const cplx db = cadd(cadd(cscale(0.125, d1111), cscale(0.25, d211)), cscale(0.5, d22));
+      BK(0) = cadd(cscale(0.5, k31), kb);
+      BK(1) = cadd(cscale(0.5, d31), db);
       break;
     }
     case ROW_OUTER: {  // _order3.py:76-102, 275-287

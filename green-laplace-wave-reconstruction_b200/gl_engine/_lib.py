@@ -25,8 +25,9 @@ STATUS_NAMES = {
 }
 
 COMP_ETA11, COMP_PSI11, COMP_ETA22, COMP_PSI22, COMP_ETA33, COMP_PSI33 = 1, 2, 4, 8, 16, 32
+COMP_ETA44 = 64
 COMP_NAMES = {COMP_ETA11: "eta11", COMP_PSI11: "psi11", COMP_ETA22: "eta22",
-              COMP_PSI22: "psi22", COMP_ETA33: "eta33", COMP_PSI33: "psi33"}
+              COMP_PSI22: "psi22", COMP_ETA33: "eta33", COMP_PSI33: "psi33", COMP_ETA44: "eta44"}
 GRID_COMPACT, GRID_REFERENCE = 0, 1
 OUT_COMPLEX, OUT_REAL = 0, 1
 SPECTRA_FULL, SPECTRA_BOX = 0, 1
@@ -43,6 +44,14 @@ class PlanDesc(C.Structure):
         ("box_x0", C.c_int), ("box_y0", C.c_int), ("box_w", C.c_int), ("box_h", C.c_int),
         ("grid", C.c_int), ("max_units", C.c_int), ("output", C.c_int),
     ]
+
+
+class Eta44Desc(C.Structure):
+    _fields_ = [("n", C.c_int), ("dk", C.c_double), ("depth", C.c_double),
+                ("peak_depth", C.c_double), ("rank", C.c_int),
+                ("nodes", C.POINTER(C.c_double)), ("weights", C.POINTER(C.c_double)),
+                ("box_x0", C.c_int), ("box_y0", C.c_int), ("box_w", C.c_int), ("box_h", C.c_int),
+                ("max_units", C.c_int), ("output", C.c_int)]
 
 
 class PlanInfo(C.Structure):
@@ -70,6 +79,7 @@ class WitStats(C.Structure):
 SIGNATURES = {
     "gl_plan_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(PlanDesc)]),
     "gl_plan_destroy": (None, [C.c_void_p]),
+    "gl_eta44_plan_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(Eta44Desc)]),
     "gl_plan_get_info": (C.c_int, [C.c_void_p, C.POINTER(PlanInfo)]),
     "gl_workspace_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "gl_deposit_modes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,

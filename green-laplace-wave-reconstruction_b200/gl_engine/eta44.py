@@ -1,0 +1,163 @@
+"""Fourth-order GL eta44 (no Stokes corrections) on the GPU, and the
+reference's binary formats for it.
+
+* :func:`eta44` runs a ``gl_eta44_plan_create`` plan through ``gl_execute``;
+* :func:`read_glrti` / :func:`write_glrti` / :func:`read_gle44` /
+  :func:`write_gle44` restate the ``GLRTI001`` input and ``GLE44O01`` output
+  layouts of ``paper/order4/cpp/gl_eta44_fftw.cpp:648-691, 753-764`` (writer
+  ``paper/order4/export_cpp_gl_runtime_input.m``).  Those files store arrays
+  x-major (flat index ix*n + iy); this module returns numpy ``[iy, ix]``.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import struct
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import _lib
+from .api import Plan, _engine_call, _status_error
+
+
+@dataclass
+class GlInput:
+    n: int
+    dk: float
+    depth: float
+    peak_depth: float
+    rules: dict            # rank -> (nodes, weights)
+    spectrum: np.ndarray   # [iy, ix] complex128, N^2-scaled
+
+
+def write_glrti(path, inp: GlInput) -> None:
+    with open(path, "wb") as f:
+        f.write(b"GLRTI001")
+        f.write(struct.pack("<Q3d", inp.n, inp.dk, inp.depth, inp.peak_depth))
+        f.write(struct.pack("<Q", len(inp.rules)))
+        for rank in sorted(inp.rules):
+            nodes, weights = inp.rules[rank]
+            f.write(struct.pack("<Q", rank))
+            f.write(np.asarray(nodes, dtype="<f8").tobytes())
+            f.write(np.asarray(weights, dtype="<f8").tobytes())
+        f.write(np.ascontiguousarray(inp.spectrum.T).astype(np.complex128).view("<f8").tobytes())
+
+
+def read_glrti(path) -> GlInput:
+    raw = Path(path).read_bytes()
+    if raw[:8] != b"GLRTI001":
+        raise ValueError("magic")
+    n, dk, depth, peak = struct.unpack_from("<Q3d", raw, 8)
+    (nr,) = struct.unpack_from("<Q", raw, 40)
+    off = 48
+    rules = {}
+    for _ in range(nr):
+        (j,) = struct.unpack_from("<Q", raw, off)
+        off += 8
+        nodes = np.frombuffer(raw, "<f8", j, off).copy()
+        off += 8 * j
+        weights = np.frombuffer(raw, "<f8", j, off).copy()
+        off += 8 * j
+        rules[int(j)] = (nodes, weights)
+    vals = np.frombuffer(raw, "<f8", 2 * n * n, off)
+    spec = (vals[0::2] + 1j * vals[1::2]).reshape(n, n).T.copy()
+    return GlInput(n=int(n), dk=dk, depth=depth, peak_depth=peak, rules=rules, spectrum=spec)
+
+
+def write_gle44(path, n: int, rank: int, field: np.ndarray, threads: int = 1,
+                elapsed: float = 0.0) -> None:
+    """``GLE44O01``: dimensionless analytic eta44 field, x-major."""
+    with open(path, "wb") as f:
+        f.write(b"GLE44O01")
+        f.write(struct.pack("<3Qd", n, rank, threads, elapsed))
+        f.write(np.ascontiguousarray(np.asarray(field).T).astype(np.complex128).view("<f8").tobytes())
+
+
+def read_gle44(path):
+    raw = Path(path).read_bytes()
+    if raw[:8] != b"GLE44O01":
+        raise ValueError("magic")
+    n, rank, threads, elapsed = struct.unpack_from("<3Qd", raw, 8)
+    vals = np.frombuffer(raw, "<f8", 2 * n * n, 40)
+    field = (vals[0::2] + 1j * vals[1::2]).reshape(n, n).T.copy()
+    return {"n": int(n), "rank": int(rank), "threads": int(threads), "elapsed": elapsed,
+            "field": field}
+
+
+def spectrum_from_modes(modes, amplitudes, n: int, depth: float) -> np.ndarray:
+    """s = n^2 c / h at (my, mx) (``paper/order4/prepare_order4_inputs.m:12-16``)."""
+    s = np.zeros((n, n), dtype=complex)
+    for (mx, my), c in zip(np.asarray(modes), np.asarray(amplitudes)):
+        s[int(my) % n, int(mx) % n] = n * n * c / depth
+    return s
+
+
+def _box(spectrum: np.ndarray):
+    n = spectrum.shape[0]
+    mag = np.abs(spectrum)
+    thr = 1e-13 * max(1.0, float(mag.max()))
+    rows = np.flatnonzero((mag > 0).any(axis=1))
+    cols = np.flatnonzero((mag > 0).any(axis=0))
+    my = np.where(rows < n // 2, rows, rows - n)
+    mx = np.where(cols < n // 2, cols, cols - n)
+    if not np.any(mag > thr):
+        raise ValueError("empty analytic support")
+    return int(mx.min()), int(my.min()), int(mx.max() - mx.min() + 1), int(my.max() - my.min() + 1)
+
+
+class Eta44Plan(Plan):
+    def __init__(self, desc: _lib.Eta44Desc, device: torch.device, keep=None):
+        self.lib = _lib.load()
+        self.device = device
+        self.desc = desc
+        self._keep = keep
+        with torch.cuda.device(device):
+            handle = C.c_void_p()
+            _engine_call(self.lib.gl_eta44_plan_create(C.byref(handle), C.byref(desc)))
+            self.handle = handle
+            info = _lib.PlanInfo()
+            _engine_call(self.lib.gl_plan_get_info(handle, C.byref(info)))
+            self.info = info
+            size = C.c_size_t()
+            _engine_call(self.lib.gl_workspace_size(handle, C.byref(size)))
+            self.workspace_bytes = int(size.value)
+            self.workspace = torch.empty(self.workspace_bytes + 256, dtype=torch.uint8, device=device)
+
+
+def eta44(spectra, *, dk: float, depth: float, peak_depth: float, rank: int, nodes=None,
+          weights=None, device=None, output: str = "complex") -> np.ndarray:
+    """Physical analytic eta44 fields (depth x the GLE44O01 field) of one or
+    more N^2-scaled analytic spectra ``[..., iy, ix]`` sharing one grid."""
+    spectra = np.asarray(spectra, dtype=np.complex128)
+    single = spectra.ndim == 2
+    if single:
+        spectra = spectra[None]
+    units, n, _ = spectra.shape
+    box = _box(np.abs(spectra).max(axis=0))
+    dev = torch.device(device if device is not None else "cuda")
+    keep = None
+    nd = wd = None
+    if nodes is not None:
+        keep = (np.ascontiguousarray(nodes, dtype=float), np.ascontiguousarray(weights, dtype=float))
+        nd = keep[0].ctypes.data_as(C.POINTER(C.c_double))
+        wd = keep[1].ctypes.data_as(C.POINTER(C.c_double))
+    out_mode = _lib.OUT_REAL if output == "real" else _lib.OUT_COMPLEX
+    desc = _lib.Eta44Desc(n=n, dk=dk, depth=depth, peak_depth=peak_depth, rank=rank, nodes=nd,
+                          weights=wd, box_x0=box[0], box_y0=box[1], box_w=box[2], box_h=box[3],
+                          max_units=1, output=out_mode)
+    plan = Eta44Plan(desc, dev, keep)
+    with torch.cuda.device(dev):
+        spec = torch.from_numpy(np.ascontiguousarray(spectra)).to(dev)
+        dtype = torch.float64 if out_mode == _lib.OUT_REAL else torch.complex128
+        out = torch.empty((units, 1, n, n), dtype=dtype, device=dev)
+        status = torch.zeros(units, dtype=torch.int32, device=dev)
+        plan.execute(units, torch.view_as_real(spec), _lib.SPECTRA_FULL, out, status,
+                     torch.cuda.current_stream(dev).cuda_stream)
+        st = status.cpu().numpy()
+        if np.any(st != 0):
+            raise _status_error(int(st[st != 0][0]))
+        res = out[:, 0].cpu().numpy()
+    return res[0] if single else res

@@ -65,6 +65,7 @@ typedef enum gl_status {
 #define GL_COMP_PSI22 0x08
 #define GL_COMP_ETA33 0x10
 #define GL_COMP_PSI33 0x20
+#define GL_COMP_ETA44 0x40  /* fourth-order plans (gl_eta44_plan_create) */
 
 #define GL_GRID_COMPACT 0   /* smallest alias-free power-of-two product grid */
 #define GL_GRID_REFERENCE 1 /* products on the reference's own Nx x Ny grid   */
@@ -107,6 +108,27 @@ typedef struct gl_plan_info {
 gl_status gl_plan_create(gl_plan** plan, const gl_plan_desc* desc);
 void gl_plan_destroy(gl_plan* plan);
 gl_status gl_plan_get_info(const gl_plan* plan, gl_plan_info* info);
+
+/* Fourth-order pure-sum eta44 (no Stokes corrections) at GL rank R for all
+ * three nested levels.  Replaces paper/order4/cpp/gl_eta44_fftw.cpp (the
+ * GLRTI001 -> GLE44O01 executor, lines 76-749) and its MATLAB authority
+ * src/internal/finite_depth_directional_green_laplace_eta44_three_kernels.m.
+ * Conventions follow the C++: qx = (depth dk) mx, the peak depth is supplied,
+ * the square grid is n x n.  The plan runs through gl_execute: inputs are the
+ * N^2-scaled analytic spectra (full [ny][nx] or box), the output is the
+ * analytic eta44 field times depth (one plane per unit). */
+typedef struct gl_eta44_desc {
+  int n;                      /* square grid (power of two)                   */
+  double dk, depth, peak_depth;
+  int rank;                   /* GL rank of every level (paper: 6, 8, 10)     */
+  const double* nodes;        /* optional host rule of length rank (NULL:     */
+  const double* weights;      /* the engine's Golub--Welsch rule)             */
+  int box_x0, box_y0, box_w, box_h;
+  int max_units;
+  int output;                 /* GL_OUT_*                                      */
+} gl_eta44_desc;
+
+gl_status gl_eta44_plan_create(gl_plan** plan, const gl_eta44_desc* desc);
 
 /* Device workspace bytes needed by gl_execute (independent of n_units). */
 gl_status gl_workspace_size(const gl_plan* plan, size_t* bytes);

@@ -1,0 +1,76 @@
+"""Fourth-order GL eta44: file formats (CPU), GPU parity with the CPU
+restatement of paper/order4/cpp/gl_eta44_fftw.cpp, and the paper's GL-vs-WIT
+metrics on the 382-mode field (paper/order4/data/eta44_no_stokes_rank_metrics.csv)."""
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from gl_engine import eta44 as E44
+from gl_engine import wit
+from oracle import gl_eta44 as OE
+from oracle import gl_oracle as O
+
+GOLD = Path(__file__).resolve().parent / "golden"
+# raw relative L2 of GL vs WIT eta44, percent (eta44_no_stokes_rank_metrics.csv:2-4)
+PAPER_L2_PCT = {6: 9.1656674905729, 8: 4.20839343830129, 10: 2.03486173251526}
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(b))
+
+
+def test_glrti_and_gle44_round_trip(tmp_path):
+    rng = np.random.default_rng(0)
+    spec = rng.standard_normal((16, 16)) + 1j * rng.standard_normal((16, 16))
+    nodes, weights = O.gauss_laguerre(6)
+    inp = E44.GlInput(n=16, dk=0.2, depth=1.0, peak_depth=1.0, rules={6: (nodes, weights)},
+                      spectrum=spec)
+    E44.write_glrti(tmp_path / "in.bin", inp)
+    back = E44.read_glrti(tmp_path / "in.bin")
+    assert np.array_equal(back.spectrum, spec) and back.rules[6][0].tolist() == nodes.tolist()
+    raw = (tmp_path / "in.bin").read_bytes()
+    # x-major storage: flat index ix*n + iy
+    off = 8 + 32 + 8 + 8 + 2 * 6 * 8
+    first = np.frombuffer(raw, "<f8", 4, off)
+    assert first[0] == spec[0, 0].real and first[2] == spec[1, 0].real
+    E44.write_gle44(tmp_path / "out.bin", 16, 6, spec)
+    assert np.array_equal(E44.read_gle44(tmp_path / "out.bin")["field"], spec)
+
+
+def _small(seed, n=32, m=4):
+    rng = np.random.default_rng(seed)
+    cells = [(x, y) for x in range(1, 4) for y in range(-2, 3)]
+    pick = rng.choice(len(cells), size=m, replace=False)
+    modes = np.array([cells[i] for i in pick])
+    c = 0.02 * (rng.standard_normal(m) + 1j * rng.standard_normal(m))
+    return E44.spectrum_from_modes(modes, c, n, 1.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed,rank", [(0, 2), (1, 3), (2, 4)])
+def test_eta44_matches_cpu_restatement(seed, rank):
+    s = _small(seed)
+    nodes, weights = O.gauss_laguerre(rank)
+    ref = OE.eta44(s, 0.25, 1.0, 1.0, nodes, weights)
+    got = E44.eta44(s, dk=0.25, depth=1.0, peak_depth=1.0, rank=rank)
+    err = rel(got, ref)
+    print(f"seed {seed} GL{rank}: rel L2 {err:.3e}")
+    assert err < 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rank", [6, 8, 10])
+def test_eta44_reproduces_paper_gl_vs_wit_metric(rank):
+    """GL eta44 against the WIT field (which the WIT kernel reproduces to
+    1e-14, test_wit.py) gives the paper's raw relative L2 at each rank."""
+    inp = wit.read_dir4in(GOLD / "wit_field_n0382_input.bin")
+    n = inp.nx
+    w = wit.wit_eta44(inp)
+    ref = np.real(np.fft.ifft2(w.fields["eta"][0] * n * n))
+    s = E44.spectrum_from_modes(inp.modes, inp.amplitudes[0], n, inp.depth)
+    gl = np.real(E44.eta44(s, dk=inp.dkx, depth=inp.depth, peak_depth=1.0, rank=rank))
+    pct = 100 * rel(gl, ref)
+    print(f"GL{rank} vs WIT raw rel L2 {pct:.13f} % (paper {PAPER_L2_PCT[rank]})")
+    assert abs(pct / PAPER_L2_PCT[rank] - 1) < 1e-6
