@@ -2654,10 +2654,37 @@ extern "C" size_t gl_wit_workspace_size(int n_modes) {
   return align_up(sizeof(WitStats)) + 5 * wit_binom_stride(n_modes) * sizeof(unsigned long long);
 }
 
+extern "C" gl_status gl_wit_read_sector_stats(int sector, const void* d_work, int n_modes,
+                                              gl_wit_stats* out);
+
+static unsigned long long wit_candidates(int sector, unsigned long long n) {
+  if (sector == 40) {
+    const unsigned long long p = n * (n + 1) / 2;
+    return p * p;
+  }
+  if (sector == 42) return n * (n + 1) * (n + 2) / 6 * n;
+  return n * (n + 1) * (n + 2) * (n + 3) / 24;
+}
+
+extern "C" gl_status gl_wit_sector(int sector, int n_modes, const int* d_modes, int n_cases,
+                                   const void* d_amp, int nx, int ny, double gravity, double depth,
+                                   double dkx, double dky, double threshold, void* d_out,
+                                   void* d_work, size_t work_bytes, void* stream);
+
 extern "C" gl_status gl_wit_eta44(int n_modes, const int* d_modes, int n_cases, const void* d_amp,
                                   int nx, int ny, double gravity, double depth, double dkx,
                                   double dky, double threshold, void* d_out, void* d_work,
                                   size_t work_bytes, void* stream) {
+  return gl_wit_sector(44, n_modes, d_modes, n_cases, d_amp, nx, ny, gravity, depth, dkx, dky,
+                       threshold, d_out, d_work, work_bytes, stream);
+}
+
+extern "C" gl_status gl_wit_sector(int sector, int n_modes, const int* d_modes, int n_cases,
+                                   const void* d_amp, int nx, int ny, double gravity, double depth,
+                                   double dkx, double dky, double threshold, void* d_out,
+                                   void* d_work, size_t work_bytes, void* stream) {
+  if (sector != 40 && sector != 42 && sector != 44)
+    return fail(GL_ERR_SECTOR, "sector must be 40, 42, or 44");
   if (n_modes < 1 || n_modes > 65535 || n_cases < 1 || !d_modes || !d_amp || !d_out || !d_work)
     return fail(GL_ERR_INVALID_ARGUMENT, "bad WIT arguments (modes 1..65535, cases >= 1, non-null buffers)");
   if (nx < 2 || ny < 2 || (nx % 2) || (ny % 2))
@@ -2699,9 +2726,10 @@ extern "C" gl_status gl_wit_eta44(int n_modes, const int* d_modes, int n_cases, 
   a.M = WitModel{gravity, depth};
   a.out = reinterpret_cast<cplx*>(d_out);
   a.stats = reinterpret_cast<WitStats*>(work);
-  a.n_quartets = binom[4 * stride + n_modes + 3];
+  a.n_quartets = wit_candidates(sector, (unsigned long long)n_modes);
   a.binom = d_binom;
   a.binom_stride = (int)stride;
+  a.sector = sector;
   const int blocks = (int)std::min<unsigned long long>((a.n_quartets + 127) / 128, 148ull * 32);
   {
     LaunchScope ls("wit44_kernel", st, 0.0);
@@ -2712,11 +2740,15 @@ extern "C" gl_status gl_wit_eta44(int n_modes, const int* d_modes, int n_cases, 
 }
 
 extern "C" gl_status gl_wit_read_stats(const void* d_work, int n_modes, gl_wit_stats* out) {
+  return gl_wit_read_sector_stats(44, d_work, n_modes, out);
+}
+
+extern "C" gl_status gl_wit_read_sector_stats(int sector, const void* d_work, int n_modes,
+                                              gl_wit_stats* out) {
   if (!d_work || !out || n_modes < 1) return fail(GL_ERR_INVALID_ARGUMENT, "bad WIT stats arguments");
   WitStats w;
   CUDA_TRY(cudaMemcpy(&w, d_work, sizeof w, cudaMemcpyDeviceToHost));
-  const unsigned long long n = (unsigned long long)n_modes;
-  out->candidates = n * (n + 1) * (n + 2) * (n + 3) / 24;
+  out->candidates = wit_candidates(sector, (unsigned long long)n_modes);
   out->kept = w.kept;
   out->near = w.near;
   out->strict_zero_output = w.strict_zero_output;

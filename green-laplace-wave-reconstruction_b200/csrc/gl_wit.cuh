@@ -317,9 +317,10 @@ struct WitArgs {
   WitModel M;
   cplx* out;                // 5 planes [field][case][ny][nx]
   WitStats* stats;
-  unsigned long long n_quartets;
+  unsigned long long n_quartets;   // candidates of the sector
   const unsigned long long* binom;  // binom[r][v] = C(v, r), r = 1..4, v <= n_modes + 3
   int binom_stride;
+  int sector;                       // 44, 40 or 42
 };
 
 // Largest v with C(v, r) <= q (v in [r-1, hi]).
@@ -333,59 +334,106 @@ GL_D int wit_unrank_step(const unsigned long long* row, int hi, unsigned long lo
   return lo;
 }
 
+// Sectors of the fourth-order sum (directional_eta4_openmp.cpp:604-734):
+//   44: unordered quartets of + parents, all targets inside the grid;
+//   40: unordered + pair x unordered - pair, analytic half-plane targets;
+//   42: unordered + triple x one - parent.
 __global__ void __launch_bounds__(128) wit44_kernel(WitArgs a) {
   unsigned long long kept = 0, near = 0, szo = 0, szi = 0;
   double max_res = 0.0, min_det = INFINITY, max_src = 0.0;
-  const int top = a.n_modes + 2;
+  const int M = a.n_modes;
+  const unsigned long long* b1 = a.binom + 1 * a.binom_stride;
+  const unsigned long long* b2 = a.binom + 2 * a.binom_stride;
+  const unsigned long long* b3 = a.binom + 3 * a.binom_stride;
+  const unsigned long long* b4 = a.binom + 4 * a.binom_stride;
+  const unsigned long long pairs = b2[M + 1];  // M (M + 1) / 2
+  (void)b1;
   for (unsigned long long qi = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
        qi < a.n_quartets; qi += (unsigned long long)gridDim.x * blockDim.x) {
-    // combinatorial number system: q = C(d,4) + C(c,3) + C(b,2) + C(a,1),
-    // d > c > b > a >= 0; the multiset is (a, b-1, c-2, d-3)
-    unsigned long long q = qi;
-    const int d4 = wit_unrank_step(a.binom + 4 * a.binom_stride, top, q);
-    q -= a.binom[4 * a.binom_stride + d4];
-    const int c3 = wit_unrank_step(a.binom + 3 * a.binom_stride, d4 - 1, q);
-    q -= a.binom[3 * a.binom_stride + c3];
-    const int b2 = wit_unrank_step(a.binom + 2 * a.binom_stride, c3 - 1, q);
-    q -= a.binom[2 * a.binom_stride + b2];
-    const int a1 = (int)q;
-    const int idx[4] = {a1, b2 - 1, c3 - 2, d4 - 3};
+    int idx[4];
+    int sign[4] = {1, 1, 1, 1};
+    if (a.sector == 44) {
+      // combinatorial number system: q = C(d,4) + C(c,3) + C(b,2) + C(a,1),
+      // d > c > b > a >= 0; the multiset is (a, b-1, c-2, d-3)
+      unsigned long long q = qi;
+      const int d4 = wit_unrank_step(b4, M + 2, q);
+      q -= b4[d4];
+      const int c3 = wit_unrank_step(b3, d4 - 1, q);
+      q -= b3[c3];
+      const int bb = wit_unrank_step(b2, c3 - 1, q);
+      q -= b2[bb];
+      idx[0] = (int)q;
+      idx[1] = bb - 1;
+      idx[2] = c3 - 2;
+      idx[3] = d4 - 3;
+    } else if (a.sector == 40) {
+      unsigned long long qp = qi / pairs, qm = qi % pairs;
+      const int pb = wit_unrank_step(b2, M, qp);
+      const int mb = wit_unrank_step(b2, M, qm);
+      idx[0] = (int)(qp - b2[pb]);
+      idx[1] = pb - 1;
+      idx[2] = (int)(qm - b2[mb]);
+      idx[3] = mb - 1;
+      sign[2] = sign[3] = -1;
+    } else {
+      const unsigned long long qt = qi / M;
+      unsigned long long q = qt;
+      const int c3 = wit_unrank_step(b3, M + 1, q);
+      q -= b3[c3];
+      const int bb = wit_unrank_step(b2, c3 - 1, q);
+      q -= b2[bb];
+      idx[0] = (int)q;
+      idx[1] = bb - 1;
+      idx[2] = c3 - 2;
+      idx[3] = (int)(qi % M);
+      sign[3] = -1;
+    }
     int tx = 0, ty = 0;
     for (int s = 0; s < 4; ++s) {
-      tx += a.modes[2 * idx[s]];
-      ty += a.modes[2 * idx[s] + 1];
+      tx += sign[s] * a.modes[2 * idx[s]];
+      ty += sign[s] * a.modes[2 * idx[s] + 1];
     }
     if (tx == 0 && ty == 0) {
       ++szo;
       continue;
     }
+    if (a.sector == 40 && !(tx > 0 || (tx == 0 && ty > 0))) continue;
     if (abs(tx) >= a.nx / 2 || abs(ty) >= a.ny / 2) continue;
     double pkx[4], pky[4];
-    const int sign[4] = {1, 1, 1, 1};
     for (int s = 0; s < 4; ++s) {
       pkx[s] = a.modes[2 * idx[s]] * a.dkx;
       pky[s] = a.modes[2 * idx[s] + 1] * a.dky;
     }
     WitOut r;
     wit_evaluate(a.M, pkx, pky, sign, a.thr, r);
-    // multiset repeat factor: product of factorials of run lengths
-    int rep = 1, run = 1;
-    for (int s = 1; s < 4; ++s) {
-      if (idx[s] == idx[s - 1]) {
-        ++run;
-      } else {
-        for (int v = 2; v <= run; ++v) rep *= v;
-        run = 1;
+    int rep = 1;
+    if (a.sector == 44) {
+      // multiset repeat factor: product of factorials of run lengths
+      int run = 1;
+      for (int s = 1; s < 4; ++s) {
+        if (idx[s] == idx[s - 1]) {
+          ++run;
+        } else {
+          for (int v = 2; v <= run; ++v) rep *= v;
+          run = 1;
+        }
       }
+      for (int v = 2; v <= run; ++v) rep *= v;
+    } else if (a.sector == 40) {
+      rep = (1 + (idx[0] == idx[1])) * (1 + (idx[2] == idx[3]));
+    } else {
+      rep = idx[0] == idx[2] ? 6 : ((idx[0] == idx[1] || idx[1] == idx[2]) ? 2 : 1);
     }
-    for (int v = 2; v <= run; ++v) rep *= v;
     const int ix = ((tx % a.nx) + a.nx) % a.nx, iy = ((ty % a.ny) + a.ny) % a.ny;  // any even size
     const size_t plane = (size_t)a.nx * a.ny;
     const size_t field = plane * a.n_cases;
     for (int cs = 0; cs < a.n_cases; ++cs) {
       const cplx* amp = a.amp + (size_t)cs * a.n_modes;
       cplx w = cscale(2.0, amp[idx[0]]);
-      w = cmul(cmul(cmul(w, amp[idx[1]]), amp[idx[2]]), amp[idx[3]]);
+      for (int s = 1; s < 4; ++s) {
+        const cplx as = amp[idx[s]];
+        w = cmul(w, sign[s] > 0 ? as : cmk(as.x, -as.y));
+      }
       w = cdiv_real(w, (double)rep);
       const size_t o = (size_t)cs * plane + (size_t)iy * a.nx + ix;
       const cplx vals[5] = {cmul(w, r.eta), cmul(w, r.psi), cmul(w, r.eta_c), cmul(w, r.psi_c),

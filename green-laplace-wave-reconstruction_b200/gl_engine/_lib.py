@@ -95,6 +95,10 @@ SIGNATURES = {
                                C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
     "gl_wit_read_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(WitStats)]),
+    "gl_wit_sector": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
+    "gl_wit_read_sector_stats": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.POINTER(WitStats)]),
     "gl_gauss_laguerre": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "gl_dispersion_solve": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.c_double, C.c_double,
                                       C.POINTER(C.c_double)]),

@@ -93,8 +93,8 @@ def read_dir4out(path) -> WitOutput:
     return WitOutput(fields=fields, stats=stats)
 
 
-def wit_eta44(inp: WitInput, *, device=None, as_numpy: bool = True) -> WitOutput:
-    """Sector-44 WIT fields of every amplitude case on one GPU."""
+def wit_sector(inp: WitInput, sector: int = 44, *, device=None, as_numpy: bool = True) -> WitOutput:
+    """WIT fourth-order fields of one sector (44, 40 or 42) for every amplitude case."""
     lib = _lib.load()
     dev = torch.device(device if device is not None else "cuda")
     modes = np.ascontiguousarray(inp.modes, dtype=np.int32).reshape(-1, 2)
@@ -106,14 +106,20 @@ def wit_eta44(inp: WitInput, *, device=None, as_numpy: bool = True) -> WitOutput
         out = torch.empty((5, cases, inp.ny, inp.nx), dtype=torch.complex128, device=dev)
         work = torch.empty(int(lib.gl_wit_workspace_size(m)) + 256, dtype=torch.uint8, device=dev)
         stream = torch.cuda.current_stream(dev).cuda_stream
-        _lib.check(lib.gl_wit_eta44(m, C.c_void_p(d_modes.data_ptr()), cases,
-                                    C.c_void_p(d_amp.data_ptr()), inp.nx, inp.ny, inp.gravity,
-                                    inp.depth, inp.dkx, inp.dky, inp.threshold,
-                                    C.c_void_p(out.data_ptr()), C.c_void_p(work.data_ptr()),
-                                    work.numel(), C.c_void_p(stream)))
+        _lib.check(lib.gl_wit_sector(int(sector), m, C.c_void_p(d_modes.data_ptr()), cases,
+                                     C.c_void_p(d_amp.data_ptr()), inp.nx, inp.ny, inp.gravity,
+                                     inp.depth, inp.dkx, inp.dky, inp.threshold,
+                                     C.c_void_p(out.data_ptr()), C.c_void_p(work.data_ptr()),
+                                     work.numel(), C.c_void_p(stream)))
         torch.cuda.current_stream(dev).synchronize()
         st = _lib.WitStats()
-        _lib.check(lib.gl_wit_read_stats(C.c_void_p(work.data_ptr()), m, C.byref(st)))
+        _lib.check(lib.gl_wit_read_sector_stats(int(sector), C.c_void_p(work.data_ptr()), m,
+                                                C.byref(st)))
     stats = {name: getattr(st, name) for name, _ in _lib.WitStats._fields_}
     data = out.cpu().numpy() if as_numpy else out
     return WitOutput(fields={name: data[k] for k, name in enumerate(FIELDS)}, stats=stats)
+
+
+def wit_eta44(inp: WitInput, *, device=None, as_numpy: bool = True) -> WitOutput:
+    """Sector-44 WIT fields of every amplitude case on one GPU."""
+    return wit_sector(inp, 44, device=device, as_numpy=as_numpy)

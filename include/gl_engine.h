@@ -198,6 +198,16 @@ gl_status gl_wit_eta44(int n_modes, const int* d_modes, int n_cases, const void*
                        void* stream);
 gl_status gl_wit_read_stats(const void* d_work, int n_modes, gl_wit_stats* out);
 
+/* Any sector of the same sum: 44 as above; 40 (unordered + pair x unordered
+ * - pair, analytic half-plane targets, weight 2 a a conj(a) conj(a)) and 42
+ * (unordered + triple x one - parent, weight 2 a a a conj(a)); lines 604-689
+ * of directional_eta4_openmp.cpp.  Statistics as gl_wit_read_stats. */
+gl_status gl_wit_sector(int sector, int n_modes, const int* d_modes, int n_cases,
+                        const void* d_amp, int nx, int ny, double gravity, double depth,
+                        double dkx, double dky, double threshold, void* d_out, void* d_work,
+                        size_t work_bytes, void* stream);
+gl_status gl_wit_read_sector_stats(int sector, const void* d_work, int n_modes, gl_wit_stats* out);
+
 /* Host FP64 Gauss--Laguerre rule (Golub--Welsch with the moment gate). */
 gl_status gl_gauss_laguerre(int rank, double* nodes, double* weights);
 

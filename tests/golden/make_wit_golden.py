@@ -43,12 +43,15 @@ def main(reference: Path) -> None:
         subprocess.run(["make", "-C", str(ROOT / "oracle"), f"REF={reference}"], check=True)
     out = {}
     with tempfile.TemporaryDirectory() as tmp:
-        for tag, (seed, m, n, cases) in {"small10": (1, 10, 32, 2), "small24": (2, 24, 64, 1)}.items():
+        cases_ = {"small10": (1, 10, 32, 2, 44), "small24": (2, 24, 64, 1, 44),
+                  "s40_small12": (3, 12, 32, 2, 40), "s42_small12": (4, 12, 32, 2, 42)}
+        for tag, (seed, m, n, cases, sector) in cases_.items():
             inp = small_case(seed, m, n, cases)
             fin, fout = Path(tmp) / f"{tag}.bin", Path(tmp) / f"{tag}.out"
             wit.write_dir4in(fin, inp)
-            subprocess.run([str(binary), str(fin), str(fout), "--sector", "44"], check=True,
-                           capture_output=True)
+            subprocess.run([str(binary), str(fin), str(fout), "--sector", str(sector)],
+                           check=True, capture_output=True)
+            out[f"{tag}/sector"] = np.array(sector)
             res = wit.read_dir4out(fout)
             out[f"{tag}/modes"] = inp.modes
             out[f"{tag}/amplitudes"] = inp.amplitudes
