@@ -1957,8 +1957,97 @@ extern "C" gl_status gl_eta44_plan_create(gl_plan** out, const gl_eta44_desc* de
   return GL_OK;
 }
 
-static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int layout,
-                                 void* outputs, void* ws, int* status, cudaStream_t st) {
+__global__ void plane_max_kernel(const cplx* x, int plane, unsigned long long* out) {
+  const int u = blockIdx.y;
+  double l = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
+    const double m = cabs_(x[(size_t)u * plane + i]);
+    l = (m > l || m != m) ? m : l;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double other = __shfl_xor_sync(0xffffffffu, l, o);
+    l = (other > l || other != other) ? other : l;
+  }
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out + u, l);
+}
+
+// Final roundoff floor of the summed order-4 spectra and transform to the
+// reference grid (gl_eta44_fftw.cpp:750-751).
+static gl_status e44_finalize(gl_plan* p, int gu, const cplx* OUT, unsigned long long* maxOUT,
+                              bool max_ready, void* outputs, char* tr, UnitScalars* us,
+                              int* status, cudaStream_t st) {
+  const int T = 256;
+  const Box B4 = p->b4;
+  const int pl4 = B4.w * B4.h;
+  gl_status s;
+  if (!max_ready) {
+    CUDA_TRY(cudaMemsetAsync(maxOUT, 0, (size_t)gu * 8, st));
+    dim3 g(grid_for(pl4, T, 64), gu);
+    {
+      LaunchScope ls_("plane_max_kernel", st, 0.0);
+      plane_max_kernel<<<g, T, 0, st>>>(OUT, pl4, maxOUT);
+    }
+    LAUNCH_CHECK("plane_max_kernel");
+  }
+  const int m1[1] = {M_ONE};
+  ColArgs a;
+  std::memset(&a, 0, sizeof a);
+  a.kind = COL_FLOORED;
+  a.nbanks = 1;
+  a.mult[0] = m1[0];
+  a.src_of[0] = 0;
+  a.box = B4;
+  a.geo = p->geo4;
+  a.spec = OUT;
+  a.spec_job_stride = pl4;
+  a.jobs_per_unit = 1;
+  a.floor_max = maxOUT;
+  a.floor_nsrc = 1;
+  a.floor_rel = p->floor_rel;
+  a.out = reinterpret_cast<cplx*>(tr);
+  a.n = p->d.ny;
+  a.log2n = p->lny;
+  a.scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
+  if ((s = launch_col_ifft(a, gu, st, p->tw)) != GL_OK) return s;
+  OutArgs o;
+  std::memset(&o, 0, sizeof o);
+  o.in = reinterpret_cast<cplx*>(tr);
+  o.w = B4.w;
+  o.x0 = B4.x0;
+  o.nx = p->d.nx;
+  o.log2nx = p->lnx;
+  o.ny = p->d.ny;
+  o.ncomp = 1;
+  o.comp_offset = 0;
+  o.out_ncomp = 1;
+  o.comp_scale = p->comp_scale;
+  o.out = outputs;
+  o.real_only = p->d.output == GL_OUT_REAL;
+  if ((s = launch_out_rows(o, gu, st, p->tw)) != GL_OK) return s;
+  if (us) {
+    const size_t per_unit = (size_t)p->d.nx * p->d.ny;
+    dim3 g(grid_for(per_unit, T, 256), gu);
+    {
+      LaunchScope ls_("nonfinite_kernel", st, 0.0);
+      nonfinite_kernel<<<g, T, 0, st>>>(outputs, per_unit, p->d.output == GL_OUT_REAL, us);
+    }
+    LAUNCH_CHECK("nonfinite_kernel");
+    if (status) {
+      {
+        LaunchScope ls_("status_kernel", st, 0.0);
+        status_kernel<<<(gu + 63) / 64, 64, 0, st>>>(us, gu, status);
+      }
+      LAUNCH_CHECK("status_kernel");
+    }
+  }
+  return GL_OK;
+}
+
+// One group of units over outer nodes [o0, o0 + Ro).  With `partial` set,
+// the accumulated order-4 spectra (before the final floor) are written there
+// and nothing else is produced; otherwise the fields are finished.
+static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, int o0, int Ro,
+                         cplx* partial, void* outputs, void* ws, int* status, cudaStream_t st) {
   const int T = 256, R = p->R44;
   const Box B1 = p->b1, B2 = p->b2, B3 = p->b3, B4 = p->b4;
   const int pl1 = B1.w * B1.h, pl2 = B2.w * B2.h, pl3 = B3.w * B3.h, pl4 = B4.w * B4.h;
@@ -1981,7 +2070,7 @@ static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int la
   unsigned long long* maxE = reinterpret_cast<unsigned long long*>(e44 + L.maxE);
   cplx* TS = reinterpret_cast<cplx*>(e44 + L.T);
   unsigned long long* maxT = reinterpret_cast<unsigned long long*>(e44 + L.maxT);
-  cplx* OUT = reinterpret_cast<cplx*>(e44 + L.OUT);
+  cplx* OUT = partial ? partial : reinterpret_cast<cplx*>(e44 + L.OUT);
   unsigned long long* maxOUT = reinterpret_cast<unsigned long long*>(e44 + L.maxOUT);
   char* tr = e44 + L.transient;
   const double* dn = p->nodes;  // nodes, then weights at +MAX_RANK
@@ -2088,7 +2177,7 @@ static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int la
   const double fwd_scale = ((double)p->d.nx * (double)p->d.ny) / ((double)p->ncx * (double)p->ncy);
   const double inv_scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
   const int ncy = p->ncy;
-  const int JP = R * R * R + R * R, GP = R * R + R;
+  const int JP = Ro * R * R + Ro * R, GP = Ro * R + Ro;
   CUDA_TRY(cudaMemsetAsync(maxE, 0, (size_t)gu * GP * 5 * 8, st));
   CUDA_TRY(cudaMemsetAsync(maxT, 0, (size_t)gu * R * 3 * 8, st));
   CUDA_TRY(cudaMemsetAsync(maxOUT, 0, (size_t)gu * 8, st));
@@ -2113,6 +2202,8 @@ static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int la
     a.us = us;
     a.nodes = dn;
     a.n_inner = R;
+    a.n_outer = Ro;
+    a.outer0 = o0;
     a.floor_rel = p->floor_rel;
     a.out = outp;
     a.n = ncy;
@@ -2152,7 +2243,7 @@ static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int la
     return launch_col_fft(f, njs, st, p->tw);
   };
 
-  // ---- stage 1: every pair level (R^3 third-level + R^2 order-4 pair jobs)
+  // ---- stage 1: every pair level (Ro R^2 third-level + Ro R order-4 pair jobs)
   {
     const int nj = gu * JP;
     Bump b;
@@ -2181,6 +2272,9 @@ static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int la
     c.weights = dn + MAX_RANK;
     c.R = R;
     c.groups_per_unit = GP;
+    c.jobs_per_unit = JP;
+    c.Ro = Ro;
+    c.outer0 = o0;
     c.floor_rel = p->floor_rel;
     dim3 g(grid_for(pl2, T, 64), gu * GP);
     {
@@ -2189,9 +2283,9 @@ static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int la
     }
     LAUNCH_CHECK("acc_e44_pair_kernel");
   }
-  // ---- stage 2: third level (R^2 jobs per unit)
+  // ---- stage 2: third level (Ro R jobs per unit)
   {
-    const int nj = gu * R * R;
+    const int nj = gu * Ro * R;
     Bump b;
     cplx* PF = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 16 * B1.w * ncy * sizeof(cplx)));
     cplx* PP = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 15 * B2.w * ncy * sizeof(cplx)));
@@ -2199,24 +2293,24 @@ static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int la
     cplx* R3 = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 4 * pl3 * sizeof(cplx)));
     unsigned long long* mR3 = reinterpret_cast<unsigned long long*>(tr + b.take((size_t)nj * 4 * 8));
     CUDA_TRY(cudaMemsetAsync(mR3, 0, (size_t)nj * 4 * 8, st));
-    ColArgs a = colargs(COL_E44_FIRST3, 16, E44_FIRST_MULT, nullptr, B1, p->geo1, spec, pl1, 0, R * R, PF);
+    ColArgs a = colargs(COL_E44_FIRST3, 16, E44_FIRST_MULT, nullptr, B1, p->geo1, spec, pl1, 0, Ro * R, PF);
     if ((s = launch_col_ifft(a, nj, st, p->tw)) != GL_OK) return s;
-    // pair outputs of third-level groups: group g = o R + t of unit u sits at E[u GP + g]
-    // and job (u, o, t) = u R^2 + o R + t, so job -> group index u GP + (job mod R^2).
+    // pair outputs of third-level groups: group g = ol R + t of unit u sits at
+    // E[u GP + g] and job (u, ol, t) = u Ro R + ol R + t.
     for (int u = 0; u < gu; ++u) {
       ColArgs a2 = colargs(COL_FLOORED, 15, E44_POUT_MULT, E44_POUT_SRC, B2, p->geo2,
-                           E + (size_t)u * GP * 5 * pl2, 5LL * pl2, pl2, R * R,
-                           PP + (size_t)u * R * R * 15 * B2.w * ncy);
+                           E + (size_t)u * GP * 5 * pl2, 5LL * pl2, pl2, Ro * R,
+                           PP + (size_t)u * Ro * R * 15 * B2.w * ncy);
       a2.floor_max = maxE + (size_t)u * GP * 5;
       a2.floor_nsrc = 5;
-      if ((s = launch_col_ifft(a2, R * R, st, p->tw)) != GL_OK) return s;
+      if ((s = launch_col_ifft(a2, Ro * R, st, p->tw)) != GL_OK) return s;
     }
     RowArgs r = rowargs(ROW_E44_THIRD, 4, B3, Q);
     r.grp[0] = BankGroup{PF, 16, B1.x0, B1.w};
     r.grp[1] = BankGroup{PP, 15, B2.x0, B2.w};
     r.ngrp = 2;
     if ((s = launch_row(r, nj, st, p->tw)) != GL_OK) return s;
-    if ((s = colfft(Q, R3, B3, 4, s3, mR3, R * R, nj * 4)) != GL_OK) return s;
+    if ((s = colfft(Q, R3, B3, 4, s3, mR3, Ro * R, nj * 4)) != GL_OK) return s;
     E44Acc c;
     std::memset(&c, 0, sizeof c);
     c.us = us;
@@ -2229,18 +2323,20 @@ static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int la
     c.nodes = dn;
     c.weights = dn + MAX_RANK;
     c.R = R;
-    c.groups_per_unit = R;
+    c.groups_per_unit = Ro;
+    c.Ro = Ro;
+    c.outer0 = o0;
     c.floor_rel = p->floor_rel;
-    dim3 g(grid_for(pl3, T, 64), gu * R);
+    dim3 g(grid_for(pl3, T, 64), gu * Ro);
     {
       LaunchScope ls_("acc_e44_third_kernel", st, 0.0);
       acc_e44_third_kernel<<<g, T, 0, st>>>(c);
     }
     LAUNCH_CHECK("acc_e44_third_kernel");
   }
-  // ---- stage 3: order-4 forcing (R jobs per unit)
+  // ---- stage 3: order-4 forcing (Ro jobs per unit)
   {
-    const int nj = gu * R;
+    const int nj = gu * Ro;
     Bump b;
     cplx* PF = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 19 * B1.w * ncy * sizeof(cplx)));
     cplx* PP = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 18 * B2.w * ncy * sizeof(cplx)));
@@ -2249,18 +2345,18 @@ static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int la
     cplx* R4 = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 2 * pl4 * sizeof(cplx)));
     unsigned long long* mR4 = reinterpret_cast<unsigned long long*>(tr + b.take((size_t)nj * 2 * 8));
     CUDA_TRY(cudaMemsetAsync(mR4, 0, (size_t)nj * 2 * 8, st));
-    ColArgs a = colargs(COL_E44_FIRST4, 19, E44_FIRST_MULT, nullptr, B1, p->geo1, spec, pl1, 0, R, PF);
+    ColArgs a = colargs(COL_E44_FIRST4, 19, E44_FIRST_MULT, nullptr, B1, p->geo1, spec, pl1, 0, Ro, PF);
     if ((s = launch_col_ifft(a, nj, st, p->tw)) != GL_OK) return s;
     for (int u = 0; u < gu; ++u) {
       ColArgs a2 = colargs(COL_FLOORED, 18, E44_POUT_MULT, E44_POUT_SRC, B2, p->geo2,
-                           E + ((size_t)u * GP + R * R) * 5 * pl2, 5LL * pl2, pl2, R,
-                           PP + (size_t)u * R * 18 * B2.w * ncy);
-      a2.floor_max = maxE + ((size_t)u * GP + R * R) * 5;
+                           E + ((size_t)u * GP + Ro * R) * 5 * pl2, 5LL * pl2, pl2, Ro,
+                           PP + (size_t)u * Ro * 18 * B2.w * ncy);
+      a2.floor_max = maxE + ((size_t)u * GP + Ro * R) * 5;
       a2.floor_nsrc = 5;
-      if ((s = launch_col_ifft(a2, R, st, p->tw)) != GL_OK) return s;
+      if ((s = launch_col_ifft(a2, Ro, st, p->tw)) != GL_OK) return s;
     }
     ColArgs a3 = colargs(COL_FLOORED, 8, E44_TOUT_MULT, E44_TOUT_SRC, B3, p->geo3, TS, 3LL * pl3, pl3,
-                         R, PT);
+                         Ro, PT);
     a3.floor_max = maxT;
     a3.floor_nsrc = 3;
     if ((s = launch_col_ifft(a3, nj, st, p->tw)) != GL_OK) return s;
@@ -2270,7 +2366,7 @@ static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int la
     r.grp[2] = BankGroup{PT, 8, B3.x0, B3.w};
     r.ngrp = 3;
     if ((s = launch_row(r, nj, st, p->tw)) != GL_OK) return s;
-    if ((s = colfft(Q, R4, B4, 2, s4, mR4, R, nj * 2)) != GL_OK) return s;
+    if ((s = colfft(Q, R4, B4, 2, s4, mR4, Ro, nj * 2)) != GL_OK) return s;
     E44Acc c;
     std::memset(&c, 0, sizeof c);
     c.us = us;
@@ -2284,6 +2380,8 @@ static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int la
     c.weights = dn + MAX_RANK;
     c.R = R;
     c.groups_per_unit = 1;
+    c.Ro = Ro;
+    c.outer0 = o0;
     c.floor_rel = p->floor_rel;
     dim3 g(grid_for(pl4, T, 64), gu);
     {
@@ -2292,46 +2390,68 @@ static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int la
     }
     LAUNCH_CHECK("acc_e44_order4_kernel");
   }
-  // ---- final transform on the reference grid, with the last roundoff floor
-  {
-    const int m1[1] = {M_ONE}, z1[1] = {0};
-    ColArgs a = colargs(COL_FLOORED, 1, m1, z1, B4, p->geo4, OUT, pl4, 0, 1, reinterpret_cast<cplx*>(tr));
-    a.floor_max = maxOUT;
-    a.floor_nsrc = 1;
-    a.n = p->d.ny;
-    a.log2n = p->lny;
-    if ((s = launch_col_ifft(a, gu, st, p->tw)) != GL_OK) return s;
-    OutArgs o;
-    std::memset(&o, 0, sizeof o);
-    o.in = reinterpret_cast<cplx*>(tr);
-    o.w = B4.w;
-    o.x0 = B4.x0;
-    o.nx = p->d.nx;
-    o.log2nx = p->lnx;
-    o.ny = p->d.ny;
-    o.ncomp = 1;
-    o.comp_offset = 0;
-    o.out_ncomp = 1;
-    o.comp_scale = p->comp_scale;
-    o.out = outputs;
-    o.real_only = p->d.output == GL_OUT_REAL;
-    if ((s = launch_out_rows(o, gu, st, p->tw)) != GL_OK) return s;
-  }
-  {
-    const size_t per_unit = (size_t)p->d.nx * p->d.ny;
-    dim3 g(grid_for(per_unit, T, 256), gu);
-    {
-      LaunchScope ls_("nonfinite_kernel", st, 0.0);
-      nonfinite_kernel<<<g, T, 0, st>>>(outputs, per_unit, p->d.output == GL_OUT_REAL, us);
+  if (partial) return GL_OK;
+  return e44_finalize(p, gu, OUT, maxOUT, true, outputs, tr, us, status, st);
+}
+
+static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int layout,
+                                 void* outputs, void* ws, int* status, cudaStream_t st) {
+  return e44_run(p, gu, spectra, layout, 0, p->R44, nullptr, outputs, ws, status, st);
+  return GL_OK;
+}
+
+extern "C" gl_status gl_eta44_execute_partial(gl_plan* p, int n_units, const void* d_spectra,
+                                              int layout, int outer_begin, int outer_end,
+                                              void* d_partial, void* d_ws, size_t ws_bytes,
+                                              int* d_status, void* stream) {
+  if (!p || !p->e44) return fail(GL_ERR_INVALID_ARGUMENT, "not an eta44 plan");
+  if (n_units < 0 || !d_spectra || !d_partial) return fail(GL_ERR_INVALID_ARGUMENT, "bad arguments");
+  if (outer_begin < 0 || outer_end > p->R44 || outer_begin >= outer_end)
+    return fail(GL_ERR_INVALID_ARGUMENT, "outer node range must lie in [0, rank)");
+  if (layout != GL_SPECTRA_FULL && layout != GL_SPECTRA_BOX)
+    return fail(GL_ERR_INVALID_ARGUMENT, "unknown spectra layout");
+  if (!d_ws || ws_bytes < p->ws_total || (reinterpret_cast<uintptr_t>(d_ws) & 255))
+    return fail(GL_ERR_WORKSPACE, "workspace must be 256-byte aligned and at least %zu bytes", p->ws_total);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const size_t in_unit = layout == GL_SPECTRA_FULL ? (size_t)p->d.nx * p->d.ny : (size_t)p->b1.w * p->b1.h;
+  const size_t part_unit = (size_t)p->b4.w * p->b4.h;
+  for (int u0 = 0; u0 < n_units; u0 += p->group) {
+    const int gu = std::min(p->group, n_units - u0);
+    gl_status s = e44_run(p, gu, reinterpret_cast<const cplx*>(d_spectra) + (size_t)u0 * in_unit, layout,
+                          outer_begin, outer_end - outer_begin,
+                          reinterpret_cast<cplx*>(d_partial) + (size_t)u0 * part_unit, nullptr, d_ws,
+                          d_status ? d_status + u0 : nullptr, st);
+    if (s != GL_OK) return s;
+    if (d_status) {
+      UnitScalars* us = at<UnitScalars>(d_ws, p->o_us);
+      {
+        LaunchScope ls_("status_kernel", st, 0.0);
+        status_kernel<<<(gu + 63) / 64, 64, 0, st>>>(us, gu, d_status + u0);
+      }
+      LAUNCH_CHECK("status_kernel");
     }
-    LAUNCH_CHECK("nonfinite_kernel");
   }
-  if (status) {
-    {
-      LaunchScope ls_("status_kernel", st, 0.0);
-      status_kernel<<<(gu + 63) / 64, 64, 0, st>>>(us, gu, status);
-    }
-    LAUNCH_CHECK("status_kernel");
+  return GL_OK;
+}
+
+extern "C" gl_status gl_eta44_finalize(gl_plan* p, int n_units, const void* d_partial_sum,
+                                       void* d_outputs, void* d_ws, size_t ws_bytes, void* stream) {
+  if (!p || !p->e44) return fail(GL_ERR_INVALID_ARGUMENT, "not an eta44 plan");
+  if (n_units < 0 || !d_partial_sum || !d_outputs) return fail(GL_ERR_INVALID_ARGUMENT, "bad arguments");
+  if (!d_ws || ws_bytes < p->ws_total || (reinterpret_cast<uintptr_t>(d_ws) & 255))
+    return fail(GL_ERR_WORKSPACE, "workspace must be 256-byte aligned and at least %zu bytes", p->ws_total);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  char* e44 = at<char>(d_ws, p->o_e44);
+  const E44Layout L = e44_layout(p, p->group);
+  unsigned long long* maxOUT = reinterpret_cast<unsigned long long*>(e44 + L.maxOUT);
+  const size_t part_unit = (size_t)p->b4.w * p->b4.h;
+  const size_t out_unit = (size_t)p->d.nx * p->d.ny * (p->d.output == GL_OUT_REAL ? sizeof(double) : sizeof(cplx));
+  for (int u0 = 0; u0 < n_units; u0 += p->group) {
+    const int gu = std::min(p->group, n_units - u0);
+    gl_status s = e44_finalize(p, gu, reinterpret_cast<const cplx*>(d_partial_sum) + (size_t)u0 * part_unit,
+                               maxOUT, false, reinterpret_cast<char*>(d_outputs) + u0 * out_unit,
+                               e44 + L.transient, nullptr, nullptr, st);
+    if (s != GL_OK) return s;
   }
   return GL_OK;
 }

@@ -24,7 +24,9 @@ struct E44Acc {
   const double* nodes;
   const double* weights;
   int R;
-  int groups_per_unit;      // pair stage: R^2 + R; third stage: R
+  int groups_per_unit;      // pair stage: Ro R + Ro; third stage: Ro
+  int jobs_per_unit;        // pair stage: Ro R^2 + Ro R
+  int Ro, outer0;           // outer nodes handled by this call, first one
   double floor_rel;
 };
 
@@ -50,7 +52,7 @@ __global__ void acc_e44_pair_kernel(E44Acc a) {
   const int unit = grp / a.groups_per_unit;
   const int g = grp % a.groups_per_unit;
   const int R = a.R;
-  const int jobs_per_unit = R * R * R + R * R;
+  const int jobs_per_unit = a.jobs_per_unit;
   const int plane = a.box.w * a.box.h;
   const UnitScalars& u = a.us[unit];
   double lm[5] = {0, 0, 0, 0, 0};
@@ -86,8 +88,8 @@ __global__ void acc_e44_pair_kernel(E44Acc a) {
 
 // Third level: es, ps, pts of one outer node (gl_eta44_fftw.cpp:571-584).
 __global__ void acc_e44_third_kernel(E44Acc a) {
-  const int uo = blockIdx.y;  // unit * R + o
-  const int unit = uo / a.R;
+  const int uo = blockIdx.y;  // unit * Ro + local outer node
+  const int unit = uo / a.Ro;
   const int R = a.R;
   const int plane = a.box.w * a.box.h;
   const UnitScalars& u = a.us[unit];
@@ -123,7 +125,6 @@ __global__ void acc_e44_third_kernel(E44Acc a) {
 // Order 4: the eta44 spectrum of one unit (gl_eta44_fftw.cpp:736-748).
 __global__ void acc_e44_order4_kernel(E44Acc a) {
   const int unit = blockIdx.y;
-  const int R = a.R;
   const int plane = a.box.w * a.box.h;
   const UnitScalars& u = a.us[unit];
   double lm[1] = {0};
@@ -131,9 +132,9 @@ __global__ void acc_e44_order4_kernel(E44Acc a) {
     const GeoRef G{a.geo, plane, i};
     const double A = G.a(), sqa = __ldg(a.geo + 5 * plane + i);
     cplx acc = czero();
-    for (int o = 0; o < R; ++o) {
-      const int job = unit * R + o;
-      const double x = a.nodes[o], w = a.weights[o];
+    for (int ol = 0; ol < a.Ro; ++ol) {
+      const int job = unit * a.Ro + ol;
+      const double x = a.nodes[a.outer0 + ol], w = a.weights[a.outer0 + ol];
       const double tm = x / u.lam4;
       const double co = w * exp(x) / u.lam4 * exp(-4.0 * u.shift4 * tm);
       const double sh = sinh_over_root(sqa, tm), ch = cosh(sqa * tm);

@@ -173,7 +173,8 @@ struct ColArgs {
   const double* nodes;     // GL nodes (outer for OUTER*, eta22 for ETA22)
   const double* nodes2;    // inner nodes
   int n_inner;             // inner rank (COL_INNER) / nodes per branch (PSI22)
-  int n_outer;
+  int n_outer;             // outer rank; eta44: outer nodes handled by this call
+  int outer0;              // eta44: first outer node handled by this call
   const unsigned char* chan_mask;  // [unit][2][h][w] (COL_PSI22)
   const unsigned long long* floor_max;  // per-job max for floored spectra
   int floor_nsrc;          // COL_FLOORED: maxima per job (indexed job * floor_nsrc + src)
@@ -224,15 +225,16 @@ GL_D cplx col_base(const ColArgs& a, int job, int i, double nu) {
       return cscale(exp(-tau3 * (nu - u.shift3)), v);
     }
     case COL_E44_PAIR: {
-      const int R = a.n_inner;
-      const int r3 = R * R * R;
+      // local outer nodes ol = 0..n_outer-1 map to global o = outer0 + ol
+      const int R = a.n_inner, Ro = a.n_outer;
+      const int r3 = Ro * R * R;
       int o, t = -1, pn;
       if (sub < r3) {
-        o = sub / (R * R);
+        o = a.outer0 + sub / (R * R);
         t = (sub / R) % R;
         pn = sub % R;
       } else {
-        o = (sub - r3) / R;
+        o = a.outer0 + (sub - r3) / R;
         pn = (sub - r3) % R;
       }
       cplx d = cscale(exp(-(a.nodes[o] / u.lam4) * (nu - u.shift4)), v);
@@ -241,12 +243,12 @@ GL_D cplx col_base(const ColArgs& a, int job, int i, double nu) {
     }
     case COL_E44_FIRST3: {
       const int R = a.n_inner;
-      const int o = sub / R, t = sub % R;
+      const int o = a.outer0 + sub / R, t = sub % R;
       const cplx d = cscale(exp(-(a.nodes[o] / u.lam4) * (nu - u.shift4)), v);
       return cscale(exp(-(a.nodes[t] / u.lam3) * (nu - u.shift3)), d);
     }
     case COL_E44_FIRST4:
-      return cscale(exp(-(a.nodes[sub] / u.lam4) * (nu - u.shift4)), v);
+      return cscale(exp(-(a.nodes[a.outer0 + sub] / u.lam4) * (nu - u.shift4)), v);
   }
   return v;
 }

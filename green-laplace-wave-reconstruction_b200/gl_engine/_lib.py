@@ -80,6 +80,11 @@ SIGNATURES = {
     "gl_plan_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(PlanDesc)]),
     "gl_plan_destroy": (None, [C.c_void_p]),
     "gl_eta44_plan_create": (C.c_int, [C.POINTER(C.c_void_p), C.POINTER(Eta44Desc)]),
+    "gl_eta44_execute_partial": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                           C.c_int, C.c_void_p, C.c_void_p, C.c_size_t,
+                                           C.c_void_p, C.c_void_p]),
+    "gl_eta44_finalize": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_size_t, C.c_void_p]),
     "gl_plan_get_info": (C.c_int, [C.c_void_p, C.POINTER(PlanInfo)]),
     "gl_workspace_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "gl_deposit_modes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,

@@ -130,6 +130,21 @@ typedef struct gl_eta44_desc {
 
 gl_status gl_eta44_plan_create(gl_plan** plan, const gl_eta44_desc* desc);
 
+/* Outer-node sharding of an eta44 plan (the device analogue of the reference's
+ * process split, paper/order4/run_gl_split.sh:31-38 + merge_eta44_outer.cpp:12).
+ * gl_eta44_execute_partial accumulates the order-4 spectra of outer nodes
+ * [outer_begin, outer_end) into d_partial ([unit][box4_h][box4_w] complex128,
+ * box4 = 4 x the parent box), before the final roundoff floor; summing the
+ * partials of a partition of [0, rank) (one NCCL all-reduce across GPUs) and
+ * calling gl_eta44_finalize gives the monolithic result. */
+gl_status gl_eta44_execute_partial(gl_plan* plan, int n_units, const void* d_spectra,
+                                   int spectra_layout, int outer_begin, int outer_end,
+                                   void* d_partial, void* d_workspace, size_t workspace_bytes,
+                                   int* d_unit_status, void* stream);
+gl_status gl_eta44_finalize(gl_plan* plan, int n_units, const void* d_partial_sum,
+                            void* d_outputs, void* d_workspace, size_t workspace_bytes,
+                            void* stream);
+
 /* Device workspace bytes needed by gl_execute (independent of n_units). */
 gl_status gl_workspace_size(const gl_plan* plan, size_t* bytes);
 

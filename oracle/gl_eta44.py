@@ -267,6 +267,31 @@ def eta44(spectrum, dk, depth, peak, nodes, weights, outer_subset=None):
     return _ifft(out)
 
 
+def eta44_partial(spectrum, dk, depth, peak, nodes, weights, outer_subset):
+    """Order-4 spectrum accumulated over ``outer_subset`` only, before the final
+    floor (the quantity one GPU contributes when outer nodes are sharded)."""
+    g = Grid(spectrum, dk, depth, peak, nodes, weights)
+    out = np.zeros_like(spectrum)
+    for oi, (x, w) in enumerate(zip(g.nodes, g.weights)):
+        if oi not in outer_subset:
+            continue
+        tm = x / g.l4
+        damp = spectrum * np.exp(-tm * (g.nu - g.shift4))
+        t = third(g, damp)
+        f = first(g, damp, True)
+        p = pair(g, damp, True)
+        fk, fd = (zero_suppress(_fft(a), g.m4) for a in order4_forcing(f, p, t))
+        co = w * np.exp(x) / g.l4 * np.exp(-4 * g.shift4 * tm)
+        sh, ch = g.sh_ch(tm)
+        out = out + co * (g.A * sh * fd - 1j * ch * fk)
+    return out, g.m4
+
+
+def eta44_finalize(out_sum, quartic_mask):
+    """Final floor and inverse transform of a summed order-4 spectrum."""
+    return _ifft(zero_suppress(out_sum, quartic_mask))
+
+
 def spectrum_from_wit_input(modes, amplitude, n, depth):
     """Deposit s = n^2 c / h at (my, mx) (``paper/order4/prepare_order4_inputs.m:12-16``)."""
     s = np.zeros((n, n), dtype=complex)
