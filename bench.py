@@ -364,6 +364,56 @@ def run_engine(args, rank: int, world: int, local_rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_config3(args, rank: int, world: int, local_rank: int) -> None:
+    """The uneven batch (64 sea states, grids 128..1024^2, orders 2-3, ranks
+    2..8, 8 snapshots each) replayed as one captured CUDA graph, against the
+    same batch launched eagerly.  Units = (sea state, snapshot) pairs."""
+    import torch
+
+    from gl_engine import _lib, batch
+
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    items = batch.config3_items(n_states=args.states, snapshots=8, seed0=rank * args.states)
+    runner = batch.BatchRunner(items, device=device)
+    runner.capture()
+    for _ in range(max(args.warmup, 1)):
+        runner.replay()
+    torch.cuda.synchronize()
+    runner.check()
+    stream = torch.cuda.current_stream(device)
+
+    def timed(fn):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+        for k in range(args.steps):
+            ev[k][0].record(stream)
+            fn()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in ev) / 1e3
+
+    launches0 = _lib.launch_count()
+    eager_s = timed(runner.run_eager)
+    launches = (_lib.launch_count() - launches0) // max(args.steps, 1)
+    graph_s = timed(runner.replay)
+    units = runner.units
+    grids = sorted({it.nx for it in items})
+    line = {
+        "metric": "config-3 uneven batch units/s (captured graph)", "value": units * args.steps / graph_s,
+        "unit": "units/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * graph_s / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded JONSWAP sea states)",
+        "config": {"workload": f"{len(items)} sea states x 8 snapshots, grids {grids}, orders 2-3, "
+                               "ranks 2-8, h U[10,100] m, Hs U[1,4] m, 200 modes, FP64",
+                   "units_per_step_per_gpu": units},
+        "eager": {"value": units * args.steps / eager_s, "ms_per_step": 1e3 * eager_s / args.steps,
+                  "kernel_launches_per_step": int(launches)},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -374,6 +424,9 @@ def main() -> None:
     ap.add_argument("--group", type=int, default=0, help="units per engine launch group")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["config2", "config3"], default="config2",
+                    help="config2: the headline order-3 1024^2 workload; config3: uneven batch")
+    ap.add_argument("--states", type=int, default=64, help="config3: sea states per GPU")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -391,7 +444,10 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        run_engine(args, rank, world, local_rank)
+        if args.workload == "config3":
+            run_config3(args, rank, world, local_rank)
+        else:
+            run_engine(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

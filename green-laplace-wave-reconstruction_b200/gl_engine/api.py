@@ -202,8 +202,15 @@ class Plan:
             size = C.c_size_t()
             _engine_call(self.lib.gl_workspace_size(handle, C.byref(size)))
             self.workspace_bytes = int(size.value)
-            self.workspace = torch.empty(max(self.workspace_bytes, 256) + 256, dtype=torch.uint8,
-                                         device=device)
+            self._workspace = None
+
+    @property
+    def workspace(self) -> torch.Tensor:
+        """Device workspace, allocated on first use (batches pass a shared one)."""
+        if self._workspace is None:
+            self._workspace = torch.empty(max(self.workspace_bytes, 256) + 256, dtype=torch.uint8,
+                                          device=self.device)
+        return self._workspace
 
     @property
     def component_ids(self) -> list[int]:
@@ -354,11 +361,13 @@ def surface_batch_device(coeffs: GLCoefficients, Lx, Ly, Nx, Ny, times, *,
                          components: Sequence[str] | None = None, output: str = "complex",
                          grid: str = "compact", device=None, max_units: int | None = None,
                          check: bool = True, stream: torch.cuda.Stream | None = None,
-                         out: torch.Tensor | None = None) -> SurfaceBatch:
+                         out: torch.Tensor | None = None, order3_ranks=(4, 4)) -> SurfaceBatch:
     """Evaluate ``len(times)`` snapshots of one sea state on the GPU.
 
     Inputs are host arrays; outputs stay on the device.  ``components``
-    selects a subset of eta11..psi33 (default: all of the coefficients' order).
+    selects a subset of eta11..psi33 (default: all of the coefficients' order);
+    ``order3_ranks`` = (inner, outer) GL ranks of the order-3 graph (the
+    reference's unified API fixes GL4/GL4, ``_order3.py:23-26``).
     """
     if not isinstance(coeffs, GLCoefficients) or coeffs.api != API_NAME:
         raise GLError("green_laplace:Coefficients", "Input must come from gl_spectral_coefficients.")
@@ -383,7 +392,8 @@ def surface_batch_device(coeffs: GLCoefficients, Lx, Ly, Nx, Ny, times, *,
                     eta22_rank=int(coeffs.options["eta22_rank"]),
                     allow_below=coeffs.options["allow_below_model_parent_domain"], box=dep.box,
                     grid=GRID_REFERENCE if grid == "reference" else GRID_COMPACT,
-                    max_units=max_units or min(n, 8), output=out_mode, device=device)
+                    max_units=max_units or min(n, 8), output=out_mode, device=device,
+                    inner_rank=int(order3_ranks[0]), outer_rank=int(order3_ranks[1]))
     stream = stream or torch.cuda.current_stream(device)
     with torch.cuda.device(device), torch.cuda.stream(stream):
         def h2d(arr, dtype):

@@ -124,7 +124,7 @@ class Eta44Plan(Plan):
             size = C.c_size_t()
             _engine_call(self.lib.gl_workspace_size(handle, C.byref(size)))
             self.workspace_bytes = int(size.value)
-            self.workspace = torch.empty(self.workspace_bytes + 256, dtype=torch.uint8, device=device)
+            self._workspace = None
 
 
 def eta44(spectra, *, dk: float, depth: float, peak_depth: float, rank: int, nodes=None,

@@ -1,0 +1,57 @@
+"""Uneven batches captured as one CUDA graph: replay equals eager execution
+and the per-sea-state API, bit for bit."""
+
+import numpy as np
+import pytest
+import torch
+
+import gl_engine
+from gl_engine import api, batch, seastate
+
+pytestmark = pytest.mark.gpu
+
+
+def _items():
+    items = []
+    rng = np.random.default_rng(5)
+    for k, (n, order, rank) in enumerate([(64, 2, 2), (128, 3, 4), (64, 3, 6), (128, 2, 8)]):
+        st = seastate.jonswap_sea_state(n=n, length=2.0 * n, depth=float(rng.uniform(10, 60)),
+                                        hs=2.0, tp=8.0, modes=30, seed=k, order=order)
+        c = gl_engine.gl_spectral_coefficients(order, st.gravity, st.depth, st.a, st.b, st.kx,
+                                               st.ky, 0, 0, {"eta22_rank": rank})
+        r3 = rank if rank in (4, 6, 8) else 4
+        comps = ("eta22", "psi22") if order == 2 else ("eta33", "psi33")
+        items.append(batch.BatchItem(coeffs=c, lx=st.lx, ly=st.ly, nx=n, ny=n,
+                                     times=rng.uniform(0, 60, 3), components=comps,
+                                     inner_rank=r3, outer_rank=r3))
+    return items
+
+
+def test_graph_replay_equals_eager_and_single_calls():
+    items = _items()
+    runner = batch.BatchRunner(items)
+    runner.run_eager()
+    torch.cuda.synchronize()
+    runner.check()
+    eager = [t.clone() for _, _, t in runner.outputs()]
+    runner.capture()
+    for t in runner.outputs():
+        t[2].zero_()
+    runner.replay()
+    torch.cuda.synchronize()
+    runner.check()
+    for (it, names, got), want in zip(runner.outputs(), eager):
+        assert torch.equal(got, want)
+        one = api.surface_batch_device(it.coeffs, it.lx, it.ly, it.nx, it.ny, it.times,
+                                       components=list(it.components), output="real",
+                                       max_units=len(it.times),
+                                       order3_ranks=(it.inner_rank, it.outer_rank))
+        assert one.names == names
+        assert torch.equal(one.fields, got)
+
+
+def test_autotuner_picks_a_candidate():
+    item = _items()[1]
+    g = batch.autotune_group(item, candidates=(1, 3))
+    assert g in (1, 3)
+    assert batch.autotune_group(item, candidates=(1, 3)) == g  # cached
