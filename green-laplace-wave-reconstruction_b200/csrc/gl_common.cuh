@@ -29,6 +29,7 @@ GL_HD cplx cmuli(cplx a) { return cmk(-a.y, a.x); }
 GL_HD cplx cmulmi(cplx a) { return cmk(a.y, -a.x); }
 GL_HD cplx csq(cplx a) { return cmul(a, a); }
 GL_HD cplx czero() { return cmk(0.0, 0.0); }
+GL_HD cplx cconj(cplx a) { return cmk(a.x, -a.y); }
 
 // |z| as numpy computes it (hypot).
 GL_D double cabs_(cplx a) { return hypot(a.x, a.y); }

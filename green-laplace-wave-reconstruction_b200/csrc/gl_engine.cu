@@ -16,6 +16,7 @@
 #include "gl_kernels.cuh"
 #include "gl_wit.cuh"
 #include "gl_eta44.cuh"
+#include "gl_adjoint.cuh"
 
 using namespace gl;
 
@@ -1012,7 +1013,8 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
   const size_t smem = row_smem(nb, a.nx);
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    cudaFuncSetAttribute(row_kernel_t<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    cudaFuncSetAttribute(row_kernel_t<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
     attr = true;
   }
   dim3 grid(a.ny, njobs);
@@ -1022,9 +1024,19 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
   const int threads = std::max(32, std::min(256, (nb <= 12 ? 8 : 16) * (a.nx / 16)));
   double bytes = (double)njobs * a.nout * a.out_w * a.ny * sizeof(cplx);
   for (int g = 0; g < a.ngrp; ++g) bytes += (double)njobs * a.grp[g].nb * a.grp[g].w * a.ny * sizeof(cplx);
-  LaunchScope ls(a.kind == ROW_INNER ? "row_kernel[inner]" : a.kind == ROW_OUTER ? "row_kernel[outer]"
-                 : "row_kernel[order2]", st, bytes);
-  row_kernel<<<grid, threads, smem, st>>>(a, tw);
+  const bool adj = a.kind >= ROW_ADJ_ETA22;
+  const char* name = a.kind == ROW_INNER         ? "row_kernel[inner]"
+                     : a.kind == ROW_OUTER       ? "row_kernel[outer]"
+                     : a.kind == ROW_ADJ_INNER   ? "row_kernel[adj_inner]"
+                     : a.kind == ROW_ADJ_OUTER   ? "row_kernel[adj_outer]"
+                     : a.kind == ROW_ADJ_ETA22   ? "row_kernel[adj_eta22]"
+                     : a.kind >= ROW_E44_PAIR    ? "row_kernel[order4]"
+                                                 : "row_kernel[order2]";
+  LaunchScope ls(name, st, bytes);
+  if (adj)
+    row_kernel_t<1><<<grid, threads, smem, st>>>(a, tw);
+  else
+    row_kernel_t<0><<<grid, threads, smem, st>>>(a, tw);
   LAUNCH_CHECK("row_kernel");
   return GL_OK;
 }
@@ -1147,9 +1159,12 @@ static int comp_slot(const gl_plan* p, int id) {
 static gl_status run_group_eta44(gl_plan* p, int gu, const void* spectra, int layout,
                                  void* outputs, void* ws, int* status, cudaStream_t st);
 
-static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, void* outputs,
-                           void* ws, int* status, cudaStream_t st) {
-  if (p->e44) return run_group_eta44(p, gu, spectra, layout, outputs, ws, status, st);
+// Support analysis of a group of units (spatial.py:160-189, _order3.py:33-52):
+// the parent box spectra (extracted from full spectra when needed), the
+// supports S, S2 = S+S, S3 = S2+S, the psi22 radial channels and the per-unit
+// scalars.  The box spectra pointer is returned in *spec_out.
+static gl_status analyse_group(gl_plan* p, int gu, const void* spectra, int layout, void* ws,
+                               cudaStream_t st, const cplx** spec_out) {
   const int T = 256;
   const Box B1 = p->b1, B2 = p->b2, B3 = p->b3;
   const int pl1 = B1.w * B1.h, pl2 = B2.w * B2.h, pl3 = B3.w * B3.h;
@@ -1167,13 +1182,6 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
   unsigned long long* chf = at<unsigned long long>(ws, p->o_chf);
   unsigned long long* chr = at<unsigned long long>(ws, p->o_chr);
   unsigned char* pm = at<unsigned char>(ws, p->o_pm);
-  cplx* out22 = at<cplx>(ws, p->o_out22);
-  cplx* outp22 = at<cplx>(ws, p->o_outp22);
-  cplx* out33 = at<cplx>(ws, p->o_out33);
-  char* scratch = at<char>(ws, p->o_scratch);
-  const double* dn = p->nodes;  // [k*MAX_RANK] nodes, [(4+k)*MAX_RANK] weights
-  gl_status s;
-
   {
     LaunchScope ls_("slots_init_kernel", st, 0.0);
     slots_init_kernel<<<(gu + 63) / 64, 64, 0, st>>>(slots, gu);
@@ -1291,6 +1299,29 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     }
     LAUNCH_CHECK("scalars_kernel");
   }
+  *spec_out = spec;
+  return GL_OK;
+}
+
+static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, void* outputs,
+                           void* ws, int* status, cudaStream_t st) {
+  if (p->e44) return run_group_eta44(p, gu, spectra, layout, outputs, ws, status, st);
+  const int T = 256;
+  const Box B1 = p->b1, B2 = p->b2, B3 = p->b3;
+  const int pl1 = B1.w * B1.h, pl2 = B2.w * B2.h, pl3 = B3.w * B3.h;
+  UnitScalars* us = at<UnitScalars>(ws, p->o_us);
+  unsigned char* s2 = at<unsigned char>(ws, p->o_s2);
+  unsigned char* s3 = at<unsigned char>(ws, p->o_s3);
+  unsigned char* ch = at<unsigned char>(ws, p->o_ch);
+  unsigned char* pm = at<unsigned char>(ws, p->o_pm);
+  cplx* out22 = at<cplx>(ws, p->o_out22);
+  cplx* outp22 = at<cplx>(ws, p->o_outp22);
+  cplx* out33 = at<cplx>(ws, p->o_out33);
+  char* scratch = at<char>(ws, p->o_scratch);
+  const double* dn = p->nodes;  // [k*MAX_RANK] nodes, [(4+k)*MAX_RANK] weights
+  gl_status s;
+  const cplx* spec = nullptr;
+  if ((s = analyse_group(p, gu, spectra, layout, ws, st, &spec)) != GL_OK) return s;
   const double fwd_scale = ((double)p->d.nx * (double)p->d.ny) / ((double)p->ncx * (double)p->ncy);
   const double inv_scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
   const int ncy = p->ncy;
@@ -2479,6 +2510,731 @@ extern "C" gl_status gl_execute(gl_plan* p, int n_units, const void* d_spectra, 
     gl_status s = run_group(p, gu, in, layout, outp, d_ws, d_status ? d_status + u0 : nullptr, st);
     if (s != GL_OK) return s;
   }
+  return GL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// adjoint (reverse-mode) pass: gradient of a real loss of the eta components
+// ---------------------------------------------------------------------------
+//
+// The backward pass keeps no tape from the forward call: it re-runs the
+// analysis and the forward node stages it needs (to recover the node fields
+// and the roundoff-floor decisions) and then runs every stage transposed.
+// Stage buffers live only inside one call.
+
+struct AdjLayout {
+  size_t e1, e2, e3, da22, da1, dai, stage, total;  // offsets from the scratch base
+};
+
+static bool adj_eta22(const gl_plan* p) { return (p->comps & GL_COMP_ETA22) != 0; }
+static bool adj_eta33(const gl_plan* p) { return (p->comps & GL_COMP_ETA33) != 0; }
+
+struct AdjStage22 {
+  size_t P, Q, R, mx, RA, QA, end;
+};
+struct AdjStage33 {
+  size_t E, mxs, PI, QI, RI, maxRI, P1, P2, QO, RO, RAo, QA1, QA2, EA, RAi, QAi, end;
+};
+
+static AdjStage22 adj_stage22(const gl_plan* p, size_t base, int g) {
+  const size_t c = sizeof(cplx), ncy = p->ncy, pl2 = (size_t)p->b2.w * p->b2.h;
+  const size_t nj = (size_t)g * p->ranks[0];
+  Bump b;
+  b.off = base;
+  AdjStage22 s;
+  s.P = b.take(nj * 8 * p->b1.w * ncy * c);
+  s.Q = b.take(nj * 2 * p->b2.w * ncy * c);  // also the adjoint columns
+  s.R = b.take(nj * 2 * pl2 * c);
+  s.mx = b.take(nj * 2 * 8);
+  s.RA = b.take(nj * 2 * pl2 * c);
+  s.QA = b.take(nj * 8 * p->b1.w * ncy * c);
+  s.end = b.off;
+  return s;
+}
+
+static AdjStage33 adj_stage33(const gl_plan* p, size_t base, int g) {
+  const size_t c = sizeof(cplx), ncy = p->ncy;
+  const size_t pl2 = (size_t)p->b2.w * p->b2.h, pl3 = (size_t)p->b3.w * p->b3.h;
+  const size_t nuj = (size_t)g * p->ranks[3], nj = nuj * p->ranks[2];
+  Bump b;
+  b.off = base;
+  AdjStage33 s;
+  s.E = b.take(nuj * 4 * pl2 * c);
+  s.mxs = b.take(nuj * 3 * 8);                       // eta_t max [nuj], forcing maxima [nuj][2]
+  s.PI = b.take(nj * 12 * p->b1.w * ncy * c);
+  s.QI = b.take(nj * 4 * p->b2.w * ncy * c);         // also the inner adjoint columns
+  s.RI = b.take(nj * 4 * pl2 * c);
+  s.maxRI = b.take(nj * 4 * 8);
+  s.P1 = b.take(nuj * 12 * p->b1.w * ncy * c);
+  s.P2 = b.take(nuj * 9 * p->b2.w * ncy * c);
+  s.QO = b.take(nuj * 2 * p->b3.w * ncy * c);        // also the outer adjoint columns
+  s.RO = b.take(nuj * 2 * pl3 * c);
+  s.RAo = b.take(nuj * 2 * pl3 * c);
+  s.QA1 = b.take(nuj * 12 * p->b1.w * ncy * c);
+  s.QA2 = b.take(nuj * 8 * p->b2.w * ncy * c);
+  s.EA = b.take(nuj * 4 * pl2 * c);
+  s.RAi = b.take(nj * 4 * pl2 * c);
+  s.QAi = b.take(nj * 12 * p->b1.w * ncy * c);
+  s.end = b.off;
+  return s;
+}
+
+static AdjLayout adj_layout(const gl_plan* p, int g) {
+  const size_t c = sizeof(cplx);
+  const size_t pl1 = (size_t)p->b1.w * p->b1.h, pl2 = (size_t)p->b2.w * p->b2.h,
+               pl3 = (size_t)p->b3.w * p->b3.h;
+  const bool e22 = adj_eta22(p), e33 = adj_eta33(p);
+  AdjLayout L;
+  Bump b;
+  L.e1 = b.take((size_t)g * pl1 * c);
+  L.e2 = b.take(e22 ? (size_t)g * pl2 * c : 0);
+  L.e3 = b.take(e33 ? (size_t)g * pl3 * c : 0);
+  L.da22 = b.take(e22 ? (size_t)g * p->ranks[0] * pl1 * c : 0);
+  L.da1 = b.take(e33 ? (size_t)g * p->ranks[3] * pl1 * c : 0);
+  L.dai = b.take(e33 ? (size_t)g * p->ranks[3] * p->ranks[2] * pl1 * c : 0);
+  L.stage = b.off;
+  const size_t wmax = std::max({(size_t)p->b1.w, (size_t)p->b2.w, (size_t)p->b3.w});
+  size_t end = L.stage + align_up((size_t)g * p->d.ny * wmax * c);  // seed rows
+  if (e22) end = std::max(end, adj_stage22(p, L.stage, g).end);
+  if (e33) end = std::max(end, adj_stage33(p, L.stage, g).end);
+  L.total = end;
+  return L;
+}
+
+static gl_status adj_check_plan(const gl_plan* p) {
+  if (!p) return fail(GL_ERR_INVALID_ARGUMENT, "null plan");
+  if (p->e44) return fail(GL_ERR_UNSUPPORTED, "the adjoint covers the eta11/eta22/eta33 graph only");
+  if (!(p->comps & (GL_COMP_ETA11 | GL_COMP_ETA22 | GL_COMP_ETA33)))
+    return fail(GL_ERR_INVALID_ARGUMENT, "the plan has no eta component to differentiate");
+  if (adj_eta33(p) && row_smem(23, p->ncx) > SMEM_LIMIT)
+    return fail(GL_ERR_UNSUPPORTED, "the order-3 adjoint row exceeds the shared-memory budget at %d columns",
+                p->ncx);
+  return GL_OK;
+}
+
+extern "C" gl_status gl_adjoint_workspace_size(const gl_plan* p, size_t* bytes) {
+  gl_status s = adj_check_plan(p);
+  if (s != GL_OK) return s;
+  if (!bytes) return fail(GL_ERR_INVALID_ARGUMENT, "null size pointer");
+  *bytes = p->o_scratch + adj_layout(p, p->group).total;
+  return GL_OK;
+}
+
+static gl_status launch_seed_rows(const SeedArgs& a, int nunits, cudaStream_t st, const cplx* tw) {
+  const int G = 256 / (a.nx / 16);
+  const size_t smem = (size_t)G * padded_len(a.nx) * sizeof(cplx);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(seed_row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    attr = true;
+  }
+  dim3 grid((a.ny + G - 1) / G, nunits);
+  const double bytes = (double)nunits * a.ny * ((double)a.nx * sizeof(double) + (double)a.w * sizeof(cplx));
+  LaunchScope ls("seed_row_kernel", st, bytes);
+  seed_row_kernel<<<grid, 256, smem, st>>>(a, tw);
+  LAUNCH_CHECK("seed_row_kernel");
+  return GL_OK;
+}
+
+static gl_status launch_combine(const CmbArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
+  // columns per block: all banks of `cw` columns staged at once, within
+  // ~110 KB of shared memory (two blocks per SM)
+  const size_t col_bytes = (size_t)a.nbanks * padded_len(a.n) * sizeof(cplx);
+  const int cw = (int)std::max<size_t>(1, std::min<size_t>((size_t)a.box.w, (110 * 1024) / col_bytes));
+  const size_t smem = (size_t)cw * col_bytes;
+  if (smem > SMEM_LIMIT) return fail(GL_ERR_UNSUPPORTED, "adjoint column stage exceeds shared memory");
+  if (a.nout < 1 || a.nout > 4) return fail(GL_ERR_INVALID_ARGUMENT, "adjoint column stage: 1..4 outputs");
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(col_combine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    attr = true;
+  }
+  dim3 grid((a.box.w + cw - 1) / cw, njobs);
+  const double bytes = (double)njobs * a.nbanks * a.box.w * a.n * sizeof(cplx) +
+                       (double)njobs * a.nout * a.box.w * a.box.h * sizeof(cplx);
+  LaunchScope ls("col_combine_kernel", st, bytes);
+  col_combine_kernel<<<grid, 256, smem, st>>>(a, tw, cw);
+  LAUNCH_CHECK("col_combine_kernel");
+  return GL_OK;
+}
+
+// Ebar of one output box from the residual: + sign transforms, h/(Nx Ny).
+static gl_status adj_seed(gl_plan* p, int gu, const double* resid, const Box& box, cplx* rows,
+                          cplx* out, cudaStream_t st) {
+  SeedArgs sa;
+  sa.r = resid;
+  sa.nx = p->d.nx;
+  sa.log2nx = p->lnx;
+  sa.ny = p->d.ny;
+  sa.x0 = box.x0;
+  sa.w = box.w;
+  sa.out = rows;
+  gl_status s = launch_seed_rows(sa, gu, st, p->tw);
+  if (s != GL_OK) return s;
+  ColFftArgs f;
+  f.in = rows;
+  f.out = out;
+  f.box = box;
+  f.n = p->d.ny;
+  f.log2n = p->lny;
+  f.nsrc = 1;
+  f.jobs_per_unit = 1;
+  f.mask = nullptr;
+  f.maxslot = nullptr;
+  f.scale = p->d.depth / ((double)p->d.nx * (double)p->d.ny);
+  f.conj_io = 1;
+  return launch_col_fft(f, gu, st, p->tw);
+}
+
+// Adjoint column stage: + or - sign column transforms of `nb` adjoint
+// spectra per job (COL_PLAIN, the transposed forward transform).
+static gl_status adj_cols(gl_plan* p, const Box& box, const double* geo, const cplx* spec, int nb,
+                          int njobs, cplx* out, cudaStream_t st) {
+  ColArgs a;
+  std::memset(&a, 0, sizeof a);
+  a.kind = COL_PLAIN;
+  a.nbanks = nb;
+  for (int k = 0; k < nb; ++k) {
+    a.mult[k] = M_ONE;
+    a.src_of[k] = k;
+  }
+  a.box = box;
+  a.geo = geo;
+  a.spec = spec;
+  a.spec_job_stride = (long long)nb * box.w * box.h;
+  a.spec_sub_stride = (long long)box.w * box.h;
+  a.jobs_per_unit = 1;
+  a.out = out;
+  a.n = p->ncy;
+  a.log2n = p->lncy;
+  a.scale = ((double)p->d.nx * (double)p->d.ny) / ((double)p->ncx * (double)p->ncy);
+  a.conj_io = 1;
+  return launch_col_ifft(a, njobs, st, p->tw);
+}
+
+static CmbArgs cmb_args(gl_plan* p, int kind, int nb, const int* mults, const int* dsts, int nout,
+                        const Box& box, const double* geo, const cplx* in, cplx* out,
+                        const UnitScalars* us, int jobs_per_unit) {
+  CmbArgs a;
+  std::memset(&a, 0, sizeof a);
+  a.kind = kind;
+  a.nbanks = nb;
+  for (int k = 0; k < nb; ++k) {
+    a.mult[k] = mults[k];
+    a.dst_of[k] = dsts ? dsts[k] : 0;
+  }
+  a.nout = nout;
+  a.box = box;
+  a.geo = geo;
+  a.in = in;
+  a.out = out;
+  a.n = p->ncy;
+  a.log2n = p->lncy;
+  a.scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
+  a.us = us;
+  a.jobs_per_unit = jobs_per_unit;
+  return a;
+}
+
+static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int layout,
+                                   const double* resid, cplx* grad, void* ws, int* status,
+                                   cudaStream_t st) {
+  const int T = 256;
+  const Box B1 = p->b1, B2 = p->b2, B3 = p->b3;
+  const int pl1 = B1.w * B1.h, pl2 = B2.w * B2.h, pl3 = B3.w * B3.h;
+  UnitScalars* us = at<UnitScalars>(ws, p->o_us);
+  unsigned char* s2 = at<unsigned char>(ws, p->o_s2);
+  unsigned char* s3 = at<unsigned char>(ws, p->o_s3);
+  char* base = at<char>(ws, p->o_scratch);
+  const double* dn = p->nodes;
+  const int ncy = p->ncy;
+  const double fwd_scale = ((double)p->d.nx * (double)p->d.ny) / ((double)p->ncx * (double)p->ncy);
+  const double inv_scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
+  const AdjLayout L = adj_layout(p, p->group);
+  cplx* E1 = reinterpret_cast<cplx*>(base + L.e1);
+  cplx* E2 = reinterpret_cast<cplx*>(base + L.e2);
+  cplx* E3 = reinterpret_cast<cplx*>(base + L.e3);
+  cplx* DA22 = reinterpret_cast<cplx*>(base + L.da22);
+  cplx* DA1 = reinterpret_cast<cplx*>(base + L.da1);
+  cplx* DAI = reinterpret_cast<cplx*>(base + L.dai);
+  gl_status s;
+  const cplx* spec = nullptr;
+  if ((s = analyse_group(p, gu, spectra, layout, ws, st, &spec)) != GL_OK) return s;
+
+  // seeds: Ebar on each differentiated component's box
+  cplx* rows = reinterpret_cast<cplx*>(base + L.stage);
+  const bool e11 = p->comps & GL_COMP_ETA11, e22 = adj_eta22(p), e33 = adj_eta33(p);
+  if (e11 && (s = adj_seed(p, gu, resid, B1, rows, E1, st)) != GL_OK) return s;
+  if (e22 && (s = adj_seed(p, gu, resid, B2, rows, E2, st)) != GL_OK) return s;
+  if (e33 && (s = adj_seed(p, gu, resid, B3, rows, E3, st)) != GL_OK) return s;
+
+  // ---------------- eta22 (spatial.py:156-231), transposed ----------------
+  if (e22) {
+    const int J = p->ranks[0];
+    const int nj = gu * J;
+    const AdjStage22 S = adj_stage22(p, L.stage, p->group);
+    cplx* P = reinterpret_cast<cplx*>(base + S.P);
+    cplx* Q = reinterpret_cast<cplx*>(base + S.Q);
+    cplx* R = reinterpret_cast<cplx*>(base + S.R);
+    unsigned long long* mx = reinterpret_cast<unsigned long long*>(base + S.mx);
+    cplx* RA = reinterpret_cast<cplx*>(base + S.RA);
+    cplx* QA = reinterpret_cast<cplx*>(base + S.QA);
+    CUDA_TRY(cudaMemsetAsync(mx, 0, (size_t)nj * 2 * 8, st));
+    const int m8[8] = {M_ONE, M_NU, M_NU2, M_QX_DIVNU, M_QY_DIVNU, M_Q2_DIVNU, M_QX, M_QY};
+    // forward node fields and products (recomputed)
+    ColArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.kind = COL_ETA22;
+    a.nbanks = 8;
+    for (int k = 0; k < 8; ++k) a.mult[k] = m8[k];
+    a.box = B1;
+    a.geo = p->geo1;
+    a.spec = spec;
+    a.spec_job_stride = pl1;
+    a.jobs_per_unit = J;
+    a.us = us;
+    a.nodes = dn + 0 * MAX_RANK;
+    a.out = P;
+    a.n = ncy;
+    a.log2n = p->lncy;
+    a.scale = inv_scale;
+    if ((s = launch_col_ifft(a, nj, st, p->tw)) != GL_OK) return s;
+    RowArgs r;
+    std::memset(&r, 0, sizeof r);
+    r.kind = ROW_ETA22;
+    r.grp[0] = BankGroup{P, 8, B1.x0, B1.w};
+    r.ngrp = 1;
+    r.nout = 2;
+    r.out_x0 = B2.x0;
+    r.out_w = B2.w;
+    r.out = Q;
+    r.nx = p->ncx;
+    r.log2nx = p->lncx;
+    r.ny = ncy;
+    r.us = us;
+    r.jobs_per_unit = J;
+    r.gmax = ROW_GMAX;
+    if ((s = launch_row(r, nj, st, p->tw)) != GL_OK) return s;
+    ColFftArgs f;
+    f.in = Q;
+    f.out = R;
+    f.box = B2;
+    f.n = ncy;
+    f.log2n = p->lncy;
+    f.nsrc = 2;
+    f.jobs_per_unit = J;
+    f.mask = s2;
+    f.maxslot = mx;
+    f.scale = fwd_scale;
+    if ((s = launch_col_fft(f, nj * 2, st, p->tw)) != GL_OK) return s;
+    // adjoint node spectra -> adjoint fields -> transposed products
+    AdjArgs aa;
+    std::memset(&aa, 0, sizeof aa);
+    aa.us = us;
+    aa.geo = p->geo2;
+    aa.box = B2;
+    aa.seed = E2;
+    aa.fwd = R;
+    aa.fwdmax = mx;
+    aa.mask = s2;
+    aa.out = RA;
+    aa.nodes = dn + 0 * MAX_RANK;
+    aa.weights = dn + 4 * MAX_RANK;
+    aa.jobs_per_unit = J;
+    aa.floor_rel = p->floor_rel;
+    {
+      dim3 g(grid_for(pl2, T, 64), nj);
+      LaunchScope ls_("adj_eta22_kernel", st, 0.0);
+      adj_eta22_kernel<<<g, T, 0, st>>>(aa);
+    }
+    LAUNCH_CHECK("adj_eta22_kernel");
+    if ((s = adj_cols(p, B2, p->geo2, RA, 2, nj, Q, st)) != GL_OK) return s;
+    RowArgs ra;
+    std::memset(&ra, 0, sizeof ra);
+    ra.kind = ROW_ADJ_ETA22;
+    ra.grp[0] = BankGroup{P, 8, B1.x0, B1.w, 0};
+    ra.grp[1] = BankGroup{Q, 2, B2.x0, B2.w, 1};
+    ra.ngrp = 2;
+    ra.nout = 8;
+    ra.out_x0 = B1.x0;
+    ra.out_w = B1.w;
+    ra.out = QA;
+    ra.out_conj = 1;
+    ra.nx = p->ncx;
+    ra.log2nx = p->lncx;
+    ra.ny = ncy;
+    ra.us = us;
+    ra.jobs_per_unit = J;
+    ra.gmax = ROW_GMAX;
+    if ((s = launch_row(ra, nj, st, p->tw)) != GL_OK) return s;
+    CmbArgs c = cmb_args(p, CMB_ETA22, 8, m8, nullptr, 1, B1, p->geo1, QA, DA22, us, J);
+    c.nodes = dn + 0 * MAX_RANK;
+    if ((s = launch_combine(c, nj, st, p->tw)) != GL_OK) return s;
+  }
+
+  // ---------------- order 3 (_order3.py:18-148), eta33 transposed ----------------
+  if (e33) {
+    const int Jo = p->ranks[3], I = p->ranks[2];
+    const int nuj = gu * Jo, nj = nuj * I;
+    const AdjStage33 S = adj_stage33(p, L.stage, p->group);
+    cplx* E = reinterpret_cast<cplx*>(base + S.E);
+    unsigned long long* maxEt = reinterpret_cast<unsigned long long*>(base + S.mxs);
+    unsigned long long* maxRO = maxEt + nuj;
+    cplx* PI = reinterpret_cast<cplx*>(base + S.PI);
+    cplx* QI = reinterpret_cast<cplx*>(base + S.QI);
+    cplx* RI = reinterpret_cast<cplx*>(base + S.RI);
+    unsigned long long* maxRI = reinterpret_cast<unsigned long long*>(base + S.maxRI);
+    cplx* P1 = reinterpret_cast<cplx*>(base + S.P1);
+    cplx* P2 = reinterpret_cast<cplx*>(base + S.P2);
+    cplx* QO = reinterpret_cast<cplx*>(base + S.QO);
+    cplx* RO = reinterpret_cast<cplx*>(base + S.RO);
+    cplx* RAo = reinterpret_cast<cplx*>(base + S.RAo);
+    cplx* QA1 = reinterpret_cast<cplx*>(base + S.QA1);
+    cplx* QA2 = reinterpret_cast<cplx*>(base + S.QA2);
+    cplx* EA = reinterpret_cast<cplx*>(base + S.EA);
+    cplx* RAi = reinterpret_cast<cplx*>(base + S.RAi);
+    cplx* QAi = reinterpret_cast<cplx*>(base + S.QAi);
+    CUDA_TRY(cudaMemsetAsync(maxEt, 0, (size_t)nuj * 3 * 8, st));
+    CUDA_TRY(cudaMemsetAsync(maxRI, 0, (size_t)nj * 4 * 8, st));
+    const int mi[12] = {M_ONE, M_NU, M_NU2, M_NU3, M_QX_SNU, M_QY_SNU,
+                        M_QX, M_QY, M_Q2_SNU, M_Q2, M_NUQX, M_NUQY};
+    const int m1[12] = {M_ONE, M_IQX, M_IQY, M_QX_SNU, M_QY_SNU, M_MI_NU,
+                        M_NUQX, M_NUQY, M_MI_Q2_SNU, M_MI_Q2NU, M_MINUS_A, M_MINUS_Q2};
+    const int m9[9] = {M_ONE, M_IQX, M_IQY, M_IQX, M_IQY, M_A, M_Q2, M_A, M_ONE};
+    const int src9[9] = {0, 0, 0, 2, 2, 2, 2, 3, 1};
+    // forward inner stage (recomputed): inner fields PI, sources RI, pair spectra E
+    {
+      ColArgs a;
+      std::memset(&a, 0, sizeof a);
+      a.kind = COL_INNER;
+      a.nbanks = 12;
+      for (int k = 0; k < 12; ++k) a.mult[k] = mi[k];
+      a.box = B1;
+      a.geo = p->geo1;
+      a.spec = spec;
+      a.spec_job_stride = pl1;
+      a.jobs_per_unit = Jo * I;
+      a.us = us;
+      a.nodes = dn + 3 * MAX_RANK;
+      a.nodes2 = dn + 2 * MAX_RANK;
+      a.n_inner = I;
+      a.n_outer = Jo;
+      a.out = PI;
+      a.n = ncy;
+      a.log2n = p->lncy;
+      a.scale = inv_scale;
+      if ((s = launch_col_ifft(a, nj, st, p->tw)) != GL_OK) return s;
+      RowArgs r;
+      std::memset(&r, 0, sizeof r);
+      r.kind = ROW_INNER;
+      r.grp[0] = BankGroup{PI, 12, B1.x0, B1.w};
+      r.ngrp = 1;
+      r.nout = 4;
+      r.out_x0 = B2.x0;
+      r.out_w = B2.w;
+      r.out = QI;
+      r.nx = p->ncx;
+      r.log2nx = p->lncx;
+      r.ny = ncy;
+      r.us = us;
+      r.jobs_per_unit = Jo * I;
+      r.gmax = ROW_GMAX;
+      if ((s = launch_row(r, nj, st, p->tw)) != GL_OK) return s;
+      ColFftArgs f;
+      f.in = QI;
+      f.out = RI;
+      f.box = B2;
+      f.n = ncy;
+      f.log2n = p->lncy;
+      f.nsrc = 4;
+      f.jobs_per_unit = Jo * I;
+      f.mask = s2;
+      f.maxslot = maxRI;
+      f.scale = fwd_scale;
+      if ((s = launch_col_fft(f, nj * 4, st, p->tw)) != GL_OK) return s;
+      AccArgs c;
+      std::memset(&c, 0, sizeof c);
+      c.us = us;
+      c.geo = p->geo2;
+      c.box = B2;
+      c.in = RI;
+      c.maxin = maxRI;
+      c.out = E;
+      c.maxout = maxEt;
+      c.mask = s2;
+      c.nodes = dn + 2 * MAX_RANK;
+      c.weights = dn + 6 * MAX_RANK;
+      c.nnodes = I;
+      c.nsub = Jo;
+      c.floor_rel = p->floor_rel;
+      dim3 g(grid_for(pl2, T, 128), nuj);
+      {
+        LaunchScope ls_("acc_inner_kernel", st, 0.0);
+        acc_inner_kernel<<<g, T, 0, st>>>(c);
+      }
+      LAUNCH_CHECK("acc_inner_kernel");
+    }
+    // forward outer stage (recomputed): first-order fields P1, pair fields P2,
+    // the fk, fd forcing spectra RO and their maxima
+    {
+      ColArgs a;
+      std::memset(&a, 0, sizeof a);
+      a.kind = COL_OUTER1;
+      a.nbanks = 12;
+      for (int k = 0; k < 12; ++k) a.mult[k] = m1[k];
+      a.box = B1;
+      a.geo = p->geo1;
+      a.spec = spec;
+      a.spec_job_stride = pl1;
+      a.jobs_per_unit = Jo;
+      a.us = us;
+      a.nodes = dn + 3 * MAX_RANK;
+      a.out = P1;
+      a.n = ncy;
+      a.log2n = p->lncy;
+      a.scale = inv_scale;
+      if ((s = launch_col_ifft(a, nuj, st, p->tw)) != GL_OK) return s;
+      ColArgs a2;
+      std::memset(&a2, 0, sizeof a2);
+      a2.kind = COL_OUTER2;
+      a2.nbanks = 9;
+      for (int k = 0; k < 9; ++k) {
+        a2.mult[k] = m9[k];
+        a2.src_of[k] = src9[k];
+      }
+      a2.box = B2;
+      a2.geo = p->geo2;
+      a2.spec = E;
+      a2.spec_job_stride = 4LL * pl2;
+      a2.spec_sub_stride = pl2;
+      a2.jobs_per_unit = Jo;
+      a2.us = us;
+      a2.floor_max = maxEt;
+      a2.floor_rel = p->floor_rel;
+      a2.out = P2;
+      a2.n = ncy;
+      a2.log2n = p->lncy;
+      a2.scale = inv_scale;
+      if ((s = launch_col_ifft(a2, nuj, st, p->tw)) != GL_OK) return s;
+      RowArgs r;
+      std::memset(&r, 0, sizeof r);
+      r.kind = ROW_OUTER;
+      r.grp[0] = BankGroup{P1, 12, B1.x0, B1.w};
+      r.grp[1] = BankGroup{P2, 9, B2.x0, B2.w};
+      r.ngrp = 2;
+      r.nout = 2;  // fk, fd (the contact rows feed psi33 only)
+      r.out_x0 = B3.x0;
+      r.out_w = B3.w;
+      r.out = QO;
+      r.nx = p->ncx;
+      r.log2nx = p->lncx;
+      r.ny = ncy;
+      r.us = us;
+      r.jobs_per_unit = Jo;
+      r.gmax = ROW_GMAX;
+      if ((s = launch_row(r, nuj, st, p->tw)) != GL_OK) return s;
+      ColFftArgs f;
+      f.in = QO;
+      f.out = RO;
+      f.box = B3;
+      f.n = ncy;
+      f.log2n = p->lncy;
+      f.nsrc = 2;
+      f.jobs_per_unit = Jo;
+      f.mask = s3;
+      f.maxslot = maxRO;
+      f.scale = fwd_scale;
+      if ((s = launch_col_fft(f, nuj * 2, st, p->tw)) != GL_OK) return s;
+    }
+    // adjoint outer stage: forcing adjoints -> first-order and pair adjoints
+    {
+      AdjArgs aa;
+      std::memset(&aa, 0, sizeof aa);
+      aa.us = us;
+      aa.geo = p->geo3;
+      aa.box = B3;
+      aa.seed = E3;
+      aa.fwd = RO;
+      aa.fwdmax = maxRO;
+      aa.mask = s3;
+      aa.out = RAo;
+      aa.nodes = dn + 3 * MAX_RANK;
+      aa.weights = dn + 7 * MAX_RANK;
+      aa.jobs_per_unit = Jo;
+      aa.floor_rel = p->floor_rel;
+      {
+        dim3 g(grid_for(pl3, T, 128), nuj);
+        LaunchScope ls_("adj_outer_kernel", st, 0.0);
+        adj_outer_kernel<<<g, T, 0, st>>>(aa);
+      }
+      LAUNCH_CHECK("adj_outer_kernel");
+      if ((s = adj_cols(p, B3, p->geo3, RAo, 2, nuj, QO, st)) != GL_OK) return s;
+      RowArgs ra;
+      std::memset(&ra, 0, sizeof ra);
+      ra.kind = ROW_ADJ_OUTER;
+      ra.grp[0] = BankGroup{P1, 12, B1.x0, B1.w, 0};
+      ra.grp[1] = BankGroup{P2, 9, B2.x0, B2.w, 0};
+      ra.grp[2] = BankGroup{QO, 2, B3.x0, B3.w, 1};
+      ra.ngrp = 3;
+      ra.nout = 20;
+      ra.nout_a = 12;
+      ra.out_x0 = B1.x0;
+      ra.out_w = B1.w;
+      ra.out = QA1;
+      ra.out2_x0 = B2.x0;
+      ra.out2_w = B2.w;
+      ra.out2 = QA2;
+      ra.out_conj = 1;
+      ra.nx = p->ncx;
+      ra.log2nx = p->lncx;
+      ra.ny = ncy;
+      ra.us = us;
+      ra.jobs_per_unit = Jo;
+      ra.gmax = ROW_GMAX;
+      if ((s = launch_row(ra, nuj, st, p->tw)) != GL_OK) return s;
+      CmbArgs c1 = cmb_args(p, CMB_FIRST3, 12, m1, nullptr, 1, B1, p->geo1, QA1, DA1, us, Jo);
+      c1.nodes = dn + 3 * MAX_RANK;
+      if ((s = launch_combine(c1, nuj, st, p->tw)) != GL_OK) return s;
+      CmbArgs c2 = cmb_args(p, CMB_PAIR, 8, m9, src9, 4, B2, p->geo2, QA2, EA, us, Jo);
+      c2.mask = s2;
+      if ((s = launch_combine(c2, nuj, st, p->tw)) != GL_OK) return s;
+    }
+    // adjoint inner stage: pair-spectra adjoints -> source adjoints -> inner fields
+    {
+      AdjArgs aa;
+      std::memset(&aa, 0, sizeof aa);
+      aa.us = us;
+      aa.geo = p->geo2;
+      aa.box = B2;
+      aa.seed = EA;
+      aa.fwd = RI;
+      aa.fwdmax = maxRI;
+      aa.mask = s2;
+      aa.out = RAi;
+      aa.nodes = dn + 2 * MAX_RANK;
+      aa.weights = dn + 6 * MAX_RANK;
+      aa.jobs_per_unit = Jo * I;
+      aa.n_inner = I;
+      aa.floor_rel = p->floor_rel;
+      {
+        dim3 g(grid_for(pl2, T, 64), nj);
+        LaunchScope ls_("adj_inner_kernel", st, 0.0);
+        adj_inner_kernel<<<g, T, 0, st>>>(aa);
+      }
+      LAUNCH_CHECK("adj_inner_kernel");
+      if ((s = adj_cols(p, B2, p->geo2, RAi, 4, nj, QI, st)) != GL_OK) return s;
+      RowArgs ra;
+      std::memset(&ra, 0, sizeof ra);
+      ra.kind = ROW_ADJ_INNER;
+      ra.grp[0] = BankGroup{PI, 12, B1.x0, B1.w, 0};
+      ra.grp[1] = BankGroup{QI, 4, B2.x0, B2.w, 1};
+      ra.ngrp = 2;
+      ra.nout = 12;
+      ra.out_x0 = B1.x0;
+      ra.out_w = B1.w;
+      ra.out = QAi;
+      ra.out_conj = 1;
+      ra.nx = p->ncx;
+      ra.log2nx = p->lncx;
+      ra.ny = ncy;
+      ra.us = us;
+      ra.jobs_per_unit = Jo * I;
+      ra.gmax = ROW_GMAX;
+      if ((s = launch_row(ra, nj, st, p->tw)) != GL_OK) return s;
+      CmbArgs c = cmb_args(p, CMB_INNER, 12, mi, nullptr, 1, B1, p->geo1, QAi, DAI, us, Jo * I);
+      c.nodes = dn + 3 * MAX_RANK;
+      c.nodes2 = dn + 2 * MAX_RANK;
+      c.n_inner = I;
+      if ((s = launch_combine(c, nj, st, p->tw)) != GL_OK) return s;
+    }
+  }
+
+  // ---------------- gradient on the parent box ----------------
+  {
+    RedArgs ra;
+    ra.e1 = e11 ? E1 : nullptr;
+    ra.da22 = DA22;
+    ra.n22 = e22 ? p->ranks[0] : 0;
+    ra.da1 = DA1;
+    ra.n1 = e33 ? p->ranks[3] : 0;
+    ra.dai = DAI;
+    ra.ni = e33 ? p->ranks[3] * p->ranks[2] : 0;
+    ra.grad = grad;
+    ra.plane = pl1;
+    dim3 g(grid_for(pl1, T, 64), gu);
+    {
+      LaunchScope ls_("adj_reduce_kernel", st, 0.0);
+      adj_reduce_kernel<<<g, T, 0, st>>>(ra);
+    }
+    LAUNCH_CHECK("adj_reduce_kernel");
+  }
+  {
+    dim3 g(grid_for(pl1, T, 64), gu);
+    {
+      LaunchScope ls_("nonfinite_kernel", st, 0.0);
+      nonfinite_kernel<<<g, T, 0, st>>>(grad, (size_t)pl1, 0, us);
+    }
+    LAUNCH_CHECK("nonfinite_kernel");
+  }
+  if (status) {
+    {
+      LaunchScope ls_("status_kernel", st, 0.0);
+      status_kernel<<<(gu + 63) / 64, 64, 0, st>>>(us, gu, status);
+    }
+    LAUNCH_CHECK("status_kernel");
+  }
+  return GL_OK;
+}
+
+extern "C" gl_status gl_adjoint_execute(gl_plan* p, int n_units, const void* d_spectra, int layout,
+                                        const double* d_residual, void* d_grad, void* d_ws,
+                                        size_t ws_bytes, int* d_status, void* stream) {
+  gl_status s = adj_check_plan(p);
+  if (s != GL_OK) return s;
+  if (n_units < 0) return fail(GL_ERR_INVALID_ARGUMENT, "negative unit count");
+  if (n_units == 0) return GL_OK;
+  if (!d_spectra || !d_residual || !d_grad)
+    return fail(GL_ERR_INVALID_ARGUMENT, "null spectra, residual or gradient");
+  if (layout != GL_SPECTRA_FULL && layout != GL_SPECTRA_BOX)
+    return fail(GL_ERR_INVALID_ARGUMENT, "unknown spectra layout");
+  const size_t need = p->o_scratch + adj_layout(p, p->group).total;
+  if (!d_ws || ws_bytes < need || (reinterpret_cast<uintptr_t>(d_ws) & 255))
+    return fail(GL_ERR_WORKSPACE, "workspace must be 256-byte aligned and at least %zu bytes", need);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const size_t in_unit = layout == GL_SPECTRA_FULL ? (size_t)p->d.nx * p->d.ny
+                                                   : (size_t)p->b1.w * p->b1.h;
+  const size_t r_unit = (size_t)p->d.nx * p->d.ny;
+  const size_t g_unit = (size_t)p->b1.w * p->b1.h;
+  for (int u0 = 0; u0 < n_units; u0 += p->group) {
+    const int gu = std::min(p->group, n_units - u0);
+    const void* in = reinterpret_cast<const cplx*>(d_spectra) + (size_t)u0 * in_unit;
+    s = run_adjoint_group(p, gu, in, layout, d_residual + (size_t)u0 * r_unit,
+                          reinterpret_cast<cplx*>(d_grad) + (size_t)u0 * g_unit, d_ws,
+                          d_status ? d_status + u0 : nullptr, st);
+    if (s != GL_OK) return s;
+  }
+  return GL_OK;
+}
+
+extern "C" gl_status gl_deposit_modes_adjoint(const gl_plan* p, int n_units, int n_seg,
+                                              const int* seg_off, const int* seg_bin, int n_modes,
+                                              const double* omega, const double* times,
+                                              const void* d_grad, double* d_gab, void* stream) {
+  if (!p) return fail(GL_ERR_INVALID_ARGUMENT, "null plan");
+  if (n_units < 0 || n_seg < 0 || n_modes < 0) return fail(GL_ERR_INVALID_ARGUMENT, "negative size");
+  if (n_modes == 0) return GL_OK;
+  if (!d_gab || !d_grad || !times || !seg_off || !seg_bin || !omega)
+    return fail(GL_ERR_INVALID_ARGUMENT, "null deposit-adjoint buffer");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  CUDA_TRY(cudaMemsetAsync(d_gab, 0, sizeof(double) * 2 * (size_t)n_modes, st));
+  if (n_seg == 0 || n_units == 0) return GL_OK;
+  {
+    LaunchScope ls_("deposit_adjoint_kernel", st, 0.0);
+    deposit_adjoint_kernel<<<grid_for(n_seg, 128, 256), 128, 0, st>>>(
+        n_units, n_seg, seg_off, seg_bin, omega, times, (double)p->d.nx * (double)p->d.ny,
+        p->d.depth, reinterpret_cast<const cplx*>(d_grad), p->b1.w * p->b1.h, d_gab);
+  }
+  LAUNCH_CHECK("deposit_adjoint_kernel");
   return GL_OK;
 }
 

@@ -183,6 +183,10 @@ struct ColArgs {
   cplx* out;               // [job][bank][w][n]
   int n, log2n;            // transform length along y
   double scale;            // applied to the inverse transform (1/(Nx Ny))
+  // 1: run the transform with the opposite exponent sign, through
+  // conj(F(conj x)) -- the transpose of a forward transform, used by the
+  // adjoint to carry adjoint spectra to the grid
+  int conj_io;
 };
 
 // Damping base value of the job at box bin i (COL_ETA22/PSI22/INNER/OUTER1).
@@ -307,7 +311,8 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
           v = sk[i];
           if (floor_it && cabs_(v) < floor_abs) v = czero();
         }
-        return apply_mult(mult, GeoRef{a.geo, plane, i}, v);
+        const cplx mv = apply_mult(mult, GeoRef{a.geo, plane, i}, v);
+        return a.conj_io ? cconj(mv) : mv;
       };
       auto store = [&](int yb, cplx v) { buf[phys(yb)] = v; };
       fft_row<+1>(buf, f, active, tw, load, store);
@@ -316,7 +321,8 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
     cplx* dst = a.out + ((size_t)job * a.nbanks + k) * n * a.box.w + x_first;
     for (int t = threadIdx.x; t < n * ncol; t += blockDim.x) {
       const int y = t / ncol, c = t % ncol;
-      dst[(size_t)y * a.box.w + c] = cscale(a.scale, bufs[(size_t)c * L + phys(y)]);
+      const cplx v = bufs[(size_t)c * L + phys(y)];
+      dst[(size_t)y * a.box.w + c] = cscale(a.scale, a.conj_io ? cconj(v) : v);
     }
     __syncthreads();
   }
@@ -327,12 +333,15 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
 // ---------------------------------------------------------------------------
 
 enum RowKind : int { ROW_ETA22 = 0, ROW_PSI22, ROW_CONTACT22, ROW_INNER, ROW_OUTER,
-                     ROW_E44_PAIR, ROW_E44_THIRD, ROW_E44_ORDER4 };
+                     ROW_E44_PAIR, ROW_E44_THIRD, ROW_E44_ORDER4,
+                     // adjoint (transposed) products, row_kernel_t<1>
+                     ROW_ADJ_ETA22, ROW_ADJ_INNER, ROW_ADJ_OUTER };
 
 struct BankGroup {
   const cplx* data;  // [job][nb][w][n_y]
   int nb;            // banks in the group
   int x0, w;         // box columns (modes)
+  int conj;          // 1: adjoint rows, transformed with the opposite sign
 };
 
 struct RowArgs {
@@ -347,6 +356,11 @@ struct RowArgs {
   const UnitScalars* us;
   int jobs_per_unit;
   int gmax;                // FFT group size (rows through tmp)
+  // adjoint extensions (zero in the forward stages):
+  int out_conj;            // 1: outputs transformed with the + sign
+  int nout_a;              // > 0: outputs [nout_a, nout) go to out2 instead
+  int out2_x0, out2_w;
+  cplx* out2;              // [job][nout - nout_a][out2_w][n_y]
 };
 
 // Pointwise products of each stage; `b` points at the bank rows (bank k at
@@ -574,7 +588,92 @@ GL_D void row_products(int kind, cplx* b, int L, int p, int chan_count) {
 // (inputs read straight from the column-transformed rows, zero outside the
 // bank's box columns), the stage's products, forward transforms of the
 // outputs, and only the output box's columns are written: [job][out][y][col].
-__global__ void __launch_bounds__(256, 2) row_kernel(RowArgs a, const cplx* __restrict__ tw) {
+// Transposed products of the adjoint stages.  Every forward product is a
+// polynomial P(f_1..f_m) of the bank fields; given the adjoint field w of
+// each product (the transposed forward FFT of its adjoint spectrum) the
+// adjoint of bank f_b is sum_P (dP/df_b) w_P, evaluated pointwise with the
+// forward bank values recomputed in the same row.  No conjugates appear:
+// the GL graph is holomorphic in the parent spectrum.
+GL_D void row_products_adj(int kind, cplx* b, int L, int p) {
+#define BK(k) b[(k) * L + p]
+  switch (kind) {
+    case ROW_ADJ_ETA22: {  // transpose of ROW_ETA22; banks 0..7 forward, 8 w(sd), 9 w(sk)
+      const cplx v = BK(0), v1 = BK(1), v2 = BK(2), hx = BK(3), hy = BK(4), rad = BK(5), jx = BK(6),
+                 jy = BK(7), wd = BK(8), wk = BK(9);
+      const cplx d2 = cscale(2.0, wd), k2 = cscale(2.0, wk);
+      BK(0) = cadd(cmul(v2, d2), cmul(rad, k2));
+      BK(1) = cmul(v1, d2);
+      BK(2) = cmul(v, d2);
+      BK(3) = csub(cmul(jx, k2), cmul(hx, d2));
+      BK(4) = csub(cmul(jy, k2), cmul(hy, d2));
+      BK(5) = cmul(v, k2);
+      BK(6) = cmul(hx, k2);
+      BK(7) = cmul(hy, k2);
+      break;
+    }
+    case ROW_ADJ_INNER: {  // transpose of ROW_INNER; banks 0..11 forward, 12..15 w(sd, sk, sdt, skt)
+      const cplx v = BK(0), v1 = BK(1), v2 = BK(2), v3 = BK(3), hx = BK(4), hy = BK(5), jx = BK(6),
+                 jy = BK(7), rad = BK(8), qq = BK(9), njx = BK(10), njy = BK(11);
+      const cplx w0 = cscale(2.0, BK(12)), w1 = cscale(2.0, BK(13)), w2 = cscale(2.0, BK(14)),
+                 w3 = cscale(2.0, BK(15));
+      BK(0) = cadd(cadd(cmul(v2, w0), cmul(rad, w1)), cadd(cmul(v3, w2), cmul(qq, w3)));
+      BK(1) = cadd(cadd(cmul(v1, w0), cscale(2.0, cmul(v2, w2))), cmul(rad, w3));
+      BK(2) = cadd(cmul(v, w0), cscale(2.0, cmul(v1, w2)));
+      BK(3) = cmul(v, w2);
+      BK(4) = cadd(csub(cmul(jx, w1), cmul(hx, w0)), csub(cmul(njx, w3), cmul(jx, w2)));
+      BK(5) = cadd(csub(cmul(jy, w1), cmul(hy, w0)), csub(cmul(njy, w3), cmul(jy, w2)));
+      BK(6) = cadd(cmul(hx, csub(w1, w2)), cscale(2.0, cmul(jx, w3)));
+      BK(7) = cadd(cmul(hy, csub(w1, w2)), cscale(2.0, cmul(jy, w3)));
+      BK(8) = cadd(cmul(v, w1), cmul(v1, w3));
+      BK(9) = cmul(v, w3);
+      BK(10) = cmul(hx, w3);
+      BK(11) = cmul(hy, w3);
+      break;
+    }
+    case ROW_ADJ_OUTER: {
+      // transpose of the fk, fd rows of ROW_OUTER; banks 0..11 first-order,
+      // 12..20 pair (eta_t at 20 is not used by fk, fd), 21 w(fk), 22 w(fd).
+      // Outputs: 0..11 first-order adjoints, 12..19 pair adjoints (banks 12..19).
+      const cplx fe = BK(0), fex = BK(1), fey = BK(2), fpx = BK(3), fpy = BK(4), fpz = BK(5),
+                 fpxz = BK(6), fpyz = BK(7), fpzz = BK(8), fpzzz = BK(9), fptz = BK(10), fptzz = BK(11);
+      const cplx pe = BK(12), pex = BK(13), pey = BK(14), ppx = BK(15), ppy = BK(16), ppz = BK(17),
+                 ppzz = BK(18), pptz = BK(19);
+      const cplx wk = BK(21), wd = BK(22);
+      // fk = k_direct/4 + k_pair/2, fd = d_direct/4 + d_pair/2
+      const cplx K = cscale(0.5, wk), Kd = cscale(0.25, wk), D = cscale(0.5, wd), Dd = cscale(0.25, wd);
+      const cplx kin = csub(cadd(cmul(fpxz, fex), cmul(fpyz, fey)), cmul(fe, fpzzz));
+      const cplx din = cadd(cmul(fe, fptzz),
+                            cadd(cadd(cmul(fpx, fpxz), cmul(fpy, fpyz)), cmul(fpz, fpzz)));
+      const cplx hfe2 = cmul(cscale(0.5, fe), fe);
+      const cplx feKd = cmul(fe, Kd), feDd = cmul(fe, Dd);
+      BK(0) = cadd(cadd(cmul(Kd, kin), cmul(Dd, din)), csub(cmul(D, pptz), cmul(K, ppzz)));
+      BK(1) = cadd(cmul(feKd, fpxz), cmul(K, ppx));
+      BK(2) = cadd(cmul(feKd, fpyz), cmul(K, ppy));
+      BK(3) = cadd(cadd(cmul(K, pex), cmul(D, ppx)), cmul(feDd, fpxz));
+      BK(4) = cadd(cadd(cmul(K, pey), cmul(D, ppy)), cmul(feDd, fpyz));
+      BK(5) = cadd(cmul(D, ppz), cmul(feDd, fpzz));
+      BK(6) = cadd(cmul(feKd, fex), cmul(feDd, fpx));
+      BK(7) = cadd(cmul(feKd, fey), cmul(feDd, fpy));
+      BK(8) = csub(cmul(feDd, fpz), cmul(K, pe));
+      BK(9) = cscale(-1.0, cmul(Kd, hfe2));
+      BK(10) = cmul(D, pe);
+      BK(11) = cmul(Dd, hfe2);
+      BK(12) = csub(cmul(D, fptz), cmul(K, fpzz));
+      BK(13) = cmul(K, fpx);
+      BK(14) = cmul(K, fpy);
+      BK(15) = cadd(cmul(K, fex), cmul(D, fpx));
+      BK(16) = cadd(cmul(K, fey), cmul(D, fpy));
+      BK(17) = cmul(D, fpz);
+      BK(18) = cscale(-1.0, cmul(K, fe));
+      BK(19) = cmul(D, fe);
+      break;
+    }
+  }
+#undef BK
+}
+
+template <int FAMILY>
+__global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __restrict__ tw) {
   extern __shared__ cplx smem[];
   const int y = blockIdx.x;
   const int job = blockIdx.y;
@@ -608,23 +707,48 @@ __global__ void __launch_bounds__(256, 2) row_kernel(RowArgs a, const cplx* __re
     const int k = it * G + g;
     const bool active = k < nb;
     cplx* buf = banks + (size_t)(active ? k : 0) * L;
-    auto load = [&](int xb) -> cplx { return buf[phys(xb)]; };
-    auto store = [&](int xb, cplx v) { buf[phys(xb)] = v; };
+    bool cj = false;
+    if constexpr (FAMILY == 1) {
+      int k0 = 0;
+      for (int q = 0; q < a.ngrp; ++q) {
+        if (k >= k0 && k < k0 + a.grp[q].nb) cj = a.grp[q].conj != 0;
+        k0 += a.grp[q].nb;
+      }
+    }
+    auto load = [&](int xb) -> cplx {
+      const cplx v = buf[phys(xb)];
+      return cj ? cconj(v) : v;
+    };
+    auto store = [&](int xb, cplx v) { buf[phys(xb)] = cj ? cconj(v) : v; };
     fft_row<+1>(buf, f, active, tw, load, store);
   }
   __syncthreads();
-  const int chan_count = a.kind == ROW_PSI22 ? a.us[job / a.jobs_per_unit].chan_count : 0;
-  for (int p = threadIdx.x; p < n; p += blockDim.x) row_products(a.kind, banks, L, phys(p), chan_count);
+  if constexpr (FAMILY == 0) {
+    const int chan_count = a.kind == ROW_PSI22 ? a.us[job / a.jobs_per_unit].chan_count : 0;
+    for (int p = threadIdx.x; p < n; p += blockDim.x) row_products(a.kind, banks, L, phys(p), chan_count);
+  } else {
+    for (int p = threadIdx.x; p < n; p += blockDim.x) row_products_adj(a.kind, banks, L, phys(p));
+  }
   __syncthreads();
+  const int na = a.nout_a > 0 ? a.nout_a : a.nout;
+  const bool oc = FAMILY == 1 && a.out_conj != 0;
   for (int it = 0; it < (a.nout + G - 1) / G; ++it) {
     const int o = it * G + g;
     const bool active = o < a.nout;
-    cplx* buf = banks + (size_t)(active ? o : 0) * L;
-    cplx* orow = a.out + (((size_t)job * a.nout + (active ? o : 0)) * a.ny + y) * a.out_w;
-    auto load = [&](int xb) -> cplx { return buf[phys(xb)]; };
+    const int oo = active ? o : 0;
+    cplx* buf = banks + (size_t)oo * L;
+    const bool second = oo >= na;
+    const int ox0 = second ? a.out2_x0 : a.out_x0;
+    const int ow = second ? a.out2_w : a.out_w;
+    cplx* orow = second ? a.out2 + (((size_t)job * (a.nout - na) + (oo - na)) * a.ny + y) * ow
+                        : a.out + (((size_t)job * na + oo) * a.ny + y) * ow;
+    auto load = [&](int xb) -> cplx {
+      const cplx v = buf[phys(xb)];
+      return oc ? cconj(v) : v;
+    };
     auto store = [&](int xb, cplx v) {
-      const int xo = wrap(xb - a.out_x0, n);
-      if (xo < a.out_w) orow[xo] = v;
+      const int xo = wrap(xb - ox0, n);
+      if (xo < ow) orow[xo] = oc ? cconj(v) : v;
     };
     fft_row<-1>(buf, f, active, tw, load, store);
   }
@@ -644,6 +768,7 @@ struct ColFftArgs {
   const unsigned char* mask;   // [unit][h][w] or null
   unsigned long long* maxslot; // [js] or null
   double scale;            // (Nx Ny)/(Ncx Ncy)
+  int conj_io = 0;         // 1: + sign transform, conj(F(conj x)) (adjoint seeds)
 };
 
 // One block: `cw` kept columns of one (job, source) spectrum.  Rows of the
@@ -663,7 +788,8 @@ __global__ void __launch_bounds__(256, 2) col_fft_kernel(ColFftArgs a, const cpl
   const cplx* src = a.in + (size_t)js * n * a.box.w + x_first;
   for (int t = threadIdx.x; t < n * ncol; t += blockDim.x) {
     const int y = t / ncol, c = t % ncol;
-    bufs[(size_t)c * L + phys(y)] = src[(size_t)y * a.box.w + c];
+    const cplx v = src[(size_t)y * a.box.w + c];
+    bufs[(size_t)c * L + phys(y)] = a.conj_io ? cconj(v) : v;
   }
   __syncthreads();
   int g, G;
@@ -683,7 +809,8 @@ __global__ void __launch_bounds__(256, 2) col_fft_kernel(ColFftArgs a, const cpl
   for (int t = threadIdx.x; t < ncol * a.box.h; t += blockDim.x) {
     const int c = t % ncol, by = t / ncol;
     const int i = by * a.box.w + x_first + c;
-    cplx v = cscale(a.scale, bufs[(size_t)c * L + phys(wrap(a.box.y0 + by, n))]);
+    const cplx raw = bufs[(size_t)c * L + phys(wrap(a.box.y0 + by, n))];
+    cplx v = cscale(a.scale, a.conj_io ? cconj(raw) : raw);
     if (mask && !mask[i]) v = czero();
     dst[i] = v;
     const double m = cabs_(v);

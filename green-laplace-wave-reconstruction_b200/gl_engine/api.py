@@ -285,6 +285,7 @@ class ModeDeposit:
     seg_bins: np.ndarray
     ab: np.ndarray
     omega: np.ndarray
+    index: np.ndarray | None = None   # deposit order -> input mode index
 
 
 def prepare_deposit(coeffs: GLCoefficients, lx, ly, nx, ny) -> ModeDeposit:
@@ -317,7 +318,7 @@ def prepare_deposit(coeffs: GLCoefficients, lx, ly, nx, ny) -> ModeDeposit:
     sel = idx[order]
     ab = np.stack([coeffs.a[sel], coeffs.b[sel]], axis=1).astype(np.float64).ravel()
     return ModeDeposit(box=box, seg_offsets=seg_offsets, seg_bins=seg_bins, ab=ab,
-                       omega=coeffs.omega[sel].astype(np.float64))
+                       omega=coeffs.omega[sel].astype(np.float64), index=sel.astype(np.int64))
 
 
 def _components_for(order: int, components: Sequence[str] | None) -> int:

@@ -18,7 +18,6 @@ CSRC = PKG.parent / "csrc"
 NATIVE = PKG / "_native"
 LIB = NATIVE / "libgl_b200.so"
 SOURCES = ["gl_engine.cu"]
-HEADERS = ["gl_common.cuh", "gl_fft.cuh", "gl_analysis.cuh", "gl_kernels.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -39,7 +38,8 @@ def _stale() -> bool:
     if not LIB.exists():
         return True
     built = LIB.stat().st_mtime
-    deps = [CSRC / s for s in SOURCES + HEADERS] + [PKG.parent.parent / "include" / "gl_engine.h"]
+    deps = ([CSRC / s for s in SOURCES] + sorted(CSRC.glob("*.cuh"))
+            + [PKG.parent.parent / "include" / "gl_engine.h"])
     return any(d.exists() and d.stat().st_mtime > built for d in deps)
 
 

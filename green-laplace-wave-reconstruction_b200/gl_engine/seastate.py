@@ -95,6 +95,12 @@ def config2(seed: int = 0) -> SeaState:
                              seed=seed, order=3)
 
 
+def config4(seed: int = 0) -> SeaState:
+    """Adjoint-fit workload: h=25 m, L=512 m, 512^2, 2048 modes, Hs=2.5 m, Tp=10 s."""
+    return jonswap_sea_state(n=512, length=512.0, depth=25.0, hs=2.5, tp=10.0, modes=2048,
+                             seed=seed, order=3)
+
+
 def small_order3(seed: int = 0, n: int = 64, modes: int = 24, depth: float = 30.0,
                  length: float | None = None) -> SeaState:
     """A small order-3 sea state for parity tests (defaults: 64^2, 24 modes)."""

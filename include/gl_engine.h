@@ -168,6 +168,33 @@ gl_status gl_execute(gl_plan* plan, int n_units, const void* d_spectra, int spec
                      void* d_outputs, void* d_workspace, size_t workspace_bytes,
                      int* d_unit_status, void* stream);
 
+/* Reverse mode of gl_execute for the eta components.  The reference has no
+ * gradient path; this is the adjoint of the spatial graph it evaluates
+ * (src/gl_spectral_surface.m:26-82: eta11 + the eta22 executor
+ * src/internal/green_laplace_eta22.m:1-79 + the eta33 executor
+ * src/internal/gl_no_stokes_eta33.m:1-274; Python spatial.py:156-231,
+ * _order3.py:18-297).  For a real loss L of the physical field
+ * eta = sum of the plan's eta components (psi components are ignored),
+ * d_residual = dL/deta ([unit][ny][nx] float64) gives
+ * d_grad = g ([unit][box_h][box_w] complex128 on the parent box) with
+ * dL = Re(sum_k g_k ds_k) for perturbations ds of the box spectra, the
+ * supports, balance shifts, scales, peak and roundoff-floor decisions held at
+ * their values for the given spectra.  The call re-evaluates the forward
+ * node stages it needs (no state is kept from gl_execute).  Workspace:
+ * gl_adjoint_workspace_size bytes, 256-byte aligned. */
+gl_status gl_adjoint_workspace_size(const gl_plan* plan, size_t* bytes);
+gl_status gl_adjoint_execute(gl_plan* plan, int n_units, const void* d_spectra, int spectra_layout,
+                             const double* d_residual, void* d_grad, void* d_workspace,
+                             size_t workspace_bytes, int* d_unit_status, void* stream);
+
+/* Transpose of gl_deposit_modes: d_gab ([mode][2] float64, the deposit's
+ * mode order) = (dL/da, dL/db) summed over the n_units snapshots, from the
+ * box-spectrum gradient d_grad of gl_adjoint_execute. */
+gl_status gl_deposit_modes_adjoint(const gl_plan* plan, int n_units, int n_segments,
+                                   const int* d_seg_offsets, const int* d_seg_bins, int n_modes,
+                                   const double* d_omega, const double* d_times,
+                                   const void* d_grad, double* d_gab, void* stream);
+
 /* Batched 2-D complex FFT on [batch][ny][nx] complex128 with numpy's
  * conventions: forward = fft2 (unnormalised), inverse = ifft2 (1/(nx ny)).
  * In-place (d_in == d_out) is allowed.  Replaces the numpy.fft.fft2/ifft2
