@@ -86,6 +86,16 @@ class ClockSampler:
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+        # nvidia-smi takes a moment to start: wait for its first sample so
+        # that the timed region is covered
+        t0 = time.perf_counter()
+        while self.proc is not None and time.perf_counter() - t0 < 5.0:
+            try:
+                if Path(self.path).stat().st_size > 0:
+                    break
+            except OSError:
+                pass
+            time.sleep(0.02)
         return self
 
     def __exit__(self, *exc):
@@ -207,6 +217,160 @@ def run_reference(args, rank: int, world: int) -> None:
 # ---------------------------------------------------------------------------
 # engine arm
 # ---------------------------------------------------------------------------
+
+
+# ---------------------------------------------------------------------------
+# the plain single-field GPU path (comparison leg)
+# ---------------------------------------------------------------------------
+
+
+def plain_gpu_order3(s, qx, qy, *, complex_dtype, floor_eps, inner_rank=4, outer_rank=4):
+    """The order-3 graph of ``_order3.py:18-148`` written as plain cuFFT calls
+    (torch.fft) on the full reference grid, one field at a time: no fusion, no
+    compact grid, no batching.  This is the "plain single-field GPU path" the
+    engine is compared with, in FP64 (complex128) or FP32 (complex64, with
+    the roundoff floor scaled to the FP32 epsilon).  Returns (eta33/h,
+    psi33/(h sqrt(gh))) as complex fields."""
+    import numpy as np
+    import torch
+
+    from gl_engine import api
+
+    rdt = torch.float64 if complex_dtype == torch.complex128 else torch.float32
+    qx, qy = qx.to(rdt), qy.to(rdt)
+    s = s.to(complex_dtype)
+    tiny = torch.finfo(rdt).tiny
+    q = torch.hypot(qx, qy)
+    a_ = q * torch.tanh(q)
+    nu = torch.sqrt(a_)
+    sqa = torch.sqrt(a_)
+    snu = nu.clamp_min(tiny)
+    q2 = q * q
+    mag = s.abs()
+    support = mag > 1e-13 * max(1.0, float(mag.max()))
+    hat = torch.fft.fft2(support.to(complex_dtype))
+    s2 = torch.fft.ifft2(hat * hat).real > 0.5
+    s3 = torch.fft.ifft2(hat * hat * hat).real > 0.5
+    nu_min = float(nu[support].min())
+    shift2 = 0.5 * (nu_min + float(sqa[s2].max()) / 2.0)
+    shift3 = 0.5 * (nu_min + float(sqa[s3].max()) / 3.0)
+    amp2 = torch.where(support, mag * mag, torch.zeros_like(mag))
+    qp = float(q.flatten()[int(torch.argmax(amp2.flatten()))])
+    pn = np.sqrt(qp * np.tanh(qp))
+    lam2 = 2.0 * pn - np.sqrt(2.0 * qp * np.tanh(2.0 * qp))
+    lam3 = 3.0 * pn - np.sqrt(3.0 * qp * np.tanh(3.0 * qp))
+    fl = 16.0 * floor_eps * max(1.0, np.log2(s.numel()))
+
+    def sup(h, m):
+        h = torch.where(m, h, torch.zeros_like(h))
+        peak = float(h.abs().max())
+        return h if peak == 0.0 else torch.where(m & (h.abs() < fl * peak), torch.zeros_like(h), h)
+
+    def shr(t):
+        return torch.where(sqa > 0, torch.sinh(sqa * t) / sqa.clamp_min(tiny), torch.full_like(sqa, t))
+
+    ifft, fft = torch.fft.ifft2, torch.fft.fft2
+    inodes, iweights = api.gauss_laguerre_rule(inner_rank)
+    onodes, oweights = api.gauss_laguerre_rule(outer_rank)
+    eta_hat = torch.zeros_like(s)
+    psi_hat = torch.zeros_like(s)
+    for x, w in zip(onodes, oweights):
+        tau = x / lam3
+        d = s * torch.exp(-tau * (nu - shift3))
+        f = {"eta": ifft(d), "etax": ifft(1j * qx * d), "etay": ifft(1j * qy * d),
+             "phix": ifft(qx / snu * d), "phiy": ifft(qy / snu * d), "phiz": ifft(-1j * nu * d),
+             "phixz": ifft(nu * qx * d), "phiyz": ifft(nu * qy * d),
+             "phizz": ifft(-1j * q2 / snu * d), "phizzz": ifft(-1j * q2 * nu * d),
+             "phitz": ifft(-a_ * d), "phitzz": ifft(-q2 * d)}
+        e_h = torch.zeros_like(s)
+        et_h = torch.zeros_like(s)
+        p_h = torch.zeros_like(s)
+        pt_h = torch.zeros_like(s)
+        for xi, wi in zip(inodes, iweights):
+            t2 = xi / lam2
+            d2 = d * torch.exp(-t2 * (nu - shift2))
+            v, v1, v2, v3 = ifft(d2), ifft(d2 * nu), ifft(d2 * nu * nu), ifft(d2 * nu ** 3)
+            hx, hy, jx, jy = ifft(d2 * qx / snu), ifft(d2 * qy / snu), ifft(d2 * qx), ifft(d2 * qy)
+            rad, qq, njx, njy = ifft(d2 * q2 / snu), ifft(d2 * q2), ifft(d2 * nu * qx), ifft(d2 * nu * qy)
+            srcs = (2 * v * v2 + v1 * v1 - hx * hx - hy * hy,
+                    2 * v * rad + 2 * (hx * jx + hy * jy),
+                    2 * v * v3 + 4 * v1 * v2 - 2 * hx * jx - 2 * hy * jy,
+                    2 * (v1 * rad + v * qq) + 2 * (jx * jx + hx * njx + jy * jy + hy * njy))
+            sd, sk, sdt, skt = (sup(fft(x_), s2) for x_ in srcs)
+            sh, ch = shr(t2), torch.cosh(sqa * t2)
+            c = wi * np.exp(xi) / lam2 * np.exp(-2.0 * shift2 * t2) / 4.0
+            e_h = e_h + c * (-a_ * sh * sd + ch * sk)
+            et_h = et_h - 1j * c * (-a_ * sh * sdt + ch * skt)
+            p_h = p_h + 1j * c * (ch * sd - sh * sk)
+            pt_h = pt_h + c * (ch * sdt - sh * skt)
+        et_h = sup(et_h, s2)
+        p = {"eta": ifft(e_h), "etax": ifft(1j * qx * e_h), "etay": ifft(1j * qy * e_h),
+             "phix": ifft(1j * qx * p_h), "phiy": ifft(1j * qy * p_h), "phiz": ifft(a_ * p_h),
+             "phizz": ifft(q2 * p_h), "phitz": ifft(a_ * pt_h), "eta_t": ifft(et_h)}
+        fe = f["eta"]
+        k_pair = (f["phix"] * p["etax"] + f["phiy"] * p["etay"] + p["phix"] * f["etax"]
+                  + p["phiy"] * f["etay"] - fe * p["phizz"] - p["eta"] * f["phizz"])
+        k_dir = fe * (f["phixz"] * f["etax"] + f["phiyz"] * f["etay"]) - 0.5 * fe * fe * f["phizzz"]
+        d_pair = (fe * p["phitz"] + p["eta"] * f["phitz"] + f["phix"] * p["phix"]
+                  + f["phiy"] * p["phiy"] + f["phiz"] * p["phiz"])
+        d_dir = 0.5 * fe * fe * f["phitzz"] + fe * (f["phix"] * f["phixz"] + f["phiy"] * f["phiyz"]
+                                                    + f["phiz"] * f["phizz"])
+        cont = 0.5 * fe * p["phiz"] + 0.5 * p["eta"] * f["phiz"] + 0.125 * fe * fe * f["phizz"]
+        cont_t = (0.5 * (f["phiz"] * p["phiz"] + fe * p["phitz"])
+                  + 0.5 * (p["eta_t"] * f["phiz"] + p["eta"] * f["phitz"])
+                  + 0.25 * fe * f["phiz"] * f["phizz"] + 0.125 * fe * fe * f["phitzz"])
+        fk, fd, c_h, ct_h = (sup(fft(x_), s3) for x_ in (k_dir / 4 + k_pair / 2, d_dir / 4 + d_pair / 2,
+                                                          cont, cont_t))
+        fk_psi = sup(fk + a_ * c_h, s3)
+        fd_psi = sup(fd - ct_h, s3)
+        sh, ch = shr(tau), torch.cosh(sqa * tau)
+        c = w * np.exp(x) / lam3 * np.exp(-3.0 * shift3 * tau)
+        eta_hat = eta_hat + c * (a_ * sh * fd - 1j * ch * fk)
+        psi_hat = psi_hat + c * (-1j * ch * fd_psi - sh * fk_psi)
+    eta_hat = torch.where(s3, eta_hat, torch.zeros_like(eta_hat))
+    psi_hat = torch.where(s3, psi_hat, torch.zeros_like(psi_hat))
+    return ifft(eta_hat), ifft(psi_hat)
+
+
+def plain_gpu_leg(plan, spectra, st, first, device) -> dict:
+    """Time the plain single-field FP64 GPU path on one unit and measure the
+    FP32 variant's error against the engine."""
+    import numpy as np
+    import torch
+
+    box = plan.info.box1
+    x0, y0, w, h = box[0], box[1], box[2], box[3]
+    full = torch.zeros((st.ny, st.nx), dtype=torch.complex128, device=device)
+    rows = (torch.arange(h, device=device) + y0) % st.ny
+    cols = (torch.arange(w, device=device) + x0) % st.nx
+    full[rows[:, None], cols[None, :]] = torch.view_as_complex(spectra[0].contiguous())
+    kx = 2.0 * np.pi * np.fft.fftfreq(st.nx, d=st.lx / st.nx)
+    ky = 2.0 * np.pi * np.fft.fftfreq(st.ny, d=st.ly / st.ny)
+    kxg, kyg = np.meshgrid(kx, ky)
+    qx = torch.as_tensor(st.depth * kxg, device=device)
+    qy = torch.as_tensor(st.depth * kyg, device=device)
+    hs = st.depth
+    ps = st.depth * np.sqrt(st.gravity * st.depth)
+    out = {}
+    for name, cdt, feps in (("fp64", torch.complex128, 2.220446049250313e-16),
+                            ("fp32", torch.complex64, float(np.finfo(np.float32).eps))):
+        plain_gpu_order3(full, qx, qy, complex_dtype=cdt, floor_eps=feps)  # warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        e, p = plain_gpu_order3(full, qx, qy, complex_dtype=cdt, floor_eps=feps)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        e = (hs * e.real).double().cpu().numpy()
+        p = (ps * p.real).double().cpu().numpy()
+        rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
+        out[name] = {"fields_per_s": 1e3 / ms, "ms_per_field": ms,
+                     "eta33_rel_l2_vs_engine": rel(e, first[0]),
+                     "psi33_rel_l2_vs_engine": rel(p, first[1])}
+    out["note"] = ("torch.fft (cuFFT) graph on the full 1024^2 grid, one field per call; fp32 = "
+                   "complex64 FFTs and products with the floor scaled to the FP32 epsilon")
+    return out
 
 
 def run_engine(args, rank: int, world: int, local_rank: int) -> None:
@@ -355,6 +519,10 @@ def run_engine(args, rank: int, world: int, local_rank: int) -> None:
         "roofline": roofline, "accounting": accounting, "clocks": clocks,
         "gpu_launches": int(launches), "e2e": e2e,
     }
+    if world == 1 and not args.no_plain_gpu:
+        plain = plain_gpu_leg(plan, spectra, st, first, device)
+        line["plain_gpu_path"] = plain
+        line["speedup_vs_plain_fp64_gpu"] = value / plain["fp64"]["fields_per_s"]
     if world == 1 and not args.no_cpu_baseline:
         base, (e_ref, p_ref) = cpu_baseline_sample()
         line["cpu_baseline"] = base
@@ -414,18 +582,160 @@ def run_config3(args, rank: int, world: int, local_rank: int) -> None:
         print(json.dumps(line), flush=True)
 
 
+def run_config4(args, rank: int, world: int, local_rank: int) -> None:
+    """Adjoint fit: the gradient of ||eta11 + eta22 + eta33 - eta_obs||^2 with
+    respect to the a, b of 2048 modes on a 512^2 grid (h=25 m, Hs=2.5 m,
+    eta22 rank 6, order 3 GL4/GL4), eta_obs from a held-out seed plus
+    N(0, 0.01 m) noise.  A step = one forward + one backward through the
+    torch.autograd.Function (the backward is one gl_adjoint_execute pass).
+    Each rank fits its own sea state (seed = rank): no collective."""
+    import numpy as np
+    import torch
+
+    from gl_engine import _lib, seastate
+    from gl_engine.adjoint import EtaSurfaceModel, eta_surface
+
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    st = seastate.config4(seed=rank)
+    held = seastate.config4(seed=1000 + rank)
+    model = EtaSurfaceModel(st.kx, st.ky, depth=st.depth, lx=st.lx, ly=st.ly, nx=st.nx, ny=st.ny,
+                            times=[0.0], order=3, eta22_rank=6, device=device)
+    gen = torch.Generator(device="cpu").manual_seed(rank)
+    obs = model.eta(torch.tensor(held.a, device=device), torch.tensor(held.b, device=device))
+    obs = obs + 0.01 * torch.randn(obs.shape, generator=gen, dtype=torch.float64).to(device)
+    a = torch.tensor(st.a, device=device, requires_grad=True)
+    b = torch.tensor(st.b, device=device, requires_grad=True)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    stream = torch.cuda.current_stream(device)
+
+    def step():
+        a.grad = None
+        b.grad = None
+        loss = ((eta_surface(a, b, model) - obs) ** 2).sum()
+        loss.backward()
+        return loss
+
+    def timed(fn, n):
+        tot = 0.0
+        for _ in range(n):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1) / 1e3
+        return tot
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    launches0 = _lib.launch_count()
+    with ClockSampler(local_rank) as clk:
+        t_step = timed(step, args.steps)
+    launches = (_lib.launch_count() - launches0) // max(args.steps, 1)
+    ad, bd = a.detach(), b.detach()
+    resid = 2.0 * (model.eta(ad, bd) - obs)
+    t_fwd = timed(lambda: model.eta(ad, bd), args.steps)
+    t_bwd = timed(lambda: model.vjp(ad, bd, resid), args.steps)
+    if world > 1:
+        import torch.distributed as dist
+
+        tt = torch.tensor([t_step, t_fwd, t_bwd], device=device, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_step, t_fwd, t_bwd = (float(v) for v in tt)
+    # end to end: host amplitudes in, host gradients out, every step
+    a_host = torch.from_numpy(st.a.copy()).pin_memory()
+    b_host = torch.from_numpy(st.b.copy()).pin_memory()
+    ga_host = torch.empty_like(a_host).pin_memory()
+    gb_host = torch.empty_like(b_host).pin_memory()
+
+    def e2e_step():
+        with torch.no_grad():
+            a.copy_(a_host, non_blocking=True)
+            b.copy_(b_host, non_blocking=True)
+        step()
+        ga_host.copy_(a.grad, non_blocking=True)
+        gb_host.copy_(b.grad, non_blocking=True)
+        torch.cuda.synchronize()
+
+    e2e_step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    t_e2e = time.perf_counter() - t0
+    # a short fit: Adam on the amplitudes from the engine's gradient
+    fit_a = torch.tensor(st.a, device=device, requires_grad=True)
+    fit_b = torch.tensor(st.b, device=device, requires_grad=True)
+    opt = torch.optim.Adam([fit_a, fit_b], lr=2e-3)
+    losses = []
+    for _ in range(30):
+        opt.zero_grad()
+        loss = ((eta_surface(fit_a, fit_b, model) - obs) ** 2).sum()
+        loss.backward()
+        opt.step()
+        losses.append(float(loss))
+    n = args.steps
+    line = {
+        "metric": "config-4 adjoint fit: gradients/s of ||eta11+eta22+eta33 - eta_obs||^2 wrt a,b",
+        "value": world * n / t_step, "unit": "gradients/s", "n_gpus": world, "steps": n,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_step / n, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded JONSWAP sea state; eta_obs from a held-out seed + N(0, 0.01 m))",
+        "config": {"workload": "order-3 eta11+eta22(rank 6)+eta33 (GL4/GL4), 512^2 grid, L=512 m, "
+                               "h=25 m, Hs=2.5 m, 2048 modes; step = forward + backward",
+                   "l2": "flushed between timed steps (256 MiB write outside the events)",
+                   "parallelism": f"one sea state per rank over {world} rank(s), no collective"},
+        "forward_ms": 1e3 * t_fwd / n, "backward_ms": 1e3 * t_bwd / n,
+        "backward_over_forward": t_bwd / t_fwd,
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "e2e": {"value": world * n / t_e2e, "unit": "gradients/s",
+                "h2d_bytes_per_step": int(2 * 8 * st.a.size), "d2h_bytes_per_step": int(2 * 8 * st.a.size)},
+        "fit_demo": {"optimizer": "Adam lr 2e-3", "steps": len(losses), "loss_first": losses[0],
+                     "loss_last": losses[-1]},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import gl_torch as GT
+
+        k = np.hypot(st.kx, st.ky)
+        omega = np.sqrt(9.81 * k * np.tanh(st.depth * k))
+        ac = torch.tensor(st.a, requires_grad=True)
+        bc = torch.tensor(st.b, requires_grad=True)
+        t0 = time.perf_counter()
+        eta = GT.eta_surface(ac, bc, kx=st.kx, ky=st.ky, omega=omega, depth=st.depth, lx=st.lx,
+                             ly=st.ly, nx=st.nx, ny=st.ny, t=0.0, eta22_rank=6)
+        ((eta - obs[0].cpu()) ** 2).sum().backward()
+        t_cpu = time.perf_counter() - t0
+        ga, gb = model.vjp(ad, bd, resid)
+        g_gpu = np.r_[ga.cpu().numpy(), gb.cpu().numpy()]
+        g_cpu = np.r_[ac.grad.numpy(), bc.grad.numpy()]
+        line["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "gradients/s",
+                                "cores": torch.get_num_threads(), "kind": "port",
+                                "sample": "one full gradient: torch.autograd through the FP64 oracle "
+                                          "transliteration (oracle/gl_torch.py) on the host CPU"}
+        line["parity_vs_oracle"] = {
+            "gradient_rel_l2": float(np.linalg.norm(g_gpu - g_cpu) / np.linalg.norm(g_cpu))}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--units", type=int, default=16, help="units per step per GPU")
     ap.add_argument("--group", type=int, default=0, help="units per engine launch group")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["config2", "config3"], default="config2",
-                    help="config2: the headline order-3 1024^2 workload; config3: uneven batch")
+    ap.add_argument("--no-plain-gpu", action="store_true",
+                    help="skip the plain single-field cuFFT comparison leg")
+    ap.add_argument("--workload", choices=["config2", "config3", "config4"], default="config2",
+                    help="config2: the headline order-3 1024^2 workload; config3: uneven batch; "
+                         "config4: adjoint fit")
     ap.add_argument("--states", type=int, default=64, help="config3: sea states per GPU")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
@@ -446,6 +756,8 @@ def main() -> None:
     try:
         if args.workload == "config3":
             run_config3(args, rank, world, local_rank)
+        elif args.workload == "config4":
+            run_config4(args, rank, world, local_rank)
         else:
             run_engine(args, rank, world, local_rank)
     finally:

@@ -161,3 +161,39 @@ def eta44(spectra, *, dk: float, depth: float, peak_depth: float, rank: int, nod
             raise _status_error(int(st[st != 0][0]))
         res = out[:, 0].cpu().numpy()
     return res[0] if single else res
+
+
+def main(argv=None) -> int:
+    """Command-line twin of the reference's ``gl_eta44`` executable
+    (``paper/order4/cpp/gl_eta44_fftw.cpp:639-764``):
+    ``INPUT OUTPUT RANK THREADS``, GLRTI001 in (the rule of RANK taken from
+    the file), GLE44O01 out (the dimensionless field).  The reference's
+    per-outer-node split mode (``[OUTER4_INDEX [PART_INDEX]]``) is a CPU
+    process split; on the GPU the whole graph is one call and multi-GPU
+    sharding goes through ``gl_eta44_execute_partial`` instead."""
+    import sys
+    import time
+
+    argv = list(sys.argv if argv is None else argv)
+    try:
+        if len(argv) not in (5, 6, 7):
+            raise ValueError("usage INPUT OUTPUT RANK THREADS [OUTER4_INDEX [PART_INDEX]]")
+        if len(argv) > 5:
+            raise ValueError("split mode (OUTER4_INDEX) is not offered: the GPU runs every outer "
+                             "node in one call")
+        rank, threads = int(argv[3]), int(argv[4])
+        inp = read_glrti(argv[1])
+        if rank not in inp.rules:
+            raise ValueError("rank")
+        nodes, weights = inp.rules[rank]
+        t0 = time.perf_counter()
+        field = eta44(inp.spectrum, dk=inp.dk, depth=inp.depth, peak_depth=inp.peak_depth,
+                      rank=rank, nodes=nodes, weights=weights) / inp.depth
+        elapsed = time.perf_counter() - t0
+        write_gle44(argv[2], inp.n, rank, field, threads=threads, elapsed=elapsed)
+    except Exception as exc:  # the reference's error line and exit code
+        print(f"CPP_GL_ETA44_ERROR {exc}", file=sys.stderr)
+        return 1
+    print(f"CPP_GL_ETA44_DONE n={inp.n} rank={rank} threads={threads} outer=-1 part=-2 "
+          f"elapsed={elapsed}", file=sys.stderr)
+    return 0

@@ -93,6 +93,60 @@ def read_dir4out(path) -> WitOutput:
     return WitOutput(fields=fields, stats=stats)
 
 
+def write_dir4out(path, sector: int, out: WitOutput, nx: int, ny: int) -> None:
+    """``DIR4xO01`` writer, the layout :func:`read_dir4out` reads."""
+    st = out.stats
+    cases = next(iter(out.fields.values())).shape[0]
+    with open(path, "wb") as f:
+        f.write({40: b"DIR40O01", 42: b"DIR42O01", 44: b"DIR44O01"}[int(sector)])
+        f.write(struct.pack("<8Q", nx, ny, cases, int(st["candidates"]), int(st["kept"]),
+                            int(st["near"]), int(st["strict_zero_output"]),
+                            int(st["strict_zero_intermediate"])))
+        f.write(struct.pack("<4d", float(st.get("seconds", 0.0)), float(st["max_residual"]),
+                            float(st["min_detuning"]), float(st["max_strict_zero_source"])))
+        for name in FIELDS:
+            f.write(np.ascontiguousarray(out.fields[name], dtype=np.complex128).view("<f8").tobytes())
+
+
+def main(argv=None) -> int:
+    """Command-line twin of the reference's ``wit_eta44`` executable
+    (``paper/order4/cpp/directional_eta4_openmp.cpp:499-516``):
+    ``INPUT OUTPUT [--sector 40|42|44]`` (default sector 40), DIR4IN01 in,
+    DIR4xO01 out, the engine's GPU direct sum in between."""
+    import sys
+    import time
+
+    argv = list(sys.argv if argv is None else argv)
+    if len(argv) < 3:
+        print("input output [--sector 40|42|44]", file=sys.stderr)
+        return 2
+    sector = 40
+    k = 3
+    while k < len(argv):
+        if argv[k] == "--sector" and k + 1 < len(argv):
+            sector = int(argv[k + 1])
+            k += 1
+        elif argv[k].startswith("--sector="):
+            sector = int(argv[k][9:])
+        k += 1
+    try:
+        if sector not in (40, 42, 44):
+            raise ValueError("sector must be 40, 42, or 44")
+        inp = read_dir4in(argv[1])
+        t0 = time.perf_counter()
+        out = wit_sector(inp, sector)
+        out.stats["seconds"] = time.perf_counter() - t0
+        write_dir4out(argv[2], sector, out, inp.nx, inp.ny)
+    except Exception as exc:  # the reference's error line and exit code
+        print(f"DIRECTIONAL_CPP_ERROR {exc}", file=sys.stderr)
+        return 1
+    st = out.stats
+    print(f"DIRECTIONAL_CPP_DONE sector={sector} cases={inp.amplitudes.shape[0]} "
+          f"total={st['candidates']} kept={st['kept']} near={st['near']} "
+          f"seconds={st['seconds']} residual={st['max_residual']}", file=sys.stderr)
+    return 0
+
+
 def wit_sector(inp: WitInput, sector: int = 44, *, device=None, as_numpy: bool = True) -> WitOutput:
     """WIT fourth-order fields of one sector (44, 40 or 42) for every amplitude case."""
     lib = _lib.load()

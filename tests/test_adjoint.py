@@ -173,14 +173,15 @@ def test_adjoint_matches_central_fd_of_engine():
 
 
 @pytest.mark.gpu
-def test_adjoint_config4_directional_derivative():
-    """Full-size fit (512^2, 2048 modes, h=25 m): a size-independent check,
-    central differences of the loss along a random direction against
-    <grad, direction>.  The map is piecewise polynomial: when a step moves a
-    bin across a roundoff floor, the order-3 field jumps by ~1e-7 of its size
-    (the oracle shows the same spread), which spoils that one difference
-    quotient (measured here: 1.8e-4 at one step, 4e-7 .. 4e-6 at the others).
-    So several steps are taken and their median discrepancy is tested."""
+def test_adjoint_config4_full_size():
+    """The config-4 fit at full size (512^2, 2048 modes, h=25 m, eta22 rank 6):
+    the engine's gradient against the autograd oracle on the host (~1 s with
+    all cores), and the directional central difference along a random
+    direction.  The map is piecewise polynomial: when a step moves a bin
+    across a roundoff floor the order-3 field jumps by ~1e-7 of its size (the
+    oracle shows the same spread), so at this size difference quotients scatter
+    by 1e-5 .. 1e-4 around the derivative whatever the step; the oracle
+    gradient is the tight check, the differences a loose one."""
     st = seastate.config4(seed=0)
     held = seastate.config4(seed=1000)
     model = _model(st, [0.0], ("eta11", "eta22", "eta33"), eta22_rank=6)
@@ -189,18 +190,23 @@ def test_adjoint_config4_directional_derivative():
     obs = obs + 0.01 * torch.randn(obs.shape, generator=gen, dtype=torch.float64).cuda()
     a0 = torch.tensor(st.a, device="cuda")
     b0 = torch.tensor(st.b, device="cuda")
+    ga, gb = model.vjp(a0, b0, 2.0 * (model.eta(a0, b0) - obs))
+    g = np.r_[ga.cpu().numpy(), gb.cpu().numpy()]
+    _, ga_ref, gb_ref = _oracle_grad(st, obs[0].cpu().numpy(), 0.0, ("eta11", "eta22", "eta33"),
+                                     eta22_rank=6)
+    err = rel(g, np.r_[ga_ref, gb_ref])
+    print(f"config-4 gradient rel L2 vs autograd oracle: {err:.2e}")
+    assert err < 1e-7
+
     da = torch.randn(a0.shape, generator=gen, dtype=torch.float64).cuda() * a0.abs().mean()
     db = torch.randn(b0.shape, generator=gen, dtype=torch.float64).cuda() * b0.abs().mean()
 
     def loss(a, b):
         return float(((model.eta(a, b) - obs) ** 2).sum())
 
-    ga, gb = model.vjp(a0, b0, 2.0 * (model.eta(a0, b0) - obs))
     an = float((ga * da).sum() + (gb * db).sum())
-    errs = []
-    for eps in (1e-5, 1e-4, 1e-3, 1e-2):
+    for eps in (1e-4, 1e-2):
         fd = (loss(a0 + eps * da, b0 + eps * db) - loss(a0 - eps * da, b0 - eps * db)) / (2 * eps)
-        errs.append(abs(an - fd) / abs(an))
         print(f"config-4 directional derivative, step {eps:.0e}: adjoint {an:.10e}, "
-              f"central FD {fd:.10e}, rel {errs[-1]:.1e}")
-    assert float(np.median(errs)) < 1e-5
+              f"central FD {fd:.10e}, rel {abs(an - fd) / abs(an):.1e}")
+        assert abs(an - fd) / abs(an) < 1e-3
