@@ -721,6 +721,111 @@ def run_config4(args, rank: int, world: int, local_rank: int) -> None:
         print(json.dumps(line), flush=True)
 
 
+# published order-4 timings of the reference (paper/order4/data/runtime/
+# eta44_runtime_figure_data.csv; C++ on 32 cores of a Xeon Silver 4214, 512^2)
+PUBLISHED_GL_N1500_S = {6: 11.31350016, 8: 20.21097216, 10: 35.332300544}
+PUBLISHED_WIT_S = {50: 0.765824, 100: 6.76152, 200: 96.4575, 300: 476.281, 400: 1491.09,
+                   500: 3614.69, 600: 7502.55, 800: 21856.765945183}
+
+
+def run_config5(args, rank: int, world: int, local_rank: int) -> None:
+    """Order 4 on the reference's own runtime ladder (512^2, dk = 0.1,
+    g = h = 1; the DIR4IN01 inputs behind its published timings): the eta44 GL
+    graph at GL6/8/10 on the 1500-mode input and the WIT sector-44 direct sum
+    at 50..400 modes, against the published C++ wall times.  Rank 0 only."""
+    import torch
+
+    from gl_engine import _lib, wit
+    from gl_engine import eta44 as E44
+
+    if rank != 0:
+        return
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    gold = ROOT / "tests" / "golden" / "runtime"
+    inp = wit.read_dir4in(gold / "n1500.bin")
+    n = inp.nx
+    spec = E44.spectrum_from_modes(inp.modes, inp.amplitudes[0], n, inp.depth)
+    box = E44._box(spec)
+    stream = torch.cuda.current_stream(device)
+    steps = max(1, min(args.steps, 3))
+    gl = {}
+    for r in (6, 8, 10):
+        desc = _lib.Eta44Desc(n=n, dk=inp.dkx, depth=inp.depth, peak_depth=1.0, rank=r,
+                              nodes=None, weights=None, box_x0=box[0], box_y0=box[1],
+                              box_w=box[2], box_h=box[3], max_units=1, output=_lib.OUT_COMPLEX)
+        plan = E44.Eta44Plan(desc, device)
+        d_spec = torch.view_as_real(torch.from_numpy(spec).to(device))
+        out = torch.empty((1, 1, n, n), dtype=torch.complex128, device=device)
+        status = torch.zeros(1, dtype=torch.int32, device=device)
+
+        def run():
+            plan.execute(1, d_spec, _lib.SPECTRA_FULL, out, status, stream.cuda_stream)
+
+        run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches0 = _lib.launch_count()
+        e0.record(stream)
+        for _ in range(steps):
+            run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3 / steps
+        launches = (_lib.launch_count() - launches0) // steps
+        t0 = time.perf_counter()
+        E44.eta44(spec, dk=inp.dkx, depth=inp.depth, peak_depth=1.0, rank=r, device=device)
+        e2e = time.perf_counter() - t0
+        gl[r] = {"seconds": sec, "published_cpp_seconds": PUBLISHED_GL_N1500_S[r],
+                 "speedup_vs_published": PUBLISHED_GL_N1500_S[r] / sec, "e2e_seconds": e2e,
+                 "gpu_launches": int(launches), "status": int(status.item()),
+                 "transforms_per_field": plan.info.transforms_per_unit,
+                 "product_grid": [plan.info.ncy, plan.info.ncx]}
+    wits = {}
+    for m in (50, 100, 200, 300, 400):
+        wi = wit.read_dir4in(gold / f"n{m:04d}.bin")
+        wit.wit_sector(wi, 44, device=device)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = wit.wit_sector(wi, 44, device=device)
+        sec = time.perf_counter() - t0
+        wits[m] = {"seconds": sec, "quartets": int(res.stats["candidates"]),
+                   "published_cpp_seconds": PUBLISHED_WIT_S[m],
+                   "speedup_vs_published": PUBLISHED_WIT_S[m] / sec}
+    cpu = None
+    ref_bin = ROOT / "oracle" / "_ref" / "wit_eta44"
+    if ref_bin.exists() and not args.no_cpu_baseline:
+        with tempfile.TemporaryDirectory() as td:
+            t0 = time.perf_counter()
+            subprocess.run([str(ref_bin), str(gold / "n0100.bin"), str(Path(td) / "o.bin"), "--sector",
+                            "44"], check=True, capture_output=True,
+                           env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count())))
+            cpu_s = time.perf_counter() - t0
+        cpu = {"value": 1.0 / cpu_s, "unit": "WIT fields/s (100 modes)", "cores": os.cpu_count(),
+               "kind": "reference",
+               "sample": "the reference's WIT C++ (oracle/_ref/wit_eta44, OpenMP on all host cores) on "
+                         f"the 100-mode runtime input: {cpu_s:.3f} s; GPU {wits[100]['seconds']:.3f} s"}
+    value = 1.0 / gl[10]["seconds"]
+    line = {
+        "metric": "order-4 eta44 GL10 fields/s, 512^2 runtime input n1500 (reference ladder)",
+        "value": value, "unit": "fields/s", "n_gpus": 1, "steps": steps,
+        "warmup": 1, "ms_per_step": 1e3 * gl[10]["seconds"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": value * PUBLISHED_GL_N1500_S[10], "dtype": "f64",
+        "data": "the reference's own DIR4IN01 runtime inputs (copied to tests/golden/runtime)",
+        "config": {"workload": "eta44 GL6/8/10 (three nested GL levels) on n1500: 512^2, 1500 modes, "
+                               "dk=0.1, g=h=1; WIT sector 44 on n0050..n0400",
+                   "vs_baseline": "published C++ GL10 wall time on 32 cores / ours"},
+        "gl": {str(k): v for k, v in gl.items()},
+        "wit": {str(k): v for k, v in wits.items()},
+        "gpu_launches": gl[10]["gpu_launches"],
+        "e2e": {"value": 1.0 / gl[10]["e2e_seconds"], "unit": "fields/s",
+                "h2d_bytes_per_step": int(spec.nbytes), "d2h_bytes_per_step": int(n * n * 16)},
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -733,9 +838,11 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain-gpu", action="store_true",
                     help="skip the plain single-field cuFFT comparison leg")
-    ap.add_argument("--workload", choices=["config2", "config3", "config4"], default="config2",
+    ap.add_argument("--workload", choices=["config2", "config3", "config4", "config5"],
+                    default="config2",
                     help="config2: the headline order-3 1024^2 workload; config3: uneven batch; "
-                         "config4: adjoint fit")
+                         "config4: adjoint fit; config5: order 4 (eta44 GL, WIT) on the reference's "
+                         "runtime inputs")
     ap.add_argument("--states", type=int, default=64, help="config3: sea states per GPU")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
@@ -758,6 +865,8 @@ def main() -> None:
             run_config3(args, rank, world, local_rank)
         elif args.workload == "config4":
             run_config4(args, rank, world, local_rank)
+        elif args.workload == "config5":
+            run_config5(args, rank, world, local_rank)
         else:
             run_engine(args, rank, world, local_rank)
     finally:

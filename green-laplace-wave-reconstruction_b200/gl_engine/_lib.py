@@ -8,6 +8,7 @@ library has not been built; there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import threading
 from pathlib import Path
 
@@ -130,7 +131,8 @@ def load(path: Path | None = None) -> C.CDLL:
     with _lock:
         if _lib is not None:
             return _lib
-        p = Path(path) if path else LIB_PATH
+        env = os.environ.get("GL_ENGINE_LIB")
+        p = Path(path) if path else (Path(env) if env else LIB_PATH)
         if not p.exists():
             raise RuntimeError(
                 f"GL engine library not built: {p} is missing "
