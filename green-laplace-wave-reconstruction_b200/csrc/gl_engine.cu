@@ -656,6 +656,7 @@ struct gl_plan {
   size_t scratch_bytes;
   // fourth-order eta44 plans (gl_eta44_plan_create)
   bool e44 = false;
+  bool e44_psi = false;         // psi44 requested with eta44
   int R44 = 0;
   double dk44 = 0.0, peak44 = 0.0;
   Box b4;
@@ -962,6 +963,9 @@ extern "C" gl_status gl_plan_get_info(const gl_plan* p, gl_plan_info* info) {
     const double R = p->R44;
     const double pair = R * (16 + 6) + 18;
     t = R * (R * (16 + (R * (16 + 6) + 15) + 4) + 8 + 19 + pair + 2) + 1;
+    // psi44: the third-level eta_t (its accumulation and bank), the two contact
+    // rows of every outer node and the final psi44 transform
+    if (p->e44_psi) t += R * (1 + 2) + 1;
   }
   info->transforms_per_unit = t;
   return GL_OK;
@@ -1010,11 +1014,13 @@ static gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, c
 static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
   int nb = 0;
   for (int g = 0; g < a.ngrp; ++g) nb += a.grp[g].nb;
+  const bool e44 = a.kind >= ROW_E44_PAIR && a.kind <= ROW_E44_ORDER4_PSI;
   const size_t smem = row_smem(nb, a.nx);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(row_kernel_t<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
     cudaFuncSetAttribute(row_kernel_t<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    cudaFuncSetAttribute(row_kernel_t<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
     attr = true;
   }
   dim3 grid(a.ny, njobs);
@@ -1035,6 +1041,8 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
   LaunchScope ls(name, st, bytes);
   if (adj)
     row_kernel_t<1><<<grid, threads, smem, st>>>(a, tw);
+  else if (e44)
+    row_kernel_t<2><<<grid, threads, smem, st>>>(a, tw);
   else
     row_kernel_t<0><<<grid, threads, smem, st>>>(a, tw);
   LAUNCH_CHECK("row_kernel");
@@ -1806,8 +1814,9 @@ static const int E44_POUT_MULT[18] = {M_ONE, M_IQX, M_IQY, M_ONE, M_IQX, M_IQY, 
                                       M_Q2, M_A, M_IQX, M_IQY, M_Q2, M_A, M_IQXA, M_IQYA, M_Q2A};
 static const int E44_POUT_SRC[18] = {0, 0, 0, 1, 1, 1, 2, 2, 2, 2, 3, 3, 3, 3, 4, 2, 2, 2};
 // third outputs from (es, ps, pts) = sources 0..2
-static const int E44_TOUT_MULT[8] = {M_ONE, M_IQX, M_IQY, M_IQX, M_IQY, M_A, M_Q2, M_A};
-static const int E44_TOUT_SRC[8] = {0, 0, 0, 1, 1, 1, 1, 2};
+// third-state banks: eta ex ey px py pz pzz pzt [eta_t] from (es, ps, pts [, ets])
+static const int E44_TOUT_MULT[9] = {M_ONE, M_IQX, M_IQY, M_IQX, M_IQY, M_A, M_Q2, M_A, M_ONE};
+static const int E44_TOUT_SRC[9] = {0, 0, 0, 1, 1, 1, 1, 2, 3};
 
 struct E44Layout {
   size_t E, maxE, T, maxT, OUT, maxOUT, transient;
@@ -1819,14 +1828,15 @@ static E44Layout e44_layout(const gl_plan* p, int g) {
   const size_t b2 = (size_t)p->b2.w * p->b2.h, b3 = (size_t)p->b3.w * p->b3.h,
                b4 = (size_t)p->b4.w * p->b4.h;
   const size_t JP = R * R * R + R * R, GP = R * R + R;
+  const size_t nts = p->e44_psi ? 4 : 3, nout = p->e44_psi ? 2 : 1;
   E44Layout L;
   Bump b;
   L.E = b.take(g * GP * 5 * b2 * c);
   L.maxE = b.take(g * GP * 5 * 8);
-  L.T = b.take(g * R * 3 * b3 * c);
-  L.maxT = b.take(g * R * 3 * 8);
-  L.OUT = b.take(g * b4 * c);
-  L.maxOUT = b.take(g * 8);
+  L.T = b.take(g * R * nts * b3 * c);
+  L.maxT = b.take(g * R * nts * 8);
+  L.OUT = b.take(g * nout * b4 * c);
+  L.maxOUT = b.take(g * nout * 8);
   L.transient = b.off;
   size_t need = 0;
   {  // pair stage
@@ -1847,16 +1857,17 @@ static E44Layout e44_layout(const gl_plan* p, int g) {
     need = std::max(need, t.off);
   }
   {  // order-4 stage
+    const size_t nf = p->e44_psi ? 4 : 2;
     Bump t;
     t.take(g * R * 19 * p->b1.w * ncy * c);
     t.take(g * R * 18 * p->b2.w * ncy * c);
-    t.take(g * R * 8 * p->b3.w * ncy * c);
-    t.take(g * R * 2 * p->b4.w * ncy * c);
-    t.take(g * R * 2 * b4 * c);
-    t.take(g * R * 2 * 8);
+    t.take(g * R * (nts + 5) * p->b3.w * ncy * c);
+    t.take(g * R * nf * p->b4.w * ncy * c);
+    t.take(g * R * nf * b4 * c);
+    t.take(g * R * nf * 8);
     need = std::max(need, t.off);
   }
-  need = std::max(need, (size_t)g * p->b4.w * p->d.ny * c);  // final column transforms
+  need = std::max(need, (size_t)g * nout * p->b4.w * p->d.ny * c);  // final column transforms
   L.total = L.transient + need;
   return L;
 }
@@ -1875,6 +1886,12 @@ extern "C" gl_status gl_eta44_plan_create(gl_plan** out, const gl_eta44_desc* de
     return fail(GL_ERR_INVALID_ARGUMENT, "unknown output mode");
   if (e.box_w < 1 || e.box_h < 1) return fail(GL_ERR_INVALID_ARGUMENT, "empty parent box");
   if (e.box_x0 < 1) return fail(GL_ERR_SUPPORT, "strict-forward nonzero analytic eta1 support is required");
+  const int comps44 = e.components ? e.components : GL_COMP_ETA44;
+  if (!(comps44 & GL_COMP_ETA44) || (comps44 & ~(GL_COMP_ETA44 | GL_COMP_PSI44)))
+    return fail(GL_ERR_INVALID_ARGUMENT, "fourth-order components: eta44 with optional psi44");
+  const bool want_psi = comps44 & GL_COMP_PSI44;
+  if (want_psi && !(e.gravity > 0))
+    return fail(GL_ERR_INVALID_ARGUMENT, "psi44 needs a positive gravity");
   const int xmax = e.box_x0 + e.box_w - 1;
   const int ymax = std::max(std::abs(e.box_y0), std::abs(e.box_y0 + e.box_h - 1));
   if (4 * xmax >= e.n / 2 || 4 * ymax >= e.n / 2)
@@ -1897,8 +1914,10 @@ extern "C" gl_status gl_eta44_plan_create(gl_plan** out, const gl_eta44_desc* de
   p->dk44 = e.dk;
   p->peak44 = e.peak_depth;
   p->comps = 0;
-  p->ncomp = 1;
+  p->e44_psi = want_psi;
+  p->ncomp = want_psi ? 2 : 1;
   p->comp_ids[0] = GL_COMP_ETA44;
+  p->comp_ids[1] = GL_COMP_PSI44;
   p->b1 = Box{e.box_x0, e.box_y0, e.box_w, e.box_h};
   p->b2 = Box{2 * e.box_x0, 2 * e.box_y0, 2 * (e.box_w - 1) + 1, 2 * (e.box_h - 1) + 1};
   p->b3 = Box{3 * e.box_x0, 3 * e.box_y0, 3 * (e.box_w - 1) + 1, 3 * (e.box_h - 1) + 1};
@@ -1911,10 +1930,12 @@ extern "C" gl_status gl_eta44_plan_create(gl_plan** out, const gl_eta44_desc* de
   p->lncx = ilog2(p->ncx);
   p->lncy = ilog2(p->ncy);
   p->lnx = p->lny = ilog2(e.n);
-  if (row_smem(45, p->ncx) > SMEM_LIMIT) {
+  const int row_banks = want_psi ? 46 : 45;
+  if (row_smem(row_banks, p->ncx) > SMEM_LIMIT) {
     plan_free(p);
     return fail(GL_ERR_UNSUPPORTED,
-                "eta44 product grid width %d exceeds the shared-memory row budget (45 banks)", p->ncx);
+                "eta44 product grid width %d exceeds the shared-memory row budget (%d banks)", p->ncx,
+                row_banks);
   }
   p->floor_rel = 16.0 * 2.220446049250313e-16 * std::max(1.0, std::log2((double)e.n * (double)e.n));
   if (e.nodes && e.weights) {
@@ -1930,6 +1951,8 @@ extern "C" gl_status gl_eta44_plan_create(gl_plan** out, const gl_eta44_desc* de
     }
   }
   p->h_comp_scale[0] = e.depth;
+  p->h_comp_scale[1] = want_psi ? e.depth * std::sqrt(e.gravity * e.depth) : 0.0;
+  if (want_psi) p->d.gravity = e.gravity;
   cudaError_t err = cudaSuccess;
   auto geo_alloc = [&](double** g, const Box& b) {
     if (err == cudaSuccess) err = cudaMalloc(g, sizeof(double) * 6 * b.w * b.h);
@@ -1988,18 +2011,20 @@ extern "C" gl_status gl_eta44_plan_create(gl_plan** out, const gl_eta44_desc* de
   return GL_OK;
 }
 
-__global__ void plane_max_kernel(const cplx* x, int plane, unsigned long long* out) {
+// max |x| of the first plane of each unit (units `stride` planes apart) into
+// out[u * stride]
+__global__ void plane_max_kernel(const cplx* x, int plane, int stride, unsigned long long* out) {
   const int u = blockIdx.y;
   double l = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
-    const double m = cabs_(x[(size_t)u * plane + i]);
+    const double m = cabs_(x[(size_t)u * stride * plane + i]);
     l = (m > l || m != m) ? m : l;
   }
   for (int o = 16; o > 0; o >>= 1) {
     const double other = __shfl_xor_sync(0xffffffffu, l, o);
     l = (other > l || other != other) ? other : l;
   }
-  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out + u, l);
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out + (size_t)u * stride, l);
 }
 
 // Final roundoff floor of the summed order-4 spectra and transform to the
@@ -2010,30 +2035,33 @@ static gl_status e44_finalize(gl_plan* p, int gu, const cplx* OUT, unsigned long
   const int T = 256;
   const Box B4 = p->b4;
   const int pl4 = B4.w * B4.h;
+  const int nout = p->e44_psi ? 2 : 1;  // eta44 [, psi44]: only eta44 is floored
   gl_status s;
   if (!max_ready) {
-    CUDA_TRY(cudaMemsetAsync(maxOUT, 0, (size_t)gu * 8, st));
+    CUDA_TRY(cudaMemsetAsync(maxOUT, 0, (size_t)gu * nout * 8, st));
     dim3 g(grid_for(pl4, T, 64), gu);
     {
       LaunchScope ls_("plane_max_kernel", st, 0.0);
-      plane_max_kernel<<<g, T, 0, st>>>(OUT, pl4, maxOUT);
+      plane_max_kernel<<<g, T, 0, st>>>(OUT, pl4, nout, maxOUT);
     }
     LAUNCH_CHECK("plane_max_kernel");
   }
-  const int m1[1] = {M_ONE};
   ColArgs a;
   std::memset(&a, 0, sizeof a);
   a.kind = COL_FLOORED;
-  a.nbanks = 1;
-  a.mult[0] = m1[0];
-  a.src_of[0] = 0;
+  a.nbanks = nout;
+  for (int k = 0; k < nout; ++k) {
+    a.mult[k] = M_ONE;
+    a.src_of[k] = k;
+  }
   a.box = B4;
   a.geo = p->geo4;
   a.spec = OUT;
-  a.spec_job_stride = pl4;
+  a.spec_job_stride = (long long)nout * pl4;
+  a.spec_sub_stride = pl4;
   a.jobs_per_unit = 1;
-  a.floor_max = maxOUT;
-  a.floor_nsrc = 1;
+  a.floor_max = maxOUT;  // the psi44 slot stays 0: no floor
+  a.floor_nsrc = nout;
   a.floor_rel = p->floor_rel;
   a.out = reinterpret_cast<cplx*>(tr);
   a.n = p->d.ny;
@@ -2048,15 +2076,15 @@ static gl_status e44_finalize(gl_plan* p, int gu, const cplx* OUT, unsigned long
   o.nx = p->d.nx;
   o.log2nx = p->lnx;
   o.ny = p->d.ny;
-  o.ncomp = 1;
+  o.ncomp = nout;
   o.comp_offset = 0;
-  o.out_ncomp = 1;
+  o.out_ncomp = nout;
   o.comp_scale = p->comp_scale;
   o.out = outputs;
   o.real_only = p->d.output == GL_OUT_REAL;
-  if ((s = launch_out_rows(o, gu, st, p->tw)) != GL_OK) return s;
+  if ((s = launch_out_rows(o, gu * nout, st, p->tw)) != GL_OK) return s;
   if (us) {
-    const size_t per_unit = (size_t)p->d.nx * p->d.ny;
+    const size_t per_unit = (size_t)nout * p->d.nx * p->d.ny;
     dim3 g(grid_for(per_unit, T, 256), gu);
     {
       LaunchScope ls_("nonfinite_kernel", st, 0.0);
@@ -2209,9 +2237,13 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
   const double inv_scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
   const int ncy = p->ncy;
   const int JP = Ro * R * R + Ro * R, GP = Ro * R + Ro;
+  const bool psi = p->e44_psi;
+  const int nts = psi ? 4 : 3;   // third-state spectra: es, ps, pts [, ets]
+  const int nf4 = psi ? 4 : 2;   // order-4 rows: fk, fd [, contact, contact_t]
+  const int nout = psi ? 2 : 1;  // accumulated spectra: eta44 [, psi44]
   CUDA_TRY(cudaMemsetAsync(maxE, 0, (size_t)gu * GP * 5 * 8, st));
-  CUDA_TRY(cudaMemsetAsync(maxT, 0, (size_t)gu * R * 3 * 8, st));
-  CUDA_TRY(cudaMemsetAsync(maxOUT, 0, (size_t)gu * 8, st));
+  CUDA_TRY(cudaMemsetAsync(maxT, 0, (size_t)gu * R * nts * 8, st));
+  CUDA_TRY(cudaMemsetAsync(maxOUT, 0, (size_t)gu * nout * 8, st));
 
   auto colargs = [&](int kind, int nb, const int* mults, const int* srcs, const Box& box,
                      const double* geo, const cplx* sp, long long job_stride, long long sub_stride,
@@ -2358,6 +2390,7 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     c.Ro = Ro;
     c.outer0 = o0;
     c.floor_rel = p->floor_rel;
+    c.nspec = nts;
     dim3 g(grid_for(pl3, T, 64), gu * Ro);
     {
       LaunchScope ls_("acc_e44_third_kernel", st, 0.0);
@@ -2371,11 +2404,12 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     Bump b;
     cplx* PF = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 19 * B1.w * ncy * sizeof(cplx)));
     cplx* PP = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 18 * B2.w * ncy * sizeof(cplx)));
-    cplx* PT = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 8 * B3.w * ncy * sizeof(cplx)));
-    cplx* Q = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 2 * B4.w * ncy * sizeof(cplx)));
-    cplx* R4 = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 2 * pl4 * sizeof(cplx)));
-    unsigned long long* mR4 = reinterpret_cast<unsigned long long*>(tr + b.take((size_t)nj * 2 * 8));
-    CUDA_TRY(cudaMemsetAsync(mR4, 0, (size_t)nj * 2 * 8, st));
+    const int ntb = nts + 5;  // third-state banks (8, or 9 with eta_t)
+    cplx* PT = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * ntb * B3.w * ncy * sizeof(cplx)));
+    cplx* Q = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * nf4 * B4.w * ncy * sizeof(cplx)));
+    cplx* R4 = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * nf4 * pl4 * sizeof(cplx)));
+    unsigned long long* mR4 = reinterpret_cast<unsigned long long*>(tr + b.take((size_t)nj * nf4 * 8));
+    CUDA_TRY(cudaMemsetAsync(mR4, 0, (size_t)nj * nf4 * 8, st));
     ColArgs a = colargs(COL_E44_FIRST4, 19, E44_FIRST_MULT, nullptr, B1, p->geo1, spec, pl1, 0, Ro, PF);
     if ((s = launch_col_ifft(a, nj, st, p->tw)) != GL_OK) return s;
     for (int u = 0; u < gu; ++u) {
@@ -2386,18 +2420,18 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
       a2.floor_nsrc = 5;
       if ((s = launch_col_ifft(a2, Ro, st, p->tw)) != GL_OK) return s;
     }
-    ColArgs a3 = colargs(COL_FLOORED, 8, E44_TOUT_MULT, E44_TOUT_SRC, B3, p->geo3, TS, 3LL * pl3, pl3,
-                         Ro, PT);
+    ColArgs a3 = colargs(COL_FLOORED, ntb, E44_TOUT_MULT, E44_TOUT_SRC, B3, p->geo3, TS,
+                         (long long)nts * pl3, pl3, Ro, PT);
     a3.floor_max = maxT;
-    a3.floor_nsrc = 3;
+    a3.floor_nsrc = nts;
     if ((s = launch_col_ifft(a3, nj, st, p->tw)) != GL_OK) return s;
-    RowArgs r = rowargs(ROW_E44_ORDER4, 2, B4, Q);
+    RowArgs r = rowargs(psi ? ROW_E44_ORDER4_PSI : ROW_E44_ORDER4, nf4, B4, Q);
     r.grp[0] = BankGroup{PF, 19, B1.x0, B1.w};
     r.grp[1] = BankGroup{PP, 18, B2.x0, B2.w};
-    r.grp[2] = BankGroup{PT, 8, B3.x0, B3.w};
+    r.grp[2] = BankGroup{PT, ntb, B3.x0, B3.w};
     r.ngrp = 3;
     if ((s = launch_row(r, nj, st, p->tw)) != GL_OK) return s;
-    if ((s = colfft(Q, R4, B4, 2, s4, mR4, Ro, nj * 2)) != GL_OK) return s;
+    if ((s = colfft(Q, R4, B4, nf4, s4, mR4, Ro, nj * nf4)) != GL_OK) return s;
     E44Acc c;
     std::memset(&c, 0, sizeof c);
     c.us = us;
@@ -2414,6 +2448,7 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     c.Ro = Ro;
     c.outer0 = o0;
     c.floor_rel = p->floor_rel;
+    c.nspec = nf4;
     dim3 g(grid_for(pl4, T, 64), gu);
     {
       LaunchScope ls_("acc_e44_order4_kernel", st, 0.0);
@@ -2445,7 +2480,7 @@ extern "C" gl_status gl_eta44_execute_partial(gl_plan* p, int n_units, const voi
     return fail(GL_ERR_WORKSPACE, "workspace must be 256-byte aligned and at least %zu bytes", p->ws_total);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const size_t in_unit = layout == GL_SPECTRA_FULL ? (size_t)p->d.nx * p->d.ny : (size_t)p->b1.w * p->b1.h;
-  const size_t part_unit = (size_t)p->b4.w * p->b4.h;
+  const size_t part_unit = (size_t)p->ncomp * p->b4.w * p->b4.h;
   for (int u0 = 0; u0 < n_units; u0 += p->group) {
     const int gu = std::min(p->group, n_units - u0);
     gl_status s = e44_run(p, gu, reinterpret_cast<const cplx*>(d_spectra) + (size_t)u0 * in_unit, layout,
@@ -2475,8 +2510,9 @@ extern "C" gl_status gl_eta44_finalize(gl_plan* p, int n_units, const void* d_pa
   char* e44 = at<char>(d_ws, p->o_e44);
   const E44Layout L = e44_layout(p, p->group);
   unsigned long long* maxOUT = reinterpret_cast<unsigned long long*>(e44 + L.maxOUT);
-  const size_t part_unit = (size_t)p->b4.w * p->b4.h;
-  const size_t out_unit = (size_t)p->d.nx * p->d.ny * (p->d.output == GL_OUT_REAL ? sizeof(double) : sizeof(cplx));
+  const size_t part_unit = (size_t)p->ncomp * p->b4.w * p->b4.h;
+  const size_t out_unit = (size_t)p->ncomp * p->d.nx * p->d.ny *
+                          (p->d.output == GL_OUT_REAL ? sizeof(double) : sizeof(cplx));
   for (int u0 = 0; u0 < n_units; u0 += p->group) {
     const int gu = std::min(p->group, n_units - u0);
     gl_status s = e44_finalize(p, gu, reinterpret_cast<const cplx*>(d_partial_sum) + (size_t)u0 * part_unit,

@@ -28,6 +28,8 @@ struct E44Acc {
   int jobs_per_unit;        // pair stage: Ro R^2 + Ro R
   int Ro, outer0;           // outer nodes handled by this call, first one
   double floor_rel;
+  int nspec;                // third stage: spectra written (3, or 4 with eta_t);
+                            // order 4: forcing rows read (2, or 4 with the contact rows)
 };
 
 GL_D void e44_max_reduce(double* v, int n, unsigned long long* slots) {
@@ -86,18 +88,21 @@ __global__ void acc_e44_pair_kernel(E44Acc a) {
   e44_max_reduce(lm, 5, a.maxout + (size_t)grp * 5);
 }
 
-// Third level: es, ps, pts of one outer node (gl_eta44_fftw.cpp:571-584).
+// Third level: es, ps, pts of one outer node (gl_eta44_fftw.cpp:571-584);
+// with nspec = 4 also ets, the third-order eta_t the psi44 contact needs
+// (finite_depth_directional_nested_green_laplace_eta33.m:127-131).
 __global__ void acc_e44_third_kernel(E44Acc a) {
   const int uo = blockIdx.y;  // unit * Ro + local outer node
   const int unit = uo / a.Ro;
   const int R = a.R;
   const int plane = a.box.w * a.box.h;
   const UnitScalars& u = a.us[unit];
-  double lm[3] = {0, 0, 0};
+  const int ns = a.nspec;
+  double lm[4] = {0, 0, 0, 0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
     const GeoRef G{a.geo, plane, i};
     const double A = G.a(), sqa = __ldg(a.geo + 5 * plane + i);
-    cplx es = czero(), ps = czero(), pts = czero();
+    cplx es = czero(), ps = czero(), pts = czero(), ets = czero();
     for (int t = 0; t < R; ++t) {
       const int job = uo * R + t;
       const double x = a.nodes[t], w = a.weights[t];
@@ -111,42 +116,58 @@ __global__ void acc_e44_third_kernel(E44Acc a) {
       es = cadd(es, cscale(co, csub(cscale(A * sh, s[1]), cmul(cmk(0.0, ch), s[0]))));
       ps = cadd(ps, cscale(co, csub(cmul(cmk(0.0, -ch), s[1]), cscale(sh, s[0]))));
       pts = cadd(pts, cscale(co, csub(cmul(cmk(0.0, -ch), s[3]), cscale(sh, s[2]))));
+      if (ns == 4) ets = cadd(ets, cscale(co, csub(cscale(A * sh, s[3]), cmul(cmk(0.0, ch), s[2]))));
     }
-    cplx* dst = a.out + (size_t)uo * 3 * plane;
-    const cplx r[3] = {es, ps, pts};
-    for (int k = 0; k < 3; ++k) {
+    cplx* dst = a.out + (size_t)uo * ns * plane;
+    const cplx r[4] = {es, ps, pts, ets};
+    for (int k = 0; k < ns; ++k) {
       dst[(size_t)k * plane + i] = r[k];
       lm[k] = e44_keep_max(lm[k], r[k]);
     }
   }
-  e44_max_reduce(lm, 3, a.maxout + (size_t)uo * 3);
+  e44_max_reduce(lm, ns, a.maxout + (size_t)uo * ns);
 }
 
-// Order 4: the eta44 spectrum of one unit (gl_eta44_fftw.cpp:736-748).
+// Order 4: the eta44 spectrum of one unit (gl_eta44_fftw.cpp:736-748); with
+// nspec = 4 also psi44 (...eta44_three_kernels.m:93-111): the contact rows
+// give the surface forcings fk + A c and fd - c_t and
+// psi += coef (-i cosh fd_s - sinh/sqrt(A) fk_s).  Output [unit][1 or 2][plane];
+// only eta44 gets a maximum (its final floor), psi44 is masked only.
 __global__ void acc_e44_order4_kernel(E44Acc a) {
   const int unit = blockIdx.y;
   const int plane = a.box.w * a.box.h;
   const UnitScalars& u = a.us[unit];
+  const int ns = a.nspec;
+  const int nout = ns == 4 ? 2 : 1;
   double lm[1] = {0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
     const GeoRef G{a.geo, plane, i};
     const double A = G.a(), sqa = __ldg(a.geo + 5 * plane + i);
-    cplx acc = czero();
+    cplx acc = czero(), psi = czero();
     for (int ol = 0; ol < a.Ro; ++ol) {
       const int job = unit * a.Ro + ol;
       const double x = a.nodes[a.outer0 + ol], w = a.weights[a.outer0 + ol];
       const double tm = x / u.lam4;
       const double co = w * exp(x) / u.lam4 * exp(-4.0 * u.shift4 * tm);
       const double sh = sinh_over_root(sqa, tm), ch = cosh(sqa * tm);
-      const cplx* src = a.in + (size_t)job * 2 * plane;
-      const cplx fk = floored(src[i], a.floor_rel, a.maxin[job * 2 + 0]);
-      const cplx fd = floored(src[plane + i], a.floor_rel, a.maxin[job * 2 + 1]);
+      const cplx* src = a.in + (size_t)job * ns * plane;
+      const unsigned long long* mx = a.maxin + (size_t)job * ns;
+      const cplx fk = floored(src[i], a.floor_rel, mx[0]);
+      const cplx fd = floored(src[plane + i], a.floor_rel, mx[1]);
       acc = cadd(acc, cscale(co, csub(cscale(A * sh, fd), cmul(cmk(0.0, ch), fk))));
+      if (ns == 4) {
+        const cplx c = floored(src[2 * plane + i], a.floor_rel, mx[2]);
+        const cplx ct = floored(src[3 * plane + i], a.floor_rel, mx[3]);
+        const cplx fks = cadd(fk, cscale(A, c));
+        const cplx fds = csub(fd, ct);
+        psi = cadd(psi, cscale(co, csub(cmul(cmk(0.0, -ch), fds), cscale(sh, fks))));
+      }
     }
-    a.out[(size_t)unit * plane + i] = acc;
+    a.out[(size_t)unit * nout * plane + i] = acc;
+    if (nout == 2) a.out[((size_t)unit * nout + 1) * plane + i] = psi;
     lm[0] = e44_keep_max(lm[0], acc);
   }
-  e44_max_reduce(lm, 1, a.maxout + unit);
+  e44_max_reduce(lm, 1, a.maxout + (size_t)unit * nout);
 }
 
 }  // namespace gl

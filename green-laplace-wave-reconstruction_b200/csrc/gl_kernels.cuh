@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
 // ---------------------------------------------------------------------------
 
 enum RowKind : int { ROW_ETA22 = 0, ROW_PSI22, ROW_CONTACT22, ROW_INNER, ROW_OUTER,
-                     ROW_E44_PAIR, ROW_E44_THIRD, ROW_E44_ORDER4,
+                     ROW_E44_PAIR, ROW_E44_THIRD, ROW_E44_ORDER4, ROW_E44_ORDER4_PSI,
                      // adjoint (transposed) products, row_kernel_t<1>
                      ROW_ADJ_ETA22, ROW_ADJ_INNER, ROW_ADJ_OUTER };
 
@@ -418,6 +418,48 @@ GL_D void row_products(int kind, cplx* b, int L, int p, int chan_count) {
       BK(3) = skt;
       break;
     }
+    case ROW_OUTER: {  // _order3.py:76-102, 275-287
+      // first-order banks 0..11: eta etax etay phix phiy phiz phixz phiyz phizz phizzz phitz phitzz
+      // pair banks 12..20: eta etax etay phix phiy phiz phizz phitz eta_t
+      cplx fe = BK(0), fex = BK(1), fey = BK(2), fpx = BK(3), fpy = BK(4), fpz = BK(5),
+           fpxz = BK(6), fpyz = BK(7), fpzz = BK(8), fpzzz = BK(9), fptz = BK(10), fptzz = BK(11);
+      cplx pe = BK(12), pex = BK(13), pey = BK(14), ppx = BK(15), ppy = BK(16), ppz = BK(17),
+           ppzz = BK(18), pptz = BK(19), pet = BK(20);
+      // first-state aliases: eta_t = phiz, phiz_t = phitz, phizz_t = phitzz; pair phiz_t = phitz
+      cplx fe2 = csq(fe);
+      cplx k_pair = csub(csub(cadd(cadd(cadd(cmul(fpx, pex), cmul(fpy, pey)), cmul(ppx, fex)), cmul(ppy, fey)),
+                              cmul(fe, ppzz)),
+                         cmul(pe, fpzz));
+      cplx k_direct = csub(cmul(fe, cadd(cmul(fpxz, fex), cmul(fpyz, fey))), cmul(cscale(0.5, fe2), fpzzz));
+      cplx d_pair = cadd(cadd(cadd(cadd(cmul(fe, pptz), cmul(pe, fptz)), cmul(fpx, ppx)), cmul(fpy, ppy)),
+                         cmul(fpz, ppz));
+      cplx d_direct = cadd(cmul(cscale(0.5, fe2), fptzz),
+                           cmul(fe, cadd(cadd(cmul(fpx, fpxz), cmul(fpy, fpyz)), cmul(fpz, fpzz))));
+      cplx fk = cadd(cscale(0.25, k_direct), cscale(0.5, k_pair));
+      cplx fd = cadd(cscale(0.25, d_direct), cscale(0.5, d_pair));
+      cplx contact = cadd(cadd(cmul(cscale(0.5, fe), ppz), cmul(cscale(0.5, pe), fpz)),
+                          cmul(cscale(0.125, fe2), fpzz));
+      cplx contact_t =
+          cadd(cadd(cadd(cscale(0.5, cadd(cmul(fpz, ppz), cmul(fe, pptz))),
+                         cscale(0.5, cadd(cmul(pet, fpz), cmul(pe, fptz)))),
+                    cmul(cmul(cscale(0.25, fe), fpz), fpzz)),
+               cmul(cscale(0.125, fe2), fptzz));
+      BK(0) = fk;
+      BK(1) = fd;
+      BK(2) = contact;
+      BK(3) = contact_t;
+      break;
+    }
+  }
+#undef BK
+}
+
+// Pointwise products of the order-4 stages (gl_eta44_fftw.cpp), compiled into
+// their own row kernel so that the wide order-4 rows do not weigh on the
+// register allocation of the order-2/3 stages.
+GL_D void row_products_e44(int kind, cplx* b, int L, int p) {
+#define BK(k) b[(k) * L + p]
+  switch (kind) {
     case ROW_E44_PAIR: {  // gl_eta44_fftw.cpp:375-381: six pair sources from 16 banks
       const cplx v = BK(0), vn = BK(1), vn2 = BK(2), vn3 = BK(3), vn4 = BK(4), hx = BK(5),
                  hy = BK(6), jx = BK(7), jy = BK(8), ro = BK(9), qq = BK(10), q2n = BK(11),
@@ -501,7 +543,8 @@ GL_D void row_products(int kind, cplx* b, int L, int p, int chan_count) {
       BK(3) = cadd(cscale(0.25, ddt), cscale(0.5, dpt));
       break;
     }
-    case ROW_E44_ORDER4: {  // gl_eta44_fftw.cpp:712-735: partitions 31, 22, 211, 1111
+    case ROW_E44_ORDER4:
+    case ROW_E44_ORDER4_PSI: {  // gl_eta44_fftw.cpp:712-735: partitions 31, 22, 211, 1111
       // first4 banks 0..18: eta ex ey px py pz pxz pyz pzz pzzz ptz ptzz pxz_t pyz_t pzzz_t ptz_t pxzz pyzz pzzzz
       // pair4 banks 19..36: eta ex ey eta_t ex_t ey_t px py pz pzz ptz px_t py_t pzz_t ptz_t pxz pyz pzzz
       // third banks 37..44: eta ex ey px py pz pzz pzt
@@ -544,50 +587,36 @@ GL_D void row_products(int kind, cplx* b, int L, int p, int chan_count) {
                               cmul(hfe2, cadd(cadd(cmul(fpxz, fpxz), cmul(fpyz, fpyz)), cmul(fpzz, fpzz))));
       const cplx kb = cadd(cadd(cscale(0.125, k1111), cscale(0.25, k211)), cscale(0.5, k22));
       const cplx db = cadd(cadd(cscale(0.125, d1111), cscale(0.25, d211)), cscale(0.5, d22));
+      if (kind == ROW_E44_ORDER4_PSI) {
+        // psi44 surface contact and its time derivative
+        // (...eta44_three_kernels.m:221-241); bank 45 = third-order eta_t,
+        // first-order eta_t = phiz, phiz_t = phitz, phizz_t = phitzz
+        const cplx pet = BK(22), tet = BK(45);
+        const cplx fefe = cmul(fe, fe);
+        const cplx fepe = cmul(fe, pe);
+        const cplx c = cadd(cadd(cadd(cscale(0.5, cmul(fe, tpz)), cscale(0.5, cmul(pe, ppz))),
+                                 cadd(cscale(0.5, cmul(te, fpz)), cscale(0.125, cmul(fefe, ppzz)))),
+                            cadd(cscale(0.25, cmul(fepe, fpzz)),
+                                 cscale(1.0 / 48.0, cmul(cmul(fefe, fe), fpzzz))));
+        cplx ct = cscale(0.5, cadd(cmul(fpz, tpz), cmul(fe, tpzt)));
+        ct = cadd(ct, cscale(0.5, cadd(cmul(pet, ppz), cmul(pe, pptz))));
+        ct = cadd(ct, cscale(0.5, cadd(cmul(tet, fpz), cmul(te, fptz))));
+        ct = cadd(ct, cscale(0.125, cadd(cscale(2.0, cmul(cmul(fe, fpz), ppzz)), cmul(fefe, ppzzt))));
+        ct = cadd(ct, cscale(0.25, cadd(cadd(cmul(cmul(fpz, pe), fpzz), cmul(cmul(fe, pet), fpzz)),
+                                        cmul(fepe, fptzz))));
+        ct = cadd(ct, cscale(1.0 / 48.0, cadd(cscale(3.0, cmul(cmul(fefe, fpz), fpzzz)),
+                                              cmul(cmul(fefe, fe), fpzzzt))));
+        BK(2) = c;
+        BK(3) = ct;
+      }
       BK(0) = cadd(cscale(0.5, k31), kb);
       BK(1) = cadd(cscale(0.5, d31), db);
-      break;
-    }
-    case ROW_OUTER: {  // _order3.py:76-102, 275-287
-      // first-order banks 0..11: eta etax etay phix phiy phiz phixz phiyz phizz phizzz phitz phitzz
-      // pair banks 12..20: eta etax etay phix phiy phiz phizz phitz eta_t
-      cplx fe = BK(0), fex = BK(1), fey = BK(2), fpx = BK(3), fpy = BK(4), fpz = BK(5),
-           fpxz = BK(6), fpyz = BK(7), fpzz = BK(8), fpzzz = BK(9), fptz = BK(10), fptzz = BK(11);
-      cplx pe = BK(12), pex = BK(13), pey = BK(14), ppx = BK(15), ppy = BK(16), ppz = BK(17),
-           ppzz = BK(18), pptz = BK(19), pet = BK(20);
-      // first-state aliases: eta_t = phiz, phiz_t = phitz, phizz_t = phitzz; pair phiz_t = phitz
-      cplx fe2 = csq(fe);
-      cplx k_pair = csub(csub(cadd(cadd(cadd(cmul(fpx, pex), cmul(fpy, pey)), cmul(ppx, fex)), cmul(ppy, fey)),
-                              cmul(fe, ppzz)),
-                         cmul(pe, fpzz));
-      cplx k_direct = csub(cmul(fe, cadd(cmul(fpxz, fex), cmul(fpyz, fey))), cmul(cscale(0.5, fe2), fpzzz));
-      cplx d_pair = cadd(cadd(cadd(cadd(cmul(fe, pptz), cmul(pe, fptz)), cmul(fpx, ppx)), cmul(fpy, ppy)),
-                         cmul(fpz, ppz));
-      cplx d_direct = cadd(cmul(cscale(0.5, fe2), fptzz),
-                           cmul(fe, cadd(cadd(cmul(fpx, fpxz), cmul(fpy, fpyz)), cmul(fpz, fpzz))));
-      cplx fk = cadd(cscale(0.25, k_direct), cscale(0.5, k_pair));
-      cplx fd = cadd(cscale(0.25, d_direct), cscale(0.5, d_pair));
-      cplx contact = cadd(cadd(cmul(cscale(0.5, fe), ppz), cmul(cscale(0.5, pe), fpz)),
-                          cmul(cscale(0.125, fe2), fpzz));
-      cplx contact_t =
-          cadd(cadd(cadd(cscale(0.5, cadd(cmul(fpz, ppz), cmul(fe, pptz))),
-                         cscale(0.5, cadd(cmul(pet, fpz), cmul(pe, fptz)))),
-                    cmul(cmul(cscale(0.25, fe), fpz), fpzz)),
-               cmul(cscale(0.125, fe2), fptzz));
-      BK(0) = fk;
-      BK(1) = fd;
-      BK(2) = contact;
-      BK(3) = contact_t;
       break;
     }
   }
 #undef BK
 }
 
-// One block per (row y, job): inverse transforms along x of every bank
-// (inputs read straight from the column-transformed rows, zero outside the
-// bank's box columns), the stage's products, forward transforms of the
-// outputs, and only the output box's columns are written: [job][out][y][col].
 // Transposed products of the adjoint stages.  Every forward product is a
 // polynomial P(f_1..f_m) of the bank fields; given the adjoint field w of
 // each product (the transposed forward FFT of its adjoint spectrum) the
@@ -672,6 +701,13 @@ GL_D void row_products_adj(int kind, cplx* b, int L, int p) {
 #undef BK
 }
 
+// One block per (row y, job): inverse transforms along x of every bank (the
+// first pass reads the column-transformed rows straight from global memory,
+// zero outside the bank's box columns, 16 loads in flight per thread), the
+// stage's products, forward transforms of the outputs, and only the output
+// box's columns are written: [job][out][y][col].
+// FAMILY 0: order-2/3 stages, 1: adjoint stages, 2: order-4 stages (their
+// rows are wider than 24 banks and are staged in shared memory first).
 template <int FAMILY>
 __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __restrict__ tw) {
   extern __shared__ cplx smem[];
@@ -682,11 +718,13 @@ __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __
   int nb = 0;
   for (int q = 0; q < a.ngrp; ++q) nb += a.grp[q].nb;
   cplx* banks = smem;  // nb * L
-  // stage 0: zero the rows and gather every bank's box columns with
-  // coalesced loads (all loads in flight at once)
-  for (int t = threadIdx.x; t < nb * L; t += blockDim.x) banks[t] = czero();
-  __syncthreads();
-  {
+  constexpr bool PREFETCH = FAMILY == 2;
+  if constexpr (PREFETCH) {
+    // wide rows (the order-4 stages, > 24 banks): gather every bank's box
+    // columns first with coalesced loads, all in flight at once, since the
+    // transform loop takes several rounds of groups
+    for (int t = threadIdx.x; t < nb * L; t += blockDim.x) banks[t] = czero();
+    __syncthreads();
     int k0 = 0;
     for (int q = 0; q < a.ngrp; ++q) {
       const BankGroup B = a.grp[q];
@@ -694,13 +732,12 @@ __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __
       const cplx* src = B.data + ((size_t)job * B.nb * a.ny + y) * B.w;
       for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
         const int kk = t / B.w, xi = t % B.w;
-        banks[(size_t)(k0 + kk) * L + phys(wrap(B.x0 + xi, n))] =
-            src[(size_t)kk * a.ny * B.w + xi];
+        banks[(size_t)(k0 + kk) * L + phys(wrap(B.x0 + xi, n))] = src[(size_t)kk * a.ny * B.w + xi];
       }
       k0 += B.nb;
     }
+    __syncthreads();
   }
-  __syncthreads();
   int g, G;
   const FftGroup f = fft_group(n, a.log2nx, g, G);
   for (int it = 0; it < (nb + G - 1) / G; ++it) {
@@ -708,15 +745,30 @@ __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __
     const bool active = k < nb;
     cplx* buf = banks + (size_t)(active ? k : 0) * L;
     bool cj = false;
-    if constexpr (FAMILY == 1) {
+    const cplx* srow = nullptr;
+    int bx0 = 0, bw = 0;
+    {
+      const int kk0 = active ? k : 0;
       int k0 = 0;
       for (int q = 0; q < a.ngrp; ++q) {
-        if (k >= k0 && k < k0 + a.grp[q].nb) cj = a.grp[q].conj != 0;
+        if (kk0 >= k0 && kk0 < k0 + a.grp[q].nb) {
+          const BankGroup& B = a.grp[q];
+          cj = FAMILY == 1 && B.conj != 0;
+          srow = B.data + (((size_t)job * B.nb + (kk0 - k0)) * a.ny + y) * B.w;
+          bx0 = B.x0;
+          bw = B.w;
+        }
         k0 += a.grp[q].nb;
       }
     }
     auto load = [&](int xb) -> cplx {
-      const cplx v = buf[phys(xb)];
+      cplx v;
+      if constexpr (PREFETCH) {
+        v = buf[phys(xb)];
+      } else {
+        const int xi = wrap(xb - bx0, n);
+        v = xi < bw ? srow[xi] : czero();
+      }
       return cj ? cconj(v) : v;
     };
     auto store = [&](int xb, cplx v) { buf[phys(xb)] = cj ? cconj(v) : v; };
@@ -726,6 +778,8 @@ __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __
   if constexpr (FAMILY == 0) {
     const int chan_count = a.kind == ROW_PSI22 ? a.us[job / a.jobs_per_unit].chan_count : 0;
     for (int p = threadIdx.x; p < n; p += blockDim.x) row_products(a.kind, banks, L, phys(p), chan_count);
+  } else if constexpr (FAMILY == 2) {
+    for (int p = threadIdx.x; p < n; p += blockDim.x) row_products_e44(a.kind, banks, L, phys(p));
   } else {
     for (int p = threadIdx.x; p < n; p += blockDim.x) row_products_adj(a.kind, banks, L, phys(p));
   }

@@ -26,9 +26,10 @@ STATUS_NAMES = {
 }
 
 COMP_ETA11, COMP_PSI11, COMP_ETA22, COMP_PSI22, COMP_ETA33, COMP_PSI33 = 1, 2, 4, 8, 16, 32
-COMP_ETA44 = 64
+COMP_ETA44, COMP_PSI44 = 64, 128
 COMP_NAMES = {COMP_ETA11: "eta11", COMP_PSI11: "psi11", COMP_ETA22: "eta22",
-              COMP_PSI22: "psi22", COMP_ETA33: "eta33", COMP_PSI33: "psi33", COMP_ETA44: "eta44"}
+              COMP_PSI22: "psi22", COMP_ETA33: "eta33", COMP_PSI33: "psi33", COMP_ETA44: "eta44",
+              COMP_PSI44: "psi44"}
 GRID_COMPACT, GRID_REFERENCE = 0, 1
 OUT_COMPLEX, OUT_REAL = 0, 1
 SPECTRA_FULL, SPECTRA_BOX = 0, 1
@@ -52,7 +53,8 @@ class Eta44Desc(C.Structure):
                 ("peak_depth", C.c_double), ("rank", C.c_int),
                 ("nodes", C.POINTER(C.c_double)), ("weights", C.POINTER(C.c_double)),
                 ("box_x0", C.c_int), ("box_y0", C.c_int), ("box_w", C.c_int), ("box_h", C.c_int),
-                ("max_units", C.c_int), ("output", C.c_int)]
+                ("max_units", C.c_int), ("output", C.c_int), ("components", C.c_int),
+                ("gravity", C.c_double)]
 
 
 class PlanInfo(C.Structure):

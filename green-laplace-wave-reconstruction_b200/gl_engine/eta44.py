@@ -128,9 +128,13 @@ class Eta44Plan(Plan):
 
 
 def eta44(spectra, *, dk: float, depth: float, peak_depth: float, rank: int, nodes=None,
-          weights=None, device=None, output: str = "complex") -> np.ndarray:
+          weights=None, device=None, output: str = "complex", psi44: bool = False,
+          gravity: float = 1.0):
     """Physical analytic eta44 fields (depth x the GLE44O01 field) of one or
-    more N^2-scaled analytic spectra ``[..., iy, ix]`` sharing one grid."""
+    more N^2-scaled analytic spectra ``[..., iy, ix]`` sharing one grid.
+
+    With ``psi44=True`` returns ``(eta44, psi44)``; psi44 is the surface
+    potential of ``src/gl_pure_sum_order4.m`` scaled by depth sqrt(g depth)."""
     spectra = np.asarray(spectra, dtype=np.complex128)
     single = spectra.ndim == 2
     if single:
@@ -145,22 +149,51 @@ def eta44(spectra, *, dk: float, depth: float, peak_depth: float, rank: int, nod
         nd = keep[0].ctypes.data_as(C.POINTER(C.c_double))
         wd = keep[1].ctypes.data_as(C.POINTER(C.c_double))
     out_mode = _lib.OUT_REAL if output == "real" else _lib.OUT_COMPLEX
+    comps = _lib.COMP_ETA44 | (_lib.COMP_PSI44 if psi44 else 0)
     desc = _lib.Eta44Desc(n=n, dk=dk, depth=depth, peak_depth=peak_depth, rank=rank, nodes=nd,
                           weights=wd, box_x0=box[0], box_y0=box[1], box_w=box[2], box_h=box[3],
-                          max_units=1, output=out_mode)
+                          max_units=1, output=out_mode, components=comps, gravity=gravity)
     plan = Eta44Plan(desc, dev, keep)
+    ncomp = 2 if psi44 else 1
     with torch.cuda.device(dev):
         spec = torch.from_numpy(np.ascontiguousarray(spectra)).to(dev)
         dtype = torch.float64 if out_mode == _lib.OUT_REAL else torch.complex128
-        out = torch.empty((units, 1, n, n), dtype=dtype, device=dev)
+        out = torch.empty((units, ncomp, n, n), dtype=dtype, device=dev)
         status = torch.zeros(units, dtype=torch.int32, device=dev)
         plan.execute(units, torch.view_as_real(spec), _lib.SPECTRA_FULL, out, status,
                      torch.cuda.current_stream(dev).cuda_stream)
         st = status.cpu().numpy()
         if np.any(st != 0):
             raise _status_error(int(st[st != 0][0]))
-        res = out[:, 0].cpu().numpy()
-    return res[0] if single else res
+        res = out.cpu().numpy()
+    if single:
+        res = res[0]
+        return (res[0], res[1]) if psi44 else res[0]
+    return (res[:, 0], res[:, 1]) if psi44 else res[:, 0]
+
+
+def gl_pure_sum_order4(s, qx, qy, qp: float, rank: int = 4, *, device=None):
+    """``[eta44, psi44, audit] = gl_pure_sum_order4(s, qx, qy, qp, rank)``
+    (``src/gl_pure_sum_order4.m:1-15``): dimensionless analytic eta44/h and
+    psi44/(h sqrt(gh)) of ``s = fft2(eta11_plus/h)`` on the grid ``qx = kx h``,
+    ``qy = ky h`` (square, power-of-two, equal spacing in x and y), peak
+    ``qp = kp h``, one GL rank for all three nested levels."""
+    s = np.asarray(s, dtype=np.complex128)
+    qx = np.asarray(qx, dtype=float)
+    qy = np.asarray(qy, dtype=float)
+    if rank not in (4, 6, 8, 10, 12):
+        raise ValueError("Unsupported no-Stokes order-four Green--Laplace rank.")
+    if not (s.shape == qx.shape == qy.shape) or s.ndim != 2 or s.shape[0] != s.shape[1]:
+        raise ValueError("Spectrum, qx, and qy must have identical square sizes.")
+    dq = float(qx[0, 1] - qx[0, 0])
+    if not (dq > 0) or abs(float(qy[1, 0] - qy[0, 0]) - dq) > 1e-12 * dq:
+        raise ValueError("qx and qy must be the fft2 wavenumber grids of one square lattice")
+    eta, psi = eta44(s, dk=dq, depth=1.0, peak_depth=float(qp), rank=rank, device=device,
+                     psi44=True, gravity=1.0)
+    audit = {"implementation": "no-stokes-green-laplace-order4", "quadrature_rank": rank,
+             "nested_rank_tuple": (rank, rank, rank), "order4_stokes_correction_used": False,
+             "release_status": "experimental no-Stokes migration; not a total-field API extension"}
+    return eta, psi, audit
 
 
 def main(argv=None) -> int:

@@ -66,6 +66,7 @@ typedef enum gl_status {
 #define GL_COMP_ETA33 0x10
 #define GL_COMP_PSI33 0x20
 #define GL_COMP_ETA44 0x40  /* fourth-order plans (gl_eta44_plan_create) */
+#define GL_COMP_PSI44 0x80  /* fourth-order surface potential (same plans)  */
 
 #define GL_GRID_COMPACT 0   /* smallest alias-free power-of-two product grid */
 #define GL_GRID_REFERENCE 1 /* products on the reference's own Nx x Ny grid   */
@@ -116,7 +117,11 @@ gl_status gl_plan_get_info(const gl_plan* plan, gl_plan_info* info);
  * Conventions follow the C++: qx = (depth dk) mx, the peak depth is supplied,
  * the square grid is n x n.  The plan runs through gl_execute: inputs are the
  * N^2-scaled analytic spectra (full [ny][nx] or box), the output is the
- * analytic eta44 field times depth (one plane per unit). */
+ * analytic eta44 field times depth, [unit][component][ny][nx].
+ * With components = GL_COMP_ETA44 | GL_COMP_PSI44 the plan also evaluates the
+ * surface potential psi44 of src/gl_pure_sum_order4.m:1-15 (contact terms of
+ * ...eta44_three_kernels.m:93-111, 221-241; the C++ has no psi44), as a second
+ * plane scaled by depth * sqrt(gravity * depth). */
 typedef struct gl_eta44_desc {
   int n;                      /* square grid (power of two)                   */
   double dk, depth, peak_depth;
@@ -126,6 +131,8 @@ typedef struct gl_eta44_desc {
   int box_x0, box_y0, box_w, box_h;
   int max_units;
   int output;                 /* GL_OUT_*                                      */
+  int components;             /* 0 or GL_COMP_ETA44 [| GL_COMP_PSI44]          */
+  double gravity;             /* psi44 scale (> 0 when psi44 is requested)     */
 } gl_eta44_desc;
 
 gl_status gl_eta44_plan_create(gl_plan** plan, const gl_eta44_desc* desc);
@@ -133,8 +140,8 @@ gl_status gl_eta44_plan_create(gl_plan** plan, const gl_eta44_desc* desc);
 /* Outer-node sharding of an eta44 plan (the device analogue of the reference's
  * process split, paper/order4/run_gl_split.sh:31-38 + merge_eta44_outer.cpp:12).
  * gl_eta44_execute_partial accumulates the order-4 spectra of outer nodes
- * [outer_begin, outer_end) into d_partial ([unit][box4_h][box4_w] complex128,
- * box4 = 4 x the parent box), before the final roundoff floor; summing the
+ * [outer_begin, outer_end) into d_partial ([unit][component][box4_h][box4_w]
+ * complex128, box4 = 4 x the parent box), before the final roundoff floor; summing the
  * partials of a partition of [0, rank) (one NCCL all-reduce across GPUs) and
  * calling gl_eta44_finalize gives the monolithic result. */
 gl_status gl_eta44_execute_partial(gl_plan* plan, int n_units, const void* d_spectra,

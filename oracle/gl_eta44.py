@@ -189,11 +189,16 @@ def third_forcing(f, p):
     return kd / 4 + kp / 2, dd / 4 + dp / 2, kdt / 4 + kpt / 2, ddt / 4 + dpt / 2
 
 
-def third(g: Grid, s, only=None):
-    """Nested order-3 state (``gl_eta44_fftw.cpp:537-637``)."""
+def third(g: Grid, s, only=None, eta_t=False):
+    """Nested order-3 state (``gl_eta44_fftw.cpp:537-637``).  With ``eta_t``
+    also the third-order eta_t field of the MATLAB graph
+    (``finite_depth_directional_nested_green_laplace_eta33.m:127-131, 165-166``),
+    accumulated from the time-derivative forcings and floored like its
+    siblings."""
     es = np.zeros_like(s)
     ps = np.zeros_like(s)
     pts = np.zeros_like(s)
+    ets = np.zeros_like(s)
     for oi, (x, w) in enumerate(zip(g.nodes, g.weights)):
         if only is not None and oi != only:
             continue
@@ -207,13 +212,18 @@ def third(g: Grid, s, only=None):
         es = es + co * (g.A * sh * fd - 1j * ch * fk)
         ps = ps + co * (-1j * ch * fd - sh * fk)
         pts = pts + co * (-1j * ch * fdt - sh * fkt)
+        if eta_t:
+            ets = ets + co * (g.A * sh * fdt - 1j * ch * fkt)
     es, ps, pts = (zero_suppress(a, g.m3) for a in (es, ps, pts))
     q2 = g.q * g.q
-    return {
+    out = {
         "eta": _ifft(es), "ex": _ifft(es * (1j * g.qx)), "ey": _ifft(es * (1j * g.qy)),
         "px": _ifft(ps * (1j * g.qx)), "py": _ifft(ps * (1j * g.qy)), "pz": _ifft(ps * g.A),
         "pzz": _ifft(ps * q2), "pzt": _ifft(pts * g.A),
     }
+    if eta_t:
+        out["eta_t"] = _ifft(zero_suppress(ets, g.m3))
+    return out
 
 
 def order4_forcing(f, p, t):
@@ -242,6 +252,53 @@ def order4_forcing(f, p, t):
     ksum = k31 / 2 + (k1111 / 8 + k211 / 4 + k22 / 2)
     dsum = d31 / 2 + (d1111 / 8 + d211 / 4 + d22 / 2)
     return ksum, dsum
+
+
+def order4_contact(f, p, t):
+    """Surface Taylor contact of psi44 and its time derivative
+    (``src/internal/finite_depth_directional_green_laplace_eta44_three_kernels.m:221-241``).
+    First-order aliases: eta_t = phiz (pz), phiz_t = phitz (ptz),
+    phizz_t = phitzz (ptzz); pair phiz_t = phitz (ptz)."""
+    fe, fet = f["eta"], f["pz"]
+    contact = (0.5 * fe * t["pz"] + 0.5 * p["eta"] * p["pz"] + 0.5 * t["eta"] * f["pz"]
+               + 0.125 * fe * fe * p["pzz"] + 0.25 * fe * p["eta"] * f["pzz"]
+               + (1.0 / 48.0) * fe * fe * fe * f["pzzz"])
+    contact_t = (0.5 * (fet * t["pz"] + fe * t["pzt"])
+                 + 0.5 * (p["eta_t"] * p["pz"] + p["eta"] * p["ptz"])
+                 + 0.5 * (t["eta_t"] * f["pz"] + t["eta"] * f["ptz"])
+                 + 0.125 * (2 * fe * fet * p["pzz"] + fe * fe * p["pzz_t"])
+                 + 0.25 * (fet * p["eta"] * f["pzz"] + fe * p["eta_t"] * f["pzz"]
+                           + fe * p["eta"] * f["ptzz"])
+                 + (1.0 / 48.0) * (3 * fe * fe * fet * f["pzzz"] + fe * fe * fe * f["pzzz_t"]))
+    return contact, contact_t
+
+
+def eta44_psi44(spectrum, dk, depth, peak, nodes, weights):
+    """Dimensionless analytic eta44 and surface psi44 fields
+    (``src/gl_pure_sum_order4.m:1-15`` ->
+    ``finite_depth_directional_green_laplace_eta44_three_kernels.m:52-178``):
+    per outer node the eta44 forcing of ``eta44`` plus the contact spectra
+    (masked, floored), the surface forcings fk + A c, fd - c_t and
+    psi += coef (-i cosh fd_s - sinh/sqrt(A) fk_s); psi44 is masked to the
+    quartic support (no final floor, as in the MATLAB graph)."""
+    g = Grid(spectrum, dk, depth, peak, nodes, weights)
+    out = np.zeros_like(spectrum)
+    psi = np.zeros_like(spectrum)
+    for x, w in zip(g.nodes, g.weights):
+        tm = x / g.l4
+        damp = spectrum * np.exp(-tm * (g.nu - g.shift4))
+        t = third(g, damp, eta_t=True)
+        f = first(g, damp, True)
+        p = pair(g, damp, True)
+        fk, fd = (zero_suppress(_fft(a), g.m4) for a in order4_forcing(f, p, t))
+        c, ct = (zero_suppress(_fft(a), g.m4) for a in order4_contact(f, p, t))
+        co = w * np.exp(x) / g.l4 * np.exp(-4 * g.shift4 * tm)
+        sh, ch = g.sh_ch(tm)
+        out = out + co * (g.A * sh * fd - 1j * ch * fk)
+        psi = psi + co * (-1j * ch * (fd - ct) - sh * (fk + g.A * c))
+    out = zero_suppress(out, g.m4)
+    psi = np.where(g.m4, psi, 0.0)
+    return _ifft(out), _ifft(psi)
 
 
 def eta44(spectrum, dk, depth, peak, nodes, weights, outer_subset=None):

@@ -49,8 +49,13 @@ def test_wit_cli_matches_library_call(tmp_path):
     assert "DIRECTIONAL_CPP_DONE sector=44" in r.stderr
     got = wit.read_dir4out(tmp_path / "out.bin")
     want = wit.wit_sector(inp, 44)
+    # the direct sum accumulates with FP64 atomics: two runs agree to roundoff
     for f in wit.FIELDS:
-        assert np.array_equal(got.fields[f], want.fields[f]), f
+        w = want.fields[f]
+        if np.linalg.norm(w) == 0:
+            assert np.linalg.norm(got.fields[f]) == 0, f
+        else:
+            assert np.linalg.norm(got.fields[f] - w) / np.linalg.norm(w) < 1e-12, f
     assert got.stats["kept"] == want.stats["kept"]
 
 

@@ -74,3 +74,52 @@ def test_eta44_reproduces_paper_gl_vs_wit_metric(rank):
     pct = 100 * rel(gl, ref)
     print(f"GL{rank} vs WIT raw rel L2 {pct:.13f} % (paper {PAPER_L2_PCT[rank]})")
     assert abs(pct / PAPER_L2_PCT[rank] - 1) < 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed,rank", [(0, 2), (1, 3), (2, 4)])
+def test_psi44_matches_cpu_restatement(seed, rank):
+    """psi44 (src/gl_pure_sum_order4.m; the C++ has none) against the CPU
+    restatement of the MATLAB graph; eta44 is unchanged by asking for psi44."""
+    s = _small(seed)
+    nodes, weights = O.gauss_laguerre(rank)
+    e_ref, p_ref = OE.eta44_psi44(s, 0.25, 1.0, 1.0, nodes, weights)
+    e, p = E44.eta44(s, dk=0.25, depth=1.0, peak_depth=1.0, rank=rank, psi44=True, gravity=1.0)
+    e_only = E44.eta44(s, dk=0.25, depth=1.0, peak_depth=1.0, rank=rank)
+    print(f"seed {seed} GL{rank}: eta44 {rel(e, e_ref):.3e}, psi44 {rel(p, p_ref):.3e}")
+    assert np.array_equal(e, e_only)
+    assert rel(e, e_ref) < 1e-9 and rel(p, p_ref) < 1e-9
+
+
+@pytest.mark.gpu
+def test_gl_pure_sum_order4_dimensionless_api():
+    s = _small(3)
+    n = s.shape[0]
+    line = 0.25 * np.rint(np.fft.fftfreq(n) * n)
+    qx, qy = np.meshgrid(line, line)
+    eta, psi, audit = E44.gl_pure_sum_order4(s, qx, qy, 1.0, 4)
+    nodes, weights = O.gauss_laguerre(4)
+    e_ref, p_ref = OE.eta44_psi44(s, 0.25, 1.0, 1.0, nodes, weights)
+    assert rel(eta, e_ref) < 1e-9 and rel(psi, p_ref) < 1e-9
+    assert audit["quadrature_rank"] == 4 and not audit["order4_stokes_correction_used"]
+    with pytest.raises(ValueError):
+        E44.gl_pure_sum_order4(s, qx, qy, 1.0, 5)
+
+
+@pytest.mark.gpu
+def test_psi44_approaches_wit_with_rank():
+    """No psi44 numbers are published; as a physics check the GL surface
+    potential approaches the WIT direct sum's surface potential on the paper
+    field as the rank grows, as eta44 does (9.2 / 4.2 / 2.0 %)."""
+    inp = wit.read_dir4in(GOLD / "wit_field_n0382_input.bin")
+    n = inp.nx
+    w = wit.wit_eta44(inp)
+    ref = np.real(np.fft.ifft2(w.fields["psi"][0] * n * n))
+    s = E44.spectrum_from_modes(inp.modes, inp.amplitudes[0], n, inp.depth)
+    errs = []
+    for rank in (6, 8, 10):
+        _, p = E44.eta44(s, dk=inp.dkx, depth=inp.depth, peak_depth=1.0, rank=rank, psi44=True,
+                         gravity=inp.gravity)
+        errs.append(100 * rel(np.real(p), ref))
+        print(f"GL{rank} psi44 vs WIT psi: raw rel L2 {errs[-1]:.4f} %")
+    assert errs[0] > errs[1] > errs[2]
