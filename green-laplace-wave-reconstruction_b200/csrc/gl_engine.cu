@@ -17,6 +17,7 @@
 #include "gl_wit.cuh"
 #include "gl_eta44.cuh"
 #include "gl_adjoint.cuh"
+#include "gl_modal.cuh"
 
 using namespace gl;
 
@@ -3390,6 +3391,427 @@ extern "C" gl_status gl_fft2(int batch, int nx, int ny, const void* d_in, void* 
     fft2_cols_kernel<-1><<<gc, 256, smc, st>>>(out, nx, ny, ilog2(ny), cw, tw);
     LAUNCH_CHECK("fft2_cols_kernel");
   }
+  return GL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// single-direction time path (modal GL resolvent and eta20)
+// ---------------------------------------------------------------------------
+
+static gl_status launch_sfft(const SFft& a, int outer, int sign, cudaStream_t st, const cplx* tw) {
+  const int T = a.n / 16;
+  const int cw = std::max(1, 256 / T);
+  const size_t smem = (size_t)cw * padded_len(a.n) * sizeof(cplx);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(strided_fft_kernel<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    cudaFuncSetAttribute(strided_fft_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    attr = true;
+  }
+  dim3 grid((unsigned)((a.ncount + cw - 1) / cw), (unsigned)outer);
+  LaunchScope ls("strided_fft_kernel", st, 2.0 * a.n * (double)a.ncount * outer * sizeof(cplx));
+  if (sign > 0)
+    strided_fft_kernel<+1><<<grid, 256, smem, st>>>(a, tw, cw);
+  else
+    strided_fft_kernel<-1><<<grid, 256, smem, st>>>(a, tw, cw);
+  LAUNCH_CHECK("strided_fft_kernel");
+  return GL_OK;
+}
+
+static SFft sfft(cplx* d, int n, long long stride, long long cstride, int ncount, long long ostride,
+                 double scale) {
+  SFft a;
+  std::memset(&a, 0, sizeof a);
+  a.data = d;
+  a.n = n;
+  a.log2n = ilog2(n);
+  a.stride = stride;
+  a.cstride = cstride;
+  a.ncount = ncount;
+  a.ostride = ostride;
+  a.scale = scale;
+  return a;
+}
+
+// Transform along axis 0 of a [P][M] array (length P, power of two).  sign > 0:
+// natural input, output rows permuted when P > 4096; sign < 0: the inverse
+// ordering (permuted input, natural output).  Four-step split P = P1 P2.
+static gl_status axis0_transform(cplx* d, int P, int M, int sign, double scale, cudaStream_t st,
+                                 const cplx* tw) {
+  if (P <= TW_N) return launch_sfft(sfft(d, P, M, 1, M, 0, scale), 1, sign, st, tw);
+  const int p = ilog2(P);
+  const int P1 = 1 << (p - p / 2), P2 = 1 << (p / 2);
+  gl_status s;
+  if (sign > 0) {
+    SFft a = sfft(d, P2, (long long)P1 * M, 1, P1 * M, 0, 1.0);
+    a.tw_mode = 1;
+    a.tw_div = M;
+    a.tw_log2p = p;
+    if ((s = launch_sfft(a, 1, +1, st, tw)) != GL_OK) return s;
+    return launch_sfft(sfft(d, P1, M, 1, M, (long long)P1 * M, scale), P2, +1, st, tw);
+  }
+  SFft a = sfft(d, P1, M, 1, M, (long long)P1 * M, 1.0);
+  a.tw_mode = 2;
+  a.tw_log2p = p;
+  if ((s = launch_sfft(a, P2, -1, st, tw)) != GL_OK) return s;
+  return launch_sfft(sfft(d, P2, (long long)P1 * M, 1, P1 * M, 0, scale), 1, -1, st, tw);
+}
+
+// Transform along the contiguous last axis of [rows][M].
+static gl_status axis_last_transform(cplx* d, long long rows, int M, int sign, double scale,
+                                     cudaStream_t st, const cplx* tw) {
+  return launch_sfft(sfft(d, M, 1, M, (int)rows, 0, scale), 1, sign, st, tw);
+}
+
+static int modal_pad(int w) { return std::max(16, next_pow2(w)); }
+
+static size_t modal_buffers(int order) { return order >= 3 ? 22 : 7; }
+
+static gl_status modal_check(const gl_modal_desc* d) {
+  if (!d) return fail(GL_ERR_INVALID_ARGUMENT, "null modal descriptor");
+  if (d->order != 2 && d->order != 3) return fail(GL_ERR_INVALID_ARGUMENT, "modal order must be 2 or 3");
+  if (!is_pow2(d->points) || d->points < 16 || d->points > (1 << 24))
+    return fail(GL_ERR_UNSUPPORTED, "modal_points must be a power of two from 16 to 2^24 (got %d)", d->points);
+  if (d->width < 1 || modal_pad(d->width) > TW_N)
+    return fail(GL_ERR_UNSUPPORTED, "the work band (%d bins) exceeds %d", d->width, TW_N);
+  if (d->base_bin < 1 || d->count < 1 || d->width > d->count)
+    return fail(GL_ERR_INVALID_ARGUMENT, "the nonlinear output band does not fit in the time record");
+  if (!(d->q_step > 0) || !(d->freq_step > 0) || !(d->depth > 0))
+    return fail(GL_ERR_INVALID_ARGUMENT, "modal spacings and depth must be positive");
+  if (d->rank < 1 || d->rank > MAX_RANK || !d->nodes || !d->weights)
+    return fail(GL_ERR_RANK, "modal GL rule must have 1..%d nodes", MAX_RANK);
+  return GL_OK;
+}
+
+extern "C" gl_status gl_modal_workspace_size(const gl_modal_desc* d, size_t* bytes) {
+  gl_status s = modal_check(d);
+  if (s != GL_OK) return s;
+  if (!bytes) return fail(GL_ERR_INVALID_ARGUMENT, "null size pointer");
+  const size_t plane = (size_t)d->points * modal_pad(d->width) * sizeof(cplx);
+  *bytes = align_up(4096) + modal_buffers(d->order) * align_up(plane) +
+           2 * align_up((size_t)(3 * d->width + 3) * (sizeof(cplx) + sizeof(int)));
+  return GL_OK;
+}
+
+extern "C" gl_status gl_modal_level(const gl_modal_desc* d, int nnz, const long long* d_idx,
+                                    const double* d_val, void* d_eta22, void* d_eta33, void* d_ws,
+                                    size_t ws_bytes, void* stream) {
+  gl_status s = modal_check(d);
+  if (s != GL_OK) return s;
+  size_t need = 0;
+  gl_modal_workspace_size(d, &need);
+  if (!d_ws || ws_bytes < need || (reinterpret_cast<uintptr_t>(d_ws) & 255))
+    return fail(GL_ERR_WORKSPACE, "workspace must be 256-byte aligned and at least %zu bytes", need);
+  if (nnz < 0 || (nnz && (!d_idx || !d_val)) || !d_eta22 || (d->order >= 3 && !d_eta33))
+    return fail(GL_ERR_INVALID_ARGUMENT, "null modal buffers");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  cplx* tw = nullptr;
+  if ((s = device_twiddles(&tw)) != GL_OK) return s;
+  const int P = d->points, W = d->width, M = modal_pad(W);
+  const int wmax = (W - 1) / d->order;
+  const long long total = (long long)P * M;
+  const size_t plane = align_up((size_t)total * sizeof(cplx));
+  char* base = reinterpret_cast<char*>(d_ws);
+  double* dn = reinterpret_cast<double*>(base);  // nodes then weights
+  char* bufs = base + align_up(4096);
+  auto buf = [&](int k) { return reinterpret_cast<cplx*>(bufs + (size_t)k * plane); };
+  char* small = bufs + modal_buffers(d->order) * plane;
+  cplx* coef = reinterpret_cast<cplx*>(small);
+  int* bins = reinterpret_cast<int*>(small + align_up((size_t)(3 * W + 3) * sizeof(cplx)));
+  {
+    double host[2 * MAX_RANK] = {0};
+    std::memcpy(host, d->nodes, sizeof(double) * d->rank);
+    std::memcpy(host + MAX_RANK, d->weights, sizeof(double) * d->rank);
+    CUDA_TRY(cudaMemcpyAsync(dn, host, sizeof host, cudaMemcpyHostToDevice, st));
+    std::vector<int> hb(3 * W + 3);
+    for (int w = 0; w < 3 * wmax + 1; ++w) hb[w] = 3 * d->base_bin + w;
+    for (int w = 0; w < 2 * wmax + 1; ++w) hb[3 * wmax + 1 + w] = 2 * d->base_bin + w;
+    CUDA_TRY(cudaMemcpyAsync(bins, hb.data(), sizeof(int) * hb.size(), cudaMemcpyHostToDevice, st));
+    // the host vectors must outlive the copies
+    CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  ModalGeo g;
+  g.P = P;
+  g.M = M;
+  g.W = W;
+  g.q_step = d->q_step;
+  g.fstep = d->freq_step;
+  g.b0 = d->base_bin;
+  const int T = 256;
+  const int eb = grid_for((size_t)total, T, 8192);
+  cplx* joint = buf(0);
+  CUDA_TRY(cudaMemsetAsync(joint, 0, (size_t)total * sizeof(cplx), st));
+  if (nnz) {
+    // indices arrive in [P][W]; the joint is [P][M]
+    LaunchScope ls_("modal_scatter_kernel", st, 0.0);
+    modal_scatter_kernel<<<grid_for(nnz, T, 1024), T, 0, st>>>(d_idx, d_val, nnz, joint, W, M);
+  }
+  LAUNCH_CHECK("modal_scatter_kernel");
+  auto to_field = [&](cplx* b) -> gl_status {
+    gl_status r = axis0_transform(b, P, M, +1, 1.0, st, tw);
+    if (r != GL_OK) return r;
+    return axis_last_transform(b, P, M, -1, 1.0, st, tw);
+  };
+  auto to_spectrum = [&](cplx* b) -> gl_status {
+    gl_status r = axis_last_transform(b, P, M, +1, 1.0 / M, st, tw);
+    if (r != GL_OK) return r;
+    return axis0_transform(b, P, M, -1, 1.0 / P, st, tw);
+  };
+  auto bank = [&](const cplx* src, int k, int mult) -> gl_status {
+    {
+      LaunchScope ls_("modal_bank_kernel", st, 0.0);
+      modal_bank_kernel<<<eb, T, 0, st>>>(g, src, buf(k), mult);
+    }
+    LAUNCH_CHECK("modal_bank_kernel");
+    return to_field(buf(k));
+  };
+  // order-2 banks: 1 v, 2 vn, 3 vn2, 4 hx, 5 jx, 6 radial
+  const int m6[6] = {MM_ONE, MM_NU, MM_NU2, MM_Q_SNU, MM_Q, MM_Q2_SNU};
+  for (int k = 0; k < 6; ++k)
+    if ((s = bank(joint, 1 + k, m6[k])) != GL_OK) return s;
+  {
+    LaunchScope ls_("modal_sources_kernel", st, 0.0);
+    modal_sources_kernel<<<eb, T, 0, st>>>(total, buf(1), buf(2), buf(3), buf(4), buf(5), buf(6));
+  }
+  LAUNCH_CHECK("modal_sources_kernel");
+  cplx* SD = buf(3);
+  cplx* SK = buf(6);
+  if ((s = to_spectrum(SD)) != GL_OK) return s;
+  if ((s = to_spectrum(SK)) != GL_OK) return s;
+  ModalResp r;
+  std::memset(&r, 0, sizeof r);
+  r.g = g;
+  r.depth = d->depth;
+  r.nodes = dn;
+  r.weights = dn + MAX_RANK;
+  r.rank = d->rank;
+  r.sd = SD;
+  r.sk = SK;
+  r.out = coef + 3 * wmax + 1;
+  r.nbins = 2 * wmax + 1;
+  r.mult_b0 = 2;
+  r.kind = 2;
+  r.scale = d->scale22;
+  {
+    LaunchScope ls_("modal_response_kernel", st, 0.0);
+    modal_response_kernel<<<r.nbins, 256, 0, st>>>(r);
+  }
+  LAUNCH_CHECK("modal_response_kernel");
+  {
+    LaunchScope ls_("series_synth_kernel", st, 0.0);
+    series_synth_kernel<<<grid_for(d->count, T, 1024), T, 0, st>>>(bins + 3 * wmax + 1, r.out, r.nbins,
+                                                                  d->count, d_eta22, 0);
+  }
+  LAUNCH_CHECK("series_synth_kernel");
+  if (d->order < 3) return GL_OK;
+
+  // order 3: inner pair spectra, first-order and pair fields, cubic forcing
+  cplx* E2 = buf(7);
+  cplx* P2 = buf(8);
+  ModalResp ri = r;
+  ri.scale = d->lambda2;
+  ri.nbins = 2 * wmax + 1;
+  {
+    LaunchScope ls_("modal_pair_kernel", st, 0.0);
+    modal_pair_kernel<<<eb, T, 0, st>>>(ri, E2, P2);
+  }
+  LAUNCH_CHECK("modal_pair_kernel");
+  // first-order fields: v (1) and hx (4) are eta and phix; the others in 9..15
+  const int m7[7] = {MM_IQ, MM_MI_NU, MM_NU_Q, MM_MI_Q2_SNU, MM_MI_Q2_NU, MM_MINUS_NU2, MM_MINUS_Q2};
+  for (int k = 0; k < 7; ++k)
+    if ((s = bank(joint, 9 + k, m7[k])) != GL_OK) return s;
+  // pair fields 16..21: eta, etax (from e2); phix, phiz, phizz, phitz (from p2)
+  const int mp[6] = {MM_PAIR_E, MM_PAIR_EX, MM_PAIR_PX, MM_PAIR_PZ, MM_PAIR_PZZ, MM_PAIR_PTZ};
+  for (int k = 0; k < 6; ++k)
+    if ((s = bank(k < 2 ? E2 : P2, 16 + k, mp[k])) != GL_OK) return s;
+  ModalForcing fo;
+  fo.fe = buf(1);
+  fo.fex = buf(9);
+  fo.fpx = buf(4);
+  fo.fpz = buf(10);
+  fo.fpxz = buf(11);
+  fo.fpzz = buf(12);
+  fo.fpzzz = buf(13);
+  fo.fptz = buf(14);
+  fo.fptzz = buf(15);
+  fo.pe = buf(16);
+  fo.pex = buf(17);
+  fo.ppx = buf(18);
+  fo.ppz = buf(19);
+  fo.ppzz = buf(20);
+  fo.pptz = buf(21);
+  fo.fk = buf(2);  // vn and jx are free after the order-2 sources
+  fo.fd = buf(5);
+  fo.total = total;
+  {
+    LaunchScope ls_("modal_forcing_kernel", st, 0.0);
+    modal_forcing_kernel<<<eb, T, 0, st>>>(fo);
+  }
+  LAUNCH_CHECK("modal_forcing_kernel");
+  if ((s = to_spectrum(fo.fk)) != GL_OK) return s;
+  if ((s = to_spectrum(fo.fd)) != GL_OK) return s;
+  ModalResp r3 = r;
+  r3.sd = fo.fd;
+  r3.sk = fo.fk;
+  r3.out = coef;
+  r3.nbins = 3 * wmax + 1;
+  r3.mult_b0 = 3;
+  r3.kind = 3;
+  r3.scale = d->lambda3;
+  {
+    LaunchScope ls_("modal_response_kernel", st, 0.0);
+    modal_response_kernel<<<r3.nbins, 256, 0, st>>>(r3);
+  }
+  LAUNCH_CHECK("modal_response_kernel");
+  {
+    LaunchScope ls_("series_synth_kernel", st, 0.0);
+    series_synth_kernel<<<grid_for(d->count, T, 1024), T, 0, st>>>(bins, coef, r3.nbins, d->count,
+                                                                  d_eta33, 0);
+  }
+  LAUNCH_CHECK("series_synth_kernel");
+  return GL_OK;
+}
+
+static gl_status e20_check(const gl_eta20_desc* d) {
+  if (!d) return fail(GL_ERR_INVALID_ARGUMENT, "null eta20 descriptor");
+  if (!is_pow2(d->nx) || !is_pow2(d->ny) || d->nx < 16 || d->ny < 16 || d->nx > TW_N || d->ny > TW_N)
+    return fail(GL_ERR_UNSUPPORTED, "eta20 modal grids must be powers of two from 16 to %d", TW_N);
+  if (d->span < 0 || modal_pad(2 * d->span + 1) > TW_N)
+    return fail(GL_ERR_UNSUPPORTED, "the eta20 band exceeds %d bins", TW_N);
+  if (d->base_bin < 1 || d->count < 1 || !(d->qx_step > 0) || !(d->qy_step > 0) || !(d->freq_step > 0) ||
+      !(d->depth > 0) || !(d->dq > 0))
+    return fail(GL_ERR_INVALID_ARGUMENT, "bad eta20 descriptor");
+  if (d->rank < 1 || d->rank > MAX_RANK || !d->nodes || !d->weights)
+    return fail(GL_ERR_RANK, "eta20 GL rule must have 1..%d nodes", MAX_RANK);
+  return GL_OK;
+}
+
+extern "C" gl_status gl_eta20_workspace_size(const gl_eta20_desc* d, size_t* bytes) {
+  gl_status s = e20_check(d);
+  if (s != GL_OK) return s;
+  if (!bytes) return fail(GL_ERR_INVALID_ARGUMENT, "null size pointer");
+  const size_t plane = (size_t)d->ny * d->nx * modal_pad(2 * d->span + 1) * sizeof(cplx);
+  *bytes = align_up(4096) + 11 * align_up(plane);
+  return GL_OK;
+}
+
+extern "C" gl_status gl_eta20_level(const gl_eta20_desc* d, int nnz, const long long* d_idx,
+                                    const double* d_val, void* d_coef, void* d_ws, size_t ws_bytes,
+                                    void* stream) {
+  gl_status s = e20_check(d);
+  if (s != GL_OK) return s;
+  size_t need = 0;
+  gl_eta20_workspace_size(d, &need);
+  if (!d_ws || ws_bytes < need || (reinterpret_cast<uintptr_t>(d_ws) & 255))
+    return fail(GL_ERR_WORKSPACE, "workspace must be 256-byte aligned and at least %zu bytes", need);
+  if (nnz < 0 || (nnz && (!d_idx || !d_val)) || !d_coef)
+    return fail(GL_ERR_INVALID_ARGUMENT, "null eta20 buffers");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  cplx* tw = nullptr;
+  if ((s = device_twiddles(&tw)) != GL_OK) return s;
+  const int W = 2 * d->span + 1, M = modal_pad(W), nx = d->nx, ny = d->ny;
+  const long long total = (long long)ny * nx * M;
+  const size_t plane = align_up((size_t)total * sizeof(cplx));
+  char* base = reinterpret_cast<char*>(d_ws);
+  double* dn = reinterpret_cast<double*>(base);
+  {
+    double host[2 * MAX_RANK] = {0};
+    std::memcpy(host, d->nodes, sizeof(double) * d->rank);
+    std::memcpy(host + MAX_RANK, d->weights, sizeof(double) * d->rank);
+    CUDA_TRY(cudaMemcpyAsync(dn, host, sizeof host, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  auto buf = [&](int k) { return reinterpret_cast<cplx*>(base + align_up(4096) + (size_t)k * plane); };
+  E20Geo g;
+  g.ny = ny;
+  g.nx = nx;
+  g.M = M;
+  g.qx_step = d->qx_step;
+  g.qy_step = d->qy_step;
+  g.fstep = d->freq_step;
+  g.b0 = d->base_bin;
+  const int T = 256;
+  const int eb = grid_for((size_t)total, T, 8192);
+  cplx* joint = buf(0);
+  CUDA_TRY(cudaMemsetAsync(joint, 0, (size_t)total * sizeof(cplx), st));
+  if (nnz) {
+    LaunchScope ls_("modal_scatter_kernel", st, 0.0);
+    modal_scatter_kernel<<<grid_for(nnz, T, 1024), T, 0, st>>>(d_idx, d_val, nnz, joint, W, M);
+  }
+  LAUNCH_CHECK("modal_scatter_kernel");
+  // joint fields: inverse along y and x (unnormalised), forward along the bins
+  auto to_field = [&](cplx* b) -> gl_status {
+    gl_status r = launch_sfft(sfft(b, ny, (long long)nx * M, 1, nx * M, 0, 1.0), 1, +1, st, tw);
+    if (r != GL_OK) return r;
+    r = launch_sfft(sfft(b, nx, M, 1, M, (long long)nx * M, 1.0), ny, +1, st, tw);
+    if (r != GL_OK) return r;
+    return axis_last_transform(b, (long long)ny * nx, M, -1, 1.0, st, tw);
+  };
+  auto to_spectrum = [&](cplx* b) -> gl_status {
+    gl_status r = axis_last_transform(b, (long long)ny * nx, M, +1, 1.0 / M, st, tw);
+    if (r != GL_OK) return r;
+    r = launch_sfft(sfft(b, ny, (long long)nx * M, 1, nx * M, 0, 1.0), 1, -1, st, tw);
+    if (r != GL_OK) return r;
+    return launch_sfft(sfft(b, nx, M, 1, M, (long long)nx * M, 1.0 / ((double)nx * ny)), ny, -1, st, tw);
+  };
+  const int mults[8] = {E20_ONE, E20_NU2, E20_NU, E20_BX, E20_BY, E20_QX, E20_QY, E20_RAD};
+  for (int k = 0; k < 8; ++k) {
+    {
+      LaunchScope ls_("e20_bank_kernel", st, 0.0);
+      e20_bank_kernel<<<eb, T, 0, st>>>(g, joint, buf(1 + k), mults[k]);
+    }
+    LAUNCH_CHECK("e20_bank_kernel");
+    if ((s = to_field(buf(1 + k))) != GL_OK) return s;
+  }
+  E20Forcing fo;
+  fo.one = buf(1);
+  fo.dno = buf(2);
+  fo.nuf = buf(3);
+  fo.bx = buf(4);
+  fo.by = buf(5);
+  fo.qxf = buf(6);
+  fo.qyf = buf(7);
+  fo.rad = buf(8);
+  fo.fd = buf(9);
+  fo.fk = buf(10);
+  fo.total = total;
+  {
+    LaunchScope ls_("e20_forcing_kernel", st, 0.0);
+    e20_forcing_kernel<<<eb, T, 0, st>>>(fo);
+  }
+  LAUNCH_CHECK("e20_forcing_kernel");
+  if ((s = to_spectrum(fo.fd)) != GL_OK) return s;
+  if ((s = to_spectrum(fo.fk)) != GL_OK) return s;
+  E20Resp r;
+  r.g = g;
+  r.fd = fo.fd;
+  r.fk = fo.fk;
+  r.out = reinterpret_cast<cplx*>(d_coef);
+  r.span = d->span;
+  r.dq = d->dq;
+  r.depth = d->depth;
+  r.nodes = dn;
+  r.weights = dn + MAX_RANK;
+  r.rank = d->rank;
+  {
+    LaunchScope ls_("e20_response_kernel", st, 0.0);
+    e20_response_kernel<<<W, 256, 0, st>>>(r);
+  }
+  LAUNCH_CHECK("e20_response_kernel");
+  return GL_OK;
+}
+
+extern "C" gl_status gl_series_synthesize(int count, int n_bins, const int* d_bins, const void* d_coef,
+                                          void* d_out, int real_only, void* stream) {
+  if (count < 1 || n_bins < 0 || (n_bins && (!d_bins || !d_coef)) || !d_out)
+    return fail(GL_ERR_INVALID_ARGUMENT, "bad series synthesis arguments");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  {
+    LaunchScope ls_("series_synth_kernel", st, 0.0);
+    series_synth_kernel<<<grid_for(count, 256, 1024), 256, 0, st>>>(
+        d_bins, reinterpret_cast<const cplx*>(d_coef), n_bins, count, d_out, real_only);
+  }
+  LAUNCH_CHECK("series_synth_kernel");
   return GL_OK;
 }
 

@@ -57,6 +57,22 @@ class Eta44Desc(C.Structure):
                 ("gravity", C.c_double)]
 
 
+class ModalDesc(C.Structure):
+    _fields_ = [("points", C.c_int), ("width", C.c_int), ("order", C.c_int),
+                ("base_bin", C.c_int), ("count", C.c_int), ("q_step", C.c_double),
+                ("freq_step", C.c_double), ("depth", C.c_double), ("scale22", C.c_double),
+                ("lambda2", C.c_double), ("lambda3", C.c_double), ("rank", C.c_int),
+                ("nodes", C.POINTER(C.c_double)), ("weights", C.POINTER(C.c_double))]
+
+
+class Eta20Desc(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("span", C.c_int), ("base_bin", C.c_int),
+                ("count", C.c_int), ("qx_step", C.c_double), ("qy_step", C.c_double),
+                ("freq_step", C.c_double), ("depth", C.c_double), ("dq", C.c_double),
+                ("rank", C.c_int), ("nodes", C.POINTER(C.c_double)),
+                ("weights", C.POINTER(C.c_double))]
+
+
 class PlanInfo(C.Structure):
     _fields_ = [
         ("ncx", C.c_int), ("ncy", C.c_int),
@@ -100,6 +116,14 @@ SIGNATURES = {
     "gl_deposit_modes_adjoint": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                            C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p]),
+    "gl_modal_workspace_size": (C.c_int, [C.POINTER(ModalDesc), C.POINTER(C.c_size_t)]),
+    "gl_modal_level": (C.c_int, [C.POINTER(ModalDesc), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
+    "gl_eta20_workspace_size": (C.c_int, [C.POINTER(Eta20Desc), C.POINTER(C.c_size_t)]),
+    "gl_eta20_level": (C.c_int, [C.POINTER(Eta20Desc), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_size_t, C.c_void_p]),
+    "gl_series_synthesize": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                       C.c_void_p]),
     "gl_fft2": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "gl_box_synthesize_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                             C.c_int, C.c_void_p, C.c_double, C.c_void_p, C.c_int,

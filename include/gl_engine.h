@@ -202,6 +202,58 @@ gl_status gl_deposit_modes_adjoint(const gl_plan* plan, int n_units, int n_segme
                                    const double* d_omega, const double* d_times,
                                    const void* d_grad, double* d_gab, void* stream);
 
+/* Single-direction time path: one level of the modal GL resolvent of
+ * python/src/green_laplace/modal_time.py:217-360 (_modal_sum_components).
+ * The caller selects the record's DFT band and deposits its amplitudes onto
+ * the modal q-axis (d_idx = row * width + work bin, rows in numpy's
+ * ifftshift order, d_val = complex pairs, indices distinct); the call
+ * evaluates the order-2 (and order-3) graph on the joint (q, bin) grid and
+ * writes the analytic eta22 (eta33) time series, count complex128 samples
+ * each, i.e. numpy.fft.fft of the output-bin coefficients. */
+typedef struct gl_modal_desc {
+  int points;                 /* modal q nodes P (power of two, 16 .. 2^24)  */
+  int width;                  /* work bins W = order * max work bin + 1      */
+  int order;                  /* 2 or 3                                      */
+  int base_bin;               /* first retained DFT bin                      */
+  int count;                  /* samples of the record                      */
+  double q_step;              /* q-axis spacing                              */
+  double freq_step;           /* 2 pi / (count dt) sqrt(depth / gravity)     */
+  double depth;
+  double scale22, lambda2, lambda3;  /* GL scales (standalone eta22, inner, outer) */
+  int rank;                   /* GL rank                                     */
+  const double* nodes;        /* host GL rule of length rank                 */
+  const double* weights;
+} gl_modal_desc;
+gl_status gl_modal_workspace_size(const gl_modal_desc* desc, size_t* bytes);
+gl_status gl_modal_level(const gl_modal_desc* desc, int nnz, const long long* d_idx,
+                         const double* d_val, void* d_eta22, void* d_eta33, void* d_workspace,
+                         size_t workspace_bytes, void* stream);
+
+/* Difference-frequency eta20 on a 2-D modal grid (python/src/green_laplace/
+ * _eta20.py:13-143, unidirectional_eta20): deposit indices
+ * (iy * nx + ix) * (2 span + 1) + work bin; d_coef receives the 2 span + 1
+ * output coefficients at signed bins 0..span, -span..-1 (before the
+ * Hermitian projection of _eta20.py:170-180). */
+typedef struct gl_eta20_desc {
+  int nx, ny;                 /* modal grid (powers of two, 16 .. 4096)      */
+  int span;                   /* max work bin                                */
+  int base_bin, count;
+  double qx_step, qy_step, freq_step, depth;
+  double dq;                  /* rms pair wavenumber spread (the GL scale)   */
+  int rank;
+  const double* nodes;        /* host GL rule                                */
+  const double* weights;
+} gl_eta20_desc;
+gl_status gl_eta20_workspace_size(const gl_eta20_desc* desc, size_t* bytes);
+gl_status gl_eta20_level(const gl_eta20_desc* desc, int nnz, const long long* d_idx,
+                         const double* d_val, void* d_coef, void* d_workspace,
+                         size_t workspace_bytes, void* stream);
+
+/* out[n] = sum_b coef_b exp(-2 pi i bins_b n / count), n < count (a sparse
+ * numpy.fft.fft; real parts only when real_only != 0). */
+gl_status gl_series_synthesize(int count, int n_bins, const int* d_bins, const void* d_coef,
+                               void* d_out, int real_only, void* stream);
+
 /* Batched 2-D complex FFT on [batch][ny][nx] complex128 with numpy's
  * conventions: forward = fft2 (unnormalised), inverse = ifft2 (1/(nx ny)).
  * In-place (d_in == d_out) is allowed.  Replaces the numpy.fft.fft2/ifft2

@@ -62,3 +62,56 @@ def test_oracle_matches_reference_python(tag):
         if f"{tag}/{k}" in GOLD:
             assert rel(c[k], GOLD[f"{tag}/{k}"]) < 1e-14, k
     assert rel(eta, GOLD[tag + "/eta"]) < 1e-14
+
+
+# ---------------------------------------------------------------------------
+# GPU: the engine's modal path (gl_modal_level, gl_eta20_level)
+# ---------------------------------------------------------------------------
+
+
+@pytest.mark.gpu
+def test_engine_matches_matlab_fixtures():
+    from gl_engine import modal
+
+    r = modal.reconstruct_unidirectional_modal_timeseries(GOLD["m3/eta1"], GOLD["m3/time"],
+                                                          **_matlab_m3())
+    e22, e33 = rel(r.components["eta22"], GOLD["m3/eta22"]), rel(r.components["eta33"], GOLD["m3/eta33"])
+    print(f"MATLAB modal order 3: eta22 {e22:.2e}, eta33 {e33:.2e}")
+    assert e22 < 3e-13 and e33 < 3e-13
+    r = modal.reconstruct_unidirectional_timeseries(GOLD["e20/eta1"], GOLD["e20/time"], **_matlab_e20())
+    e20 = rel(r.components["eta20"], GOLD["e20/eta20"])
+    print(f"MATLAB eta20: {e20:.2e}")
+    assert e20 < 8e-11
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tag", ["ladder3", "broad3", "o2e20"])
+def test_engine_matches_reference_python(tag):
+    from gl_engine import modal
+
+    r = modal.reconstruct_unidirectional_modal_timeseries(GOLD[tag + "/eta1"], GOLD[tag + "/time"],
+                                                          **_kw(tag))
+    assert [lv["modal_points"] for lv in r.audit["levels"]] == list(GOLD[tag + "/levels"])
+    for k in ("eta11", "eta22", "eta33", "eta20"):
+        if f"{tag}/{k}" in GOLD:
+            err = rel(r.components[k], GOLD[f"{tag}/{k}"])
+            print(f"{tag} {k}: {err:.2e}")
+            assert err < 1e-12, k
+    assert not r.audit["auxiliary_space_domain"]
+
+
+@pytest.mark.gpu
+def test_engine_four_step_axis_matches_oracle():
+    """q-axes above 4096 nodes take the two-pass (four-step) transform; the
+    level must equal the oracle's single-transform result."""
+    from gl_engine import modal
+
+    kw = dict(depth=1.0, omega_max=2 * np.pi * 24 / (512 * 0.2) + 1e-12, energy_fraction=1.0,
+              quadrature_rank=4, order=3, modal_points=8192, include_eta20=False)
+    eta1, t = GOLD["ladder3/eta1"], GOLD["ladder3/time"]
+    _, c, _ = M.modal_timeseries(eta1, t, **kw)
+    r = modal.reconstruct_unidirectional_modal_timeseries(eta1, t, **kw)
+    for k in ("eta22", "eta33"):
+        err = rel(r.components[k], c[k])
+        print(f"four-step P=8192 {k}: {err:.2e}")
+        assert err < 1e-12, k
