@@ -1012,18 +1012,22 @@ static gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, c
   return GL_OK;
 }
 
+template <int K>
+static void row_launch(dim3 grid, int threads, size_t smem, cudaStream_t st, const RowArgs& a,
+                       const cplx* tw) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(row_kernel_t<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    attr = true;
+  }
+  row_kernel_t<K><<<grid, threads, smem, st>>>(a, tw);
+}
+
 static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
   int nb = 0;
   for (int g = 0; g < a.ngrp; ++g) nb += a.grp[g].nb;
   const bool e44 = a.kind >= ROW_E44_PAIR && a.kind <= ROW_E44_ORDER4_PSI;
   const size_t smem = row_smem(nb, a.nx);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(row_kernel_t<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    cudaFuncSetAttribute(row_kernel_t<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    cudaFuncSetAttribute(row_kernel_t<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    attr = true;
-  }
   dim3 grid(a.ny, njobs);
   // 8 transform groups per block (n/16 threads each) when the row has at
   // most 12 banks (4 blocks fit per SM by shared memory), 16 for the wider
@@ -1040,12 +1044,21 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
                      : a.kind >= ROW_E44_PAIR    ? "row_kernel[order4]"
                                                  : "row_kernel[order2]";
   LaunchScope ls(name, st, bytes);
-  if (adj)
-    row_kernel_t<1><<<grid, threads, smem, st>>>(a, tw);
-  else if (e44)
-    row_kernel_t<2><<<grid, threads, smem, st>>>(a, tw);
-  else
-    row_kernel_t<0><<<grid, threads, smem, st>>>(a, tw);
+  switch (a.kind) {
+    case ROW_ETA22: row_launch<ROW_ETA22>(grid, threads, smem, st, a, tw); break;
+    case ROW_PSI22: row_launch<ROW_PSI22>(grid, threads, smem, st, a, tw); break;
+    case ROW_CONTACT22: row_launch<ROW_CONTACT22>(grid, threads, smem, st, a, tw); break;
+    case ROW_INNER: row_launch<ROW_INNER>(grid, threads, smem, st, a, tw); break;
+    case ROW_OUTER: row_launch<ROW_OUTER>(grid, threads, smem, st, a, tw); break;
+    case ROW_E44_PAIR: row_launch<ROW_E44_PAIR>(grid, threads, smem, st, a, tw); break;
+    case ROW_E44_THIRD: row_launch<ROW_E44_THIRD>(grid, threads, smem, st, a, tw); break;
+    case ROW_E44_ORDER4: row_launch<ROW_E44_ORDER4>(grid, threads, smem, st, a, tw); break;
+    case ROW_E44_ORDER4_PSI: row_launch<ROW_E44_ORDER4_PSI>(grid, threads, smem, st, a, tw); break;
+    case ROW_ADJ_ETA22: row_launch<ROW_ADJ_ETA22>(grid, threads, smem, st, a, tw); break;
+    case ROW_ADJ_INNER: row_launch<ROW_ADJ_INNER>(grid, threads, smem, st, a, tw); break;
+    case ROW_ADJ_OUTER: row_launch<ROW_ADJ_OUTER>(grid, threads, smem, st, a, tw); break;
+    default: return fail(GL_ERR_INVALID_ARGUMENT, "unknown row kind %d", a.kind);
+  }
   LAUNCH_CHECK("row_kernel");
   return GL_OK;
 }

@@ -706,10 +706,13 @@ GL_D void row_products_adj(int kind, cplx* b, int L, int p) {
 // zero outside the bank's box columns, 16 loads in flight per thread), the
 // stage's products, forward transforms of the outputs, and only the output
 // box's columns are written: [job][out][y][col].
-// FAMILY 0: order-2/3 stages, 1: adjoint stages, 2: order-4 stages (their
-// rows are wider than 24 banks and are staged in shared memory first).
-template <int FAMILY>
+// One instantiation per row kind, so that each stage's products are compiled
+// (and get registers) on their own.  FAMILY 0: order-2/3 stages, 1: adjoint
+// stages, 2: order-4 stages (their rows are wider than 24 banks and are
+// staged in shared memory first).
+template <int KIND>
 __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __restrict__ tw) {
+  constexpr int FAMILY = KIND >= ROW_ADJ_ETA22 ? 1 : (KIND >= ROW_E44_PAIR && KIND <= ROW_E44_ORDER4_PSI ? 2 : 0);
   extern __shared__ cplx smem[];
   const int y = blockIdx.x;
   const int job = blockIdx.y;
@@ -776,12 +779,12 @@ __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __
   }
   __syncthreads();
   if constexpr (FAMILY == 0) {
-    const int chan_count = a.kind == ROW_PSI22 ? a.us[job / a.jobs_per_unit].chan_count : 0;
-    for (int p = threadIdx.x; p < n; p += blockDim.x) row_products(a.kind, banks, L, phys(p), chan_count);
+    const int chan_count = KIND == ROW_PSI22 ? a.us[job / a.jobs_per_unit].chan_count : 0;
+    for (int p = threadIdx.x; p < n; p += blockDim.x) row_products(KIND, banks, L, phys(p), chan_count);
   } else if constexpr (FAMILY == 2) {
-    for (int p = threadIdx.x; p < n; p += blockDim.x) row_products_e44(a.kind, banks, L, phys(p));
+    for (int p = threadIdx.x; p < n; p += blockDim.x) row_products_e44(KIND, banks, L, phys(p));
   } else {
-    for (int p = threadIdx.x; p < n; p += blockDim.x) row_products_adj(a.kind, banks, L, phys(p));
+    for (int p = threadIdx.x; p < n; p += blockDim.x) row_products_adj(KIND, banks, L, phys(p));
   }
   __syncthreads();
   const int na = a.nout_a > 0 ? a.nout_a : a.nout;
