@@ -1130,7 +1130,7 @@ static void mink_args(MinkArgs& m, const unsigned long long* a, int ha, int wa, 
 static gl_status final_output(gl_plan* p, int gu, const Box& box, const double* geo,
                               const cplx* spec, long long spec_stride, int nb, const int* mults,
                               const int* srcs, int comp_offset, void* outputs, void* scratch,
-                              cudaStream_t st, const double* comp_scale_dev) {
+                              cudaStream_t st, const double* comp_scale_dev, UnitScalars* us) {
   ColArgs a;
   std::memset(&a, 0, sizeof a);
   a.kind = COL_PLAIN;
@@ -1165,6 +1165,7 @@ static gl_status final_output(gl_plan* p, int gu, const Box& box, const double* 
   o.comp_scale = comp_scale_dev + comp_offset;
   o.out = outputs;
   o.real_only = p->d.output == GL_OUT_REAL;
+  o.us = us;
   return launch_out_rows(o, gu * nb, st, p->tw);
 }
 
@@ -1764,19 +1765,19 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     }
     const int srcs[2] = {0, 0};  // both read the parent spectrum
     if ((s = final_output(p, gu, B1, p->geo1, spec, pl1, n, mults, srcs, off, outputs, scratch, st,
-                          p->comp_scale)) != GL_OK)
+                          p->comp_scale, us)) != GL_OK)
       return s;
   }
   if (p->want_eta22) {
     const int m1[1] = {M_ONE}, z1[1] = {0};
     if ((s = final_output(p, gu, B2, p->geo2, out22, pl2, 1, m1, z1, comp_slot(p, GL_COMP_ETA22),
-                          outputs, scratch, st, p->comp_scale)) != GL_OK)
+                          outputs, scratch, st, p->comp_scale, us)) != GL_OK)
       return s;
   }
   if (p->want_psi22) {
     const int m1[1] = {M_ONE}, z1[1] = {0};
     if ((s = final_output(p, gu, B2, p->geo2, outp22, pl2, 1, m1, z1, comp_slot(p, GL_COMP_PSI22),
-                          outputs, scratch, st, p->comp_scale)) != GL_OK)
+                          outputs, scratch, st, p->comp_scale, us)) != GL_OK)
       return s;
   }
   if (p->want_o3) {
@@ -1784,24 +1785,16 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     const int ce = comp_slot(p, GL_COMP_ETA33), cp = comp_slot(p, GL_COMP_PSI33);
     if (ce >= 0 && cp >= 0) {
       if ((s = final_output(p, gu, B3, p->geo3, out33, 2LL * pl3, 2, m2, s01, ce, outputs, scratch, st,
-                            p->comp_scale)) != GL_OK)
+                            p->comp_scale, us)) != GL_OK)
         return s;
     } else {
       const int which = ce >= 0 ? 0 : 1;
       if ((s = final_output(p, gu, B3, p->geo3, out33 + (size_t)which * pl3, 2LL * pl3, 1, m2,
-                            s01, ce >= 0 ? ce : cp, outputs, scratch, st, p->comp_scale)) != GL_OK)
+                            s01, ce >= 0 ? ce : cp, outputs, scratch, st, p->comp_scale, us)) != GL_OK)
         return s;
     }
   }
-  {
-    const size_t per_unit = (size_t)p->ncomp * p->d.nx * p->d.ny;
-    dim3 g(grid_for(per_unit, T, 256), gu);
-    {
-      LaunchScope ls_("nonfinite_kernel", st, 0.0);
-      nonfinite_kernel<<<g, T, 0, st>>>(outputs, per_unit, p->d.output == GL_OUT_REAL, us);
-    }
-    LAUNCH_CHECK("nonfinite_kernel");
-  }
+  // non-finite outputs were flagged by the final transform (out_row_kernel)
   if (status) {
     {
       LaunchScope ls_("status_kernel", st, 0.0);
@@ -2096,15 +2089,9 @@ static gl_status e44_finalize(gl_plan* p, int gu, const cplx* OUT, unsigned long
   o.comp_scale = p->comp_scale;
   o.out = outputs;
   o.real_only = p->d.output == GL_OUT_REAL;
+  o.us = us;  // non-finite outputs set the unit status inside the transform
   if ((s = launch_out_rows(o, gu * nout, st, p->tw)) != GL_OK) return s;
   if (us) {
-    const size_t per_unit = (size_t)nout * p->d.nx * p->d.ny;
-    dim3 g(grid_for(per_unit, T, 256), gu);
-    {
-      LaunchScope ls_("nonfinite_kernel", st, 0.0);
-      nonfinite_kernel<<<g, T, 0, st>>>(outputs, per_unit, p->d.output == GL_OUT_REAL, us);
-    }
-    LAUNCH_CHECK("nonfinite_kernel");
     if (status) {
       {
         LaunchScope ls_("status_kernel", st, 0.0);

@@ -58,15 +58,22 @@ __global__ void acc_e44_pair_kernel(E44Acc a) {
   const int plane = a.box.w * a.box.h;
   const UnitScalars& u = a.us[unit];
   double lm[5] = {0, 0, 0, 0, 0};
+  __shared__ double s_t[MAX_RANK], s_co[MAX_RANK];
+  if (threadIdx.x < R) {
+    const double x = a.nodes[threadIdx.x], w = a.weights[threadIdx.x];
+    const double t = x / u.lam2;
+    s_t[threadIdx.x] = t;
+    s_co[threadIdx.x] = w * exp(x) / u.lam2 * exp(-2.0 * u.shift2 * t) / 4.0;
+  }
+  __syncthreads();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
     const GeoRef G{a.geo, plane, i};
     const double A = G.a(), sqa = __ldg(a.geo + 5 * plane + i);
     cplx es = czero(), ets = czero(), ps = czero(), pts = czero(), ptts = czero();
     for (int p = 0; p < R; ++p) {
       const int job = unit * jobs_per_unit + g * R + p;
-      const double x = a.nodes[p], w = a.weights[p];
-      const double t = x / u.lam2;
-      const double co = w * exp(x) / u.lam2 * exp(-2.0 * u.shift2 * t) / 4.0;
+      const double t = s_t[p];
+      const double co = s_co[p];
       const double sh = sinh_over_root(sqa, t), ch = cosh(sqa * t);
       const cplx* src = a.in + (size_t)job * 6 * plane;
       cplx s[6];
@@ -99,15 +106,22 @@ __global__ void acc_e44_third_kernel(E44Acc a) {
   const UnitScalars& u = a.us[unit];
   const int ns = a.nspec;
   double lm[4] = {0, 0, 0, 0};
+  __shared__ double s_t[MAX_RANK], s_co[MAX_RANK];
+  if (threadIdx.x < R) {
+    const double x = a.nodes[threadIdx.x], w = a.weights[threadIdx.x];
+    const double tt = x / u.lam3;
+    s_t[threadIdx.x] = tt;
+    s_co[threadIdx.x] = w * exp(x) / u.lam3 * exp(-3.0 * u.shift3 * tt);
+  }
+  __syncthreads();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
     const GeoRef G{a.geo, plane, i};
     const double A = G.a(), sqa = __ldg(a.geo + 5 * plane + i);
     cplx es = czero(), ps = czero(), pts = czero(), ets = czero();
     for (int t = 0; t < R; ++t) {
       const int job = uo * R + t;
-      const double x = a.nodes[t], w = a.weights[t];
-      const double tt = x / u.lam3;
-      const double co = w * exp(x) / u.lam3 * exp(-3.0 * u.shift3 * tt);
+      const double tt = s_t[t];
+      const double co = s_co[t];
       const double sh = sinh_over_root(sqa, tt), ch = cosh(sqa * tt);
       const cplx* src = a.in + (size_t)job * 4 * plane;
       cplx s[4];
@@ -140,15 +154,22 @@ __global__ void acc_e44_order4_kernel(E44Acc a) {
   const int ns = a.nspec;
   const int nout = ns == 4 ? 2 : 1;
   double lm[1] = {0};
+  __shared__ double s_t[MAX_RANK], s_co[MAX_RANK];
+  if (threadIdx.x < a.Ro) {
+    const double x = a.nodes[a.outer0 + threadIdx.x], w = a.weights[a.outer0 + threadIdx.x];
+    const double tm = x / u.lam4;
+    s_t[threadIdx.x] = tm;
+    s_co[threadIdx.x] = w * exp(x) / u.lam4 * exp(-4.0 * u.shift4 * tm);
+  }
+  __syncthreads();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
     const GeoRef G{a.geo, plane, i};
     const double A = G.a(), sqa = __ldg(a.geo + 5 * plane + i);
     cplx acc = czero(), psi = czero();
     for (int ol = 0; ol < a.Ro; ++ol) {
       const int job = unit * a.Ro + ol;
-      const double x = a.nodes[a.outer0 + ol], w = a.weights[a.outer0 + ol];
-      const double tm = x / u.lam4;
-      const double co = w * exp(x) / u.lam4 * exp(-4.0 * u.shift4 * tm);
+      const double tm = s_t[ol];
+      const double co = s_co[ol];
       const double sh = sinh_over_root(sqa, tm), ch = cosh(sqa * tm);
       const cplx* src = a.in + (size_t)job * ns * plane;
       const unsigned long long* mx = a.maxin + (size_t)job * ns;

@@ -913,14 +913,22 @@ __global__ void acc_eta22_kernel(AccArgs a) {
   const int unit = blockIdx.y;
   const int plane = a.box.w * a.box.h;
   const UnitScalars& u = a.us[unit];
+  // per-node times and coefficients, once per block
+  __shared__ double s_tau[MAX_RANK], s_coef[MAX_RANK];
+  if (threadIdx.x < a.nnodes) {
+    const double x = a.nodes[threadIdx.x], w = a.weights[threadIdx.x];
+    const double tau = x / u.lam22;
+    s_tau[threadIdx.x] = tau;
+    s_coef[threadIdx.x] = w * exp(x) / u.lam22 / 4.0 * exp(-2.0 * u.shift2 * tau);
+  }
+  __syncthreads();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
     BinGeo g = load_geo(a.geo, plane, i);
     cplx acc = czero();
     for (int nn = 0; nn < a.nnodes; ++nn) {
       const int js = unit * a.nnodes + nn;
-      const double x = a.nodes[nn], w = a.weights[nn];
-      const double tau = x / u.lam22;
-      const double coef = w * exp(x) / u.lam22 / 4.0 * exp(-2.0 * u.shift2 * tau);
+      const double tau = s_tau[nn];
+      const double coef = s_coef[nn];
       const double sh = sinh_over_root(g.sqa, tau);
       const double ch = cosh(g.sqa * tau);
       cplx sd = floored(a.in[((size_t)js * 2 + 0) * plane + i], a.floor_rel, a.maxin[js * 2 + 0]);
@@ -985,14 +993,21 @@ __global__ void acc_inner_kernel(AccArgs a) {
   const int plane = a.box.w * a.box.h;
   const UnitScalars& u = a.us[unit];
   double local = 0.0;
+  __shared__ double s_tau[MAX_RANK], s_coef[MAX_RANK];
+  if (threadIdx.x < a.nnodes) {
+    const double x = a.nodes[threadIdx.x], w = a.weights[threadIdx.x];
+    const double tau = x / u.lam2;
+    s_tau[threadIdx.x] = tau;
+    s_coef[threadIdx.x] = w * exp(x) / u.lam2 * exp(-2.0 * u.shift2 * tau) / 4.0;
+  }
+  __syncthreads();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
     BinGeo g = load_geo(a.geo, plane, i);
     cplx e = czero(), et = czero(), p = czero(), pt = czero();
     for (int ii = 0; ii < a.nnodes; ++ii) {
       const int js = uj * a.nnodes + ii;
-      const double x = a.nodes[ii], w = a.weights[ii];
-      const double tau = x / u.lam2;
-      const double coef = w * exp(x) / u.lam2 * exp(-2.0 * u.shift2 * tau) / 4.0;
+      const double tau = s_tau[ii];
+      const double coef = s_coef[ii];
       const double sh = sinh_over_root(g.sqa, tau);
       const double ch = cosh(g.sqa * tau);
       const cplx* src = a.in + (size_t)js * 4 * plane;
@@ -1065,16 +1080,23 @@ __global__ void acc_outer_kernel(AccArgs a, const unsigned long long* maxpsi) {
   const int unit = blockIdx.y;
   const int plane = a.box.w * a.box.h;
   const UnitScalars& u = a.us[unit];
+  __shared__ double s_tau[MAX_RANK], s_coef[MAX_RANK];
+  if (threadIdx.x < a.nnodes) {
+    const double x = a.nodes[threadIdx.x], w = a.weights[threadIdx.x];
+    const double tau = x / u.lam3;
+    s_tau[threadIdx.x] = tau;
+    s_coef[threadIdx.x] = w * exp(x) / u.lam3 * exp(-3.0 * u.shift3 * tau);
+  }
+  __syncthreads();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
     BinGeo g = load_geo(a.geo, plane, i);
     cplx eta = czero(), psi = czero();
     for (int j = 0; j < a.nnodes; ++j) {
       const int uj = unit * a.nnodes + j;
-      const double x = a.nodes[j], w = a.weights[j];
-      const double tau = x / u.lam3;
+      const double tau = s_tau[j];
       const double sh = sinh_over_root(g.sqa, tau);
       const double ch = cosh(g.sqa * tau);
-      const double coef = w * exp(x) / u.lam3 * exp(-3.0 * u.shift3 * tau);
+      const double coef = s_coef[j];
       const cplx* fsrc = a.in + (size_t)uj * 4 * plane;
       const cplx fk = fsrc[i], fd = fsrc[plane + i];
       const cplx* psrc = a.extra + (size_t)uj * 2 * plane;
@@ -1106,6 +1128,7 @@ struct OutArgs {
   void* out;            // [unit][out_ncomp][ny][nx]
   int real_only;        // write float64 real parts instead of complex
   int rows;             // rows per block
+  UnitScalars* us;      // non-null: a non-finite output sets the unit's status
 };
 
 // Final inverse transform along x on the reference grid: each group of n/16
@@ -1131,14 +1154,27 @@ __global__ void __launch_bounds__(256, 2) out_row_kernel(OutArgs a, const cplx* 
     const int xi = wrap(xb - a.x0, n);
     return xi < a.w ? row[xi] : czero();
   };
+  bool bad = false;  // the output check of the unit's status, folded into the store
   if (a.real_only) {
     double* o = reinterpret_cast<double*>(a.out) + base;
-    auto store = [&](int xb, cplx v) { o[xb] = s * v.x; };
+    auto store = [&](int xb, cplx v) {
+      const double r = s * v.x;
+      bad |= !isfinite(r);
+      o[xb] = r;
+    };
     fft_row<+1>(buf, f, active, tw, load, store);
   } else {
     cplx* o = reinterpret_cast<cplx*>(a.out) + base;
-    auto store = [&](int xb, cplx v) { o[xb] = cscale(s, v); };
+    auto store = [&](int xb, cplx v) {
+      const cplx r = cscale(s, v);
+      bad |= !(isfinite(r.x) && isfinite(r.y));
+      o[xb] = r;
+    };
     fft_row<+1>(buf, f, active, tw, load, store);
+  }
+  if (a.us) {
+    const bool any = __any_sync(0xffffffffu, bad);
+    if (any && (threadIdx.x & 31) == 0) atomicCAS(&a.us[unit].status, 0, (int)GL_ERR_NONFINITE);
   }
 }
 
