@@ -44,6 +44,14 @@ GL_D double as_double(unsigned long long bits) { return __longlong_as_double((lo
 // Index of signed mode number m on a periodic grid of length n (power of two).
 GL_HD int wrap(int m, int n) { return m & (n - 1); }
 
+// The same for any length n > 0 (column grids of length 16 m, m not a power
+// of two); the power-of-two test is uniform across a launch.
+GL_HD int wrap_any(int m, int n) {
+  if ((n & (n - 1)) == 0) return m & (n - 1);
+  const int r = m % n;
+  return r < 0 ? r + n : r;
+}
+
 struct Box {
   int x0, y0, w, h;  // signed mode origin, width (x) and height (y)
 };

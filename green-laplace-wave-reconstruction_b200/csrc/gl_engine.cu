@@ -170,10 +170,23 @@ __global__ void geo_kernel(double* geo, Box box, int nx, int ny, double lx, doub
   }
 }
 
-__global__ void twiddle_kernel(cplx* tw) {
-  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < TW_N; m += gridDim.x * blockDim.x) {
+// tw[m] = exp(-2 pi i m/TW_N) for m < TW_N; with count = TW_ALLOC also the
+// tables of the mixed lengths n = 16 m after it (W_n^e, e < n).
+__global__ void twiddle_kernel(cplx* tw, int count) {
+  for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < count; m += gridDim.x * blockDim.x) {
+    int n = TW_N, e = m;
+    if (m >= TW_N) {
+      const int lens[7] = {48, 80, 96, 144, 160, 192, 240};
+      for (int k = 0; k < 7; ++k) {
+        const int off = TW_N + mixed_tw_offset(lens[k]);
+        if (m >= off && m < off + lens[k]) {
+          n = lens[k];
+          e = m - off;
+        }
+      }
+    }
     double s, c;
-    sincospi(2.0 * (double)m / (double)TW_N, &s, &c);
+    sincospi(2.0 * (double)e / (double)n, &s, &c);
     tw[m] = cmk(c, -s);
   }
 }
@@ -636,6 +649,11 @@ struct gl_plan {
   int ncomp;
   int comp_ids[6];
   int ncx, ncy, lncx, lncy, lnx, lny;
+  // forward column grids of the pair (eta22, psi22, inner order-3) and triple
+  // (outer order-3) stages: the smallest column lengths >= the box heights,
+  // mixed lengths 16 m allowed (log2 0 for those); ncy (a power of two) is
+  // the adjoint's grid and bounds both
+  int ncy2, lncy2, ncy3, lncy3;
   Box b1, b2, b3;
   int ww1, ww2;                 // bitset words per row (S1, S2)
   bool want_eta22, want_psi22, want_o3, want_first;
@@ -678,6 +696,17 @@ static int next_pow2(int v) {
   return p;
 }
 static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// Smallest column-transform length >= v: a power of two (>= 16) or one of the
+// mixed lengths 16 m the column kernels run.
+static int col_len(int v) {
+  int best = std::max(16, next_pow2(v));
+  const int mixed[7] = {48, 80, 96, 144, 160, 192, 240};
+  for (int k = 0; k < 7; ++k)
+    if (mixed[k] >= v && mixed[k] < best) best = mixed[k];
+  return best;
+}
+static int col_log2(int n) { return is_pow2(n) ? ilog2(n) : 0; }
 
 struct Bump {
   size_t off = 0;
@@ -837,6 +866,13 @@ extern "C" gl_status gl_plan_create(gl_plan** out, const gl_plan_desc* desc) {
   }
   p->lncx = ilog2(p->ncx);
   p->lncy = ilog2(p->ncy);
+  p->ncy2 = p->ncy3 = p->ncy;
+  if (d.grid != GL_GRID_REFERENCE && deg > 1) {
+    p->ncy2 = std::min(p->ncy, col_len(p->b2.h));
+    if (deg == 3) p->ncy3 = std::min(p->ncy, col_len(p->b3.h));
+  }
+  p->lncy2 = col_log2(p->ncy2);
+  p->lncy3 = col_log2(p->ncy3);
   p->lnx = ilog2(d.nx);
   p->lny = ilog2(d.ny);
   const int max_banks = o3 ? 21 : (p->want_psi22 ? 16 : 8);
@@ -884,9 +920,9 @@ extern "C" gl_status gl_plan_create(gl_plan** out, const gl_plan_desc* desc) {
   geo_alloc(&p->geo1, p->b1);
   geo_alloc(&p->geo2, p->b2);
   geo_alloc(&p->geo3, p->b3);
-  if (e == cudaSuccess) e = cudaMalloc(&p->tw, sizeof(cplx) * TW_N);
+  if (e == cudaSuccess) e = cudaMalloc(&p->tw, sizeof(cplx) * TW_ALLOC);
   if (e == cudaSuccess) {
-    twiddle_kernel<<<TW_N / 256, 256>>>(p->tw);
+    twiddle_kernel<<<TW_ALLOC / 256 + 1, 256>>>(p->tw, TW_ALLOC);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMalloc(&p->nodes, sizeof(double) * 8 * MAX_RANK);
@@ -944,6 +980,8 @@ extern "C" gl_status gl_plan_get_info(const gl_plan* p, gl_plan_info* info) {
   std::memset(info, 0, sizeof *info);
   info->ncx = p->ncx;
   info->ncy = p->ncy;
+  info->ncy_pair = p->e44 ? p->ncy : p->ncy2;
+  info->ncy_triple = p->e44 ? p->ncy : p->ncy3;
   const Box* bs[3] = {&p->b1, &p->b2, &p->b3};
   int* dst[3] = {info->box1, info->box2, info->box3};
   for (int k = 0; k < 3; ++k) {
@@ -990,24 +1028,56 @@ static int grid_for(size_t n, int threads, int cap = 4096) {
 }
 
 static int fft_cols_per_block(int n, int w) {
-  const int T = n / 16;
+  const int T = is_pow2(n) ? n / 16 : 16;  // threads per column transform
   return std::max(1, std::min(256 / T, w));
 }
 
-static gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
-  const int cw = fft_cols_per_block(a.n, a.box.w);
-  const size_t smem = ((size_t)cw * padded_len(a.n) + (size_t)cw * a.box.h) * sizeof(cplx);
+// Column kernels are instantiated per mixed radix (MIX = n/16 for the mixed
+// lengths, 0 for powers of two).
+template <int MIX>
+static void col_ifft_launch(dim3 grid, size_t smem, cudaStream_t st, const ColArgs& a, const cplx* tw,
+                            int cw, int bpb) {
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(col_ifft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    cudaFuncSetAttribute(col_ifft_kernel<MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
     attr = true;
   }
+  col_ifft_kernel<MIX><<<grid, 256, smem, st>>>(a, tw, cw, bpb);
+}
+
+template <int MIX>
+static void col_fft_launch(dim3 grid, size_t smem, cudaStream_t st, const ColFftArgs& a, const cplx* tw,
+                           int cw) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(col_fft_kernel<MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    attr = true;
+  }
+  col_fft_kernel<MIX><<<grid, 256, smem, st>>>(a, tw, cw);
+}
+
+#define GL_MIX_DISPATCH(n, launcher, ...)                                   \
+  switch (mixed_len(n) ? (n) / 16 : 0) {                                   \
+    case 3: launcher<3>(__VA_ARGS__); break;                               \
+    case 5: launcher<5>(__VA_ARGS__); break;                               \
+    case 6: launcher<6>(__VA_ARGS__); break;                               \
+    case 9: launcher<9>(__VA_ARGS__); break;                               \
+    case 10: launcher<10>(__VA_ARGS__); break;                             \
+    case 12: launcher<12>(__VA_ARGS__); break;                             \
+    case 15: launcher<15>(__VA_ARGS__); break;                             \
+    default: launcher<0>(__VA_ARGS__); break;                              \
+  }
+
+static gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
+  if (!is_pow2(a.n) && !mixed_len(a.n)) return fail(GL_ERR_UNSUPPORTED, "column length %d has no transform", a.n);
+  const int cw = fft_cols_per_block(a.n, a.box.w);
+  const size_t smem = ((size_t)cw * padded_len(a.n) + (size_t)cw * a.box.h) * sizeof(cplx);
   const int bpb = std::min(a.nbanks, 4);  // banks per block: grid.z spreads the rest
   dim3 grid((a.box.w + cw - 1) / cw, njobs, (a.nbanks + bpb - 1) / bpb);
   const double bytes = (double)njobs * a.nbanks * a.box.w * a.n * sizeof(cplx) +
                        (double)njobs * a.box.w * a.box.h * sizeof(cplx);
   LaunchScope ls("col_ifft_kernel", st, bytes);
-  col_ifft_kernel<<<grid, 256, smem, st>>>(a, tw, cw, bpb);
+  GL_MIX_DISPATCH(a.n, col_ifft_launch, grid, smem, st, a, tw, cw, bpb);
   LAUNCH_CHECK("col_ifft_kernel");
   return GL_OK;
 }
@@ -1064,17 +1134,13 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
 }
 
 static gl_status launch_col_fft(const ColFftArgs& a, int njs, cudaStream_t st, const cplx* tw) {
+  if (!is_pow2(a.n) && !mixed_len(a.n)) return fail(GL_ERR_UNSUPPORTED, "column length %d has no transform", a.n);
   const int cw = fft_cols_per_block(a.n, a.box.w);
   const size_t smem = (size_t)cw * padded_len(a.n) * sizeof(cplx);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(col_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    attr = true;
-  }
   dim3 grid((a.box.w + cw - 1) / cw, njs);
   const double bytes = (double)njs * a.box.w * (a.n + a.box.h) * sizeof(cplx);
   LaunchScope ls("col_fft_kernel", st, bytes);
-  col_fft_kernel<<<grid, 256, smem, st>>>(a, tw, cw);
+  GL_MIX_DISPATCH(a.n, col_fft_launch, grid, smem, st, a, tw, cw);
   LAUNCH_CHECK("col_fft_kernel");
   return GL_OK;
 }
@@ -1345,17 +1411,19 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
   gl_status s;
   const cplx* spec = nullptr;
   if ((s = analyse_group(p, gu, spectra, layout, ws, st, &spec)) != GL_OK) return s;
-  const double fwd_scale = ((double)p->d.nx * (double)p->d.ny) / ((double)p->ncx * (double)p->ncy);
   const double inv_scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
-  const int ncy = p->ncy;
+  const double nn = (double)p->d.nx * (double)p->d.ny;
+  const int ncy2 = p->ncy2, ncy3 = p->ncy3;
+  const double fwd_scale2 = nn / ((double)p->ncx * (double)ncy2);
+  const double fwd_scale3 = nn / ((double)p->ncx * (double)ncy3);
 
   // ---------------- eta22 (spatial.py:156-231) ----------------
   if (p->want_eta22) {
     const int J = p->ranks[0];
     const int njobs = gu * J;
     Bump b;
-    cplx* P = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs * 8 * B1.w * ncy * sizeof(cplx)));
-    cplx* Q = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs * 2 * B2.w * ncy * sizeof(cplx)));
+    cplx* P = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs * 8 * B1.w * ncy2 * sizeof(cplx)));
+    cplx* Q = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs * 2 * B2.w * ncy2 * sizeof(cplx)));
     cplx* R = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs * 2 * pl2 * sizeof(cplx)));
     unsigned long long* mx = reinterpret_cast<unsigned long long*>(scratch + b.take((size_t)njobs * 2 * 8));
     CUDA_TRY(cudaMemsetAsync(mx, 0, (size_t)njobs * 2 * 8, st));
@@ -1373,8 +1441,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     a.us = us;
     a.nodes = dn + 0 * MAX_RANK;
     a.out = P;
-    a.n = ncy;
-    a.log2n = p->lncy;
+    a.n = ncy2;
+    a.log2n = p->lncy2;
     a.scale = inv_scale;
     if ((s = launch_col_ifft(a, njobs, st, p->tw)) != GL_OK) return s;
     RowArgs r;
@@ -1388,7 +1456,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     r.out = Q;
     r.nx = p->ncx;
     r.log2nx = p->lncx;
-    r.ny = ncy;
+    r.ny = ncy2;
     r.us = us;
     r.jobs_per_unit = J;
     r.gmax = ROW_GMAX;
@@ -1397,13 +1465,13 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     f.in = Q;
     f.out = R;
     f.box = B2;
-    f.n = ncy;
-    f.log2n = p->lncy;
+    f.n = ncy2;
+    f.log2n = p->lncy2;
     f.nsrc = 2;
     f.jobs_per_unit = J;
     f.mask = s2;
     f.maxslot = mx;
-    f.scale = fwd_scale;
+    f.scale = fwd_scale2;
     if ((s = launch_col_fft(f, njobs * 2, st, p->tw)) != GL_OK) return s;
     AccArgs c;
     std::memset(&c, 0, sizeof c);
@@ -1430,11 +1498,11 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     const int njobs_c = gu * 2 * 2 * 2;  // (unit, branch, node, channel)
     const int njobs_r = gu * 2 * 2;      // (unit, branch, node)
     Bump b;
-    cplx* P = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs_c * 8 * B1.w * ncy * sizeof(cplx)));
-    cplx* Q = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs_r * 8 * B2.w * ncy * sizeof(cplx)));
+    cplx* P = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs_c * 8 * B1.w * ncy2 * sizeof(cplx)));
+    cplx* Q = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs_r * 8 * B2.w * ncy2 * sizeof(cplx)));
     cplx* R = reinterpret_cast<cplx*>(scratch + b.take((size_t)njobs_r * 8 * pl2 * sizeof(cplx)));
-    cplx* Pc = reinterpret_cast<cplx*>(scratch + b.take((size_t)gu * 2 * B1.w * ncy * sizeof(cplx)));
-    cplx* Qc = reinterpret_cast<cplx*>(scratch + b.take((size_t)gu * 1 * B2.w * ncy * sizeof(cplx)));
+    cplx* Pc = reinterpret_cast<cplx*>(scratch + b.take((size_t)gu * 2 * B1.w * ncy2 * sizeof(cplx)));
+    cplx* Qc = reinterpret_cast<cplx*>(scratch + b.take((size_t)gu * 1 * B2.w * ncy2 * sizeof(cplx)));
     cplx* Rc = reinterpret_cast<cplx*>(scratch + b.take((size_t)gu * pl2 * sizeof(cplx)));
     ColArgs a;
     std::memset(&a, 0, sizeof a);
@@ -1452,8 +1520,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     a.n_inner = 2;
     a.chan_mask = ch;
     a.out = P;
-    a.n = ncy;
-    a.log2n = p->lncy;
+    a.n = ncy2;
+    a.log2n = p->lncy2;
     a.scale = inv_scale;
     if ((s = launch_col_ifft(a, njobs_c, st, p->tw)) != GL_OK) return s;
     RowArgs r;
@@ -1469,7 +1537,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     r.out = Q;
     r.nx = p->ncx;
     r.log2nx = p->lncx;
-    r.ny = ncy;
+    r.ny = ncy2;
     r.us = us;
     r.jobs_per_unit = 4;
     r.gmax = ROW_GMAX;
@@ -1478,13 +1546,13 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     f.in = Q;
     f.out = R;
     f.box = B2;
-    f.n = ncy;
-    f.log2n = p->lncy;
+    f.n = ncy2;
+    f.log2n = p->lncy2;
     f.nsrc = 8;
     f.jobs_per_unit = 4;
     f.mask = nullptr;
     f.maxslot = nullptr;
-    f.scale = fwd_scale;
+    f.scale = fwd_scale2;
     if ((s = launch_col_fft(f, njobs_r * 8, st, p->tw)) != GL_OK) return s;
     // Taylor contact 0.5 eta11 phi1z
     ColArgs cc;
@@ -1501,8 +1569,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     cc.spec_job_stride = pl1;
     cc.jobs_per_unit = 1;
     cc.out = Pc;
-    cc.n = ncy;
-    cc.log2n = p->lncy;
+    cc.n = ncy2;
+    cc.log2n = p->lncy2;
     cc.scale = inv_scale;
     if ((s = launch_col_ifft(cc, gu, st, p->tw)) != GL_OK) return s;
     RowArgs rc;
@@ -1516,7 +1584,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     rc.out = Qc;
     rc.nx = p->ncx;
     rc.log2nx = p->lncx;
-    rc.ny = ncy;
+    rc.ny = ncy2;
     rc.us = us;
     rc.jobs_per_unit = 1;
     rc.gmax = ROW_GMAX;
@@ -1562,8 +1630,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     CUDA_TRY(cudaMemsetAsync(mxs, 0, (size_t)nuj * 8 * 8, st));
     // inner stage buffers
     Bump bi = b;
-    cplx* PI = reinterpret_cast<cplx*>(scratch + bi.take((size_t)njobs * 12 * B1.w * ncy * sizeof(cplx)));
-    cplx* QI = reinterpret_cast<cplx*>(scratch + bi.take((size_t)njobs * 4 * B2.w * ncy * sizeof(cplx)));
+    cplx* PI = reinterpret_cast<cplx*>(scratch + bi.take((size_t)njobs * 12 * B1.w * ncy2 * sizeof(cplx)));
+    cplx* QI = reinterpret_cast<cplx*>(scratch + bi.take((size_t)njobs * 4 * B2.w * ncy2 * sizeof(cplx)));
     cplx* RI = reinterpret_cast<cplx*>(scratch + bi.take((size_t)njobs * 4 * pl2 * sizeof(cplx)));
     unsigned long long* maxRI = reinterpret_cast<unsigned long long*>(scratch + bi.take((size_t)njobs * 4 * 8));
     CUDA_TRY(cudaMemsetAsync(maxRI, 0, (size_t)njobs * 4 * 8, st));
@@ -1586,8 +1654,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       a.n_inner = I;
       a.n_outer = J;
       a.out = PI;
-      a.n = ncy;
-      a.log2n = p->lncy;
+      a.n = ncy2;
+      a.log2n = p->lncy2;
       a.scale = inv_scale;
       if ((s = launch_col_ifft(a, njobs, st, p->tw)) != GL_OK) return s;
       RowArgs r;
@@ -1601,7 +1669,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       r.out = QI;
       r.nx = p->ncx;
       r.log2nx = p->lncx;
-      r.ny = ncy;
+      r.ny = ncy2;
       r.us = us;
       r.jobs_per_unit = J * I;
       r.gmax = ROW_GMAX;
@@ -1610,13 +1678,13 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       f.in = QI;
       f.out = RI;
       f.box = B2;
-      f.n = ncy;
-      f.log2n = p->lncy;
+      f.n = ncy2;
+      f.log2n = p->lncy2;
       f.nsrc = 4;
       f.jobs_per_unit = J * I;
       f.mask = s2;
       f.maxslot = maxRI;
-      f.scale = fwd_scale;
+      f.scale = fwd_scale2;
       if ((s = launch_col_fft(f, njobs * 4, st, p->tw)) != GL_OK) return s;
       AccArgs c;
       std::memset(&c, 0, sizeof c);
@@ -1642,9 +1710,9 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     }
     // outer stage buffers (reuse the inner region)
     Bump bo = b;
-    cplx* P1 = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 12 * B1.w * ncy * sizeof(cplx)));
-    cplx* P2 = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 9 * B2.w * ncy * sizeof(cplx)));
-    cplx* QO = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 4 * B3.w * ncy * sizeof(cplx)));
+    cplx* P1 = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 12 * B1.w * ncy3 * sizeof(cplx)));
+    cplx* P2 = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 9 * B2.w * ncy3 * sizeof(cplx)));
+    cplx* QO = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 4 * B3.w * ncy3 * sizeof(cplx)));
     cplx* RO = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 4 * pl3 * sizeof(cplx)));
     cplx* FO = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 2 * pl3 * sizeof(cplx)));
     {
@@ -1663,8 +1731,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       a.us = us;
       a.nodes = dn + 3 * MAX_RANK;
       a.out = P1;
-      a.n = ncy;
-      a.log2n = p->lncy;
+      a.n = ncy3;
+      a.log2n = p->lncy3;
       a.scale = inv_scale;
       if ((s = launch_col_ifft(a, nuj, st, p->tw)) != GL_OK) return s;
       ColArgs a2;
@@ -1687,8 +1755,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       a2.floor_max = maxEt;
       a2.floor_rel = p->floor_rel;
       a2.out = P2;
-      a2.n = ncy;
-      a2.log2n = p->lncy;
+      a2.n = ncy3;
+      a2.log2n = p->lncy3;
       a2.scale = inv_scale;
       if ((s = launch_col_ifft(a2, nuj, st, p->tw)) != GL_OK) return s;
       RowArgs r;
@@ -1703,7 +1771,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       r.out = QO;
       r.nx = p->ncx;
       r.log2nx = p->lncx;
-      r.ny = ncy;
+      r.ny = ncy3;
       r.us = us;
       r.jobs_per_unit = J;
       r.gmax = ROW_GMAX;
@@ -1712,13 +1780,13 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       f.in = QO;
       f.out = RO;
       f.box = B3;
-      f.n = ncy;
-      f.log2n = p->lncy;
+      f.n = ncy3;
+      f.log2n = p->lncy3;
       f.nsrc = 4;
       f.jobs_per_unit = J;
       f.mask = s3;
       f.maxslot = maxRO;
-      f.scale = fwd_scale;
+      f.scale = fwd_scale3;
       if ((s = launch_col_fft(f, nuj * 4, st, p->tw)) != GL_OK) return s;
       AccArgs c;
       std::memset(&c, 0, sizeof c);
@@ -1973,9 +2041,9 @@ extern "C" gl_status gl_eta44_plan_create(gl_plan** out, const gl_eta44_desc* de
   geo_alloc(&p->geo2, p->b2);
   geo_alloc(&p->geo3, p->b3);
   geo_alloc(&p->geo4, p->b4);
-  if (err == cudaSuccess) err = cudaMalloc(&p->tw, sizeof(cplx) * TW_N);
+  if (err == cudaSuccess) err = cudaMalloc(&p->tw, sizeof(cplx) * TW_ALLOC);
   if (err == cudaSuccess) {
-    twiddle_kernel<<<TW_N / 256, 256>>>(p->tw);
+    twiddle_kernel<<<TW_ALLOC / 256 + 1, 256>>>(p->tw, TW_ALLOC);
     err = cudaGetLastError();
   }
   if (err == cudaSuccess) err = cudaMalloc(&p->nodes, sizeof(double) * 2 * MAX_RANK);
@@ -3350,7 +3418,7 @@ static gl_status device_twiddles(cplx** out) {
   if (!g_tw_global[dev]) {
     cplx* tw = nullptr;
     CUDA_TRY(cudaMalloc(&tw, sizeof(cplx) * TW_N));
-    twiddle_kernel<<<TW_N / 256, 256>>>(tw);
+    twiddle_kernel<<<TW_N / 256, 256>>>(tw, TW_N);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaDeviceSynchronize());
     g_tw_global[dev] = tw;
@@ -3848,7 +3916,7 @@ static gl_status noalloc_scratch(cudaStream_t st, unsigned char** out) {
     if (e != cudaSuccess || !ptr)
       return fail(GL_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch failed: %s",
                   cudaGetErrorString(e));
-    twiddle_kernel<<<TW_N / 256, 256, 0, st>>>(reinterpret_cast<cplx*>(ptr));
+    twiddle_kernel<<<TW_N / 256, 256, 0, st>>>(reinterpret_cast<cplx*>(ptr), TW_N);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(st));
     g_noalloc_base[dev] = reinterpret_cast<unsigned char*>(ptr);

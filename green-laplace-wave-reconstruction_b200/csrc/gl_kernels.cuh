@@ -262,6 +262,7 @@ GL_D cplx col_base(const ColArgs& a, int job, int i, double nu) {
 // spectrum of the columns is computed once and every bank applies its
 // multiplier while the first FFT pass reads it.  Output layout
 // [job][bank][y][column] (rows contiguous for the row kernel).
+template <int MIX>
 __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx* __restrict__ tw,
                                                          int cw, int banks_per_block) {
   extern __shared__ cplx smem[];
@@ -301,7 +302,7 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
       const bool active = c < ncol;
       cplx* buf = bufs + (size_t)(active ? c : 0) * L;
       auto load = [&](int yb) -> cplx {
-        const int by = wrap(yb - a.box.y0, n);
+        const int by = wrap_any(yb - a.box.y0, n);
         if (by >= h) return czero();
         const int i = by * a.box.w + x_first + c;
         cplx v;
@@ -315,7 +316,7 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
         return a.conj_io ? cconj(mv) : mv;
       };
       auto store = [&](int yb, cplx v) { buf[phys(yb)] = v; };
-      fft_row<+1>(buf, f, active, tw, load, store);
+      fft_row<+1, MIX>(buf, f, active, tw, load, store);
     }
     __syncthreads();
     cplx* dst = a.out + ((size_t)job * a.nbanks + k) * n * a.box.w + x_first;
@@ -832,6 +833,7 @@ struct ColFftArgs {
 // input ([js][y][col]) are staged with coalesced loads, each column is one
 // forward transform along y, and only the output box's rows are written
 // (support-masked), with the spectrum's max |.| folded into maxslot.
+template <int MIX>
 __global__ void __launch_bounds__(256, 2) col_fft_kernel(ColFftArgs a, const cplx* __restrict__ tw, int cw) {
   extern __shared__ cplx smem[];
   const int js = blockIdx.y;
@@ -857,7 +859,7 @@ __global__ void __launch_bounds__(256, 2) col_fft_kernel(ColFftArgs a, const cpl
     cplx* buf = bufs + (size_t)(active ? c : 0) * L;
     auto load = [&](int yb) -> cplx { return buf[phys(yb)]; };
     auto store = [&](int yb, cplx v) { buf[phys(yb)] = v; };
-    fft_row<-1>(buf, f, active, tw, load, store);
+    fft_row<-1, MIX>(buf, f, active, tw, load, store);
   }
   __syncthreads();
   const unsigned char* mask = a.mask ? a.mask + (size_t)unit * a.box.w * a.box.h : nullptr;
@@ -866,7 +868,7 @@ __global__ void __launch_bounds__(256, 2) col_fft_kernel(ColFftArgs a, const cpl
   for (int t = threadIdx.x; t < ncol * a.box.h; t += blockDim.x) {
     const int c = t % ncol, by = t / ncol;
     const int i = by * a.box.w + x_first + c;
-    const cplx raw = bufs[(size_t)c * L + phys(wrap(a.box.y0 + by, n))];
+    const cplx raw = bufs[(size_t)c * L + phys(wrap_any(a.box.y0 + by, n))];
     cplx v = cscale(a.scale, a.conj_io ? cconj(raw) : raw);
     if (mask && !mask[i]) v = czero();
     dst[i] = v;

@@ -102,6 +102,8 @@ typedef struct gl_plan_info {
   int n_components;           /* output planes per unit                     */
   int component_ids[6];       /* GL_COMP_* of each plane, in order          */
   double transforms_per_unit; /* 2-D transforms of the reference graph      */
+  int ncy_pair, ncy_triple;   /* column lengths of the pair and triple stages
+                                 (ncy or a mixed length 16 m <= ncy)         */
 } gl_plan_info;
 
 /* Create a plan: validates the descriptor, picks the product grid, builds

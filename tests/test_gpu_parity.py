@@ -128,6 +128,61 @@ def test_seeded_states_match_oracle(seed, n, modes, order):
         assert err < 1e-9, name
 
 
+def _box_state(order, h, n, seed, w=4, depth=30.0):
+    """Modes on the lattice of an n x n, 256 m domain whose parent box is w
+    columns (mx = 2 .. w+1) by h rows (my spans h consecutive values centred
+    on 0), so the pair and triple boxes have heights 2h-1 and 3h-2."""
+    rng = np.random.default_rng(seed)
+    lx = 256.0
+    lo = -((h - 1) // 2)
+    cells = {(2, lo), (w + 1, lo + h - 1)}          # the box corners
+    while len(cells) < 12:
+        cells.add((int(rng.integers(2, w + 2)), int(rng.integers(lo, lo + h))))
+    m = np.array(sorted(cells), dtype=float)
+    dk = 2 * np.pi / lx
+    amp = 0.04 / np.sqrt(len(m))
+    return dict(order=order, gravity=9.81, depth=depth, a=amp * rng.standard_normal(len(m)),
+                b=amp * rng.standard_normal(len(m)), kx=dk * m[:, 0], ky=dk * m[:, 1], lx=lx,
+                ly=lx, n=n)
+
+
+# (order, parent box height, grid, expected pair / triple column lengths):
+# every mixed length 16 m the column kernels run, as a pair grid and as a
+# triple grid, next to the power-of-two lengths they replace.
+MIXED_CASES = [
+    (2, 20, 64, 48, None), (2, 36, 128, 80, None), (2, 44, 128, 96, None),
+    (2, 69, 256, 144, None), (2, 76, 256, 160, None), (2, 90, 256, 192, None),
+    (2, 110, 256, 240, None),
+    (3, 14, 128, 32, 48), (3, 25, 256, 64, 80), (3, 30, 256, 64, 96),
+    (3, 46, 256, 96, 144), (3, 52, 512, 128, 160), (3, 60, 512, 128, 192),
+    (3, 69, 256, 144, 240),
+]
+
+
+@pytest.mark.parametrize("order,h,n,pair,triple", MIXED_CASES)
+def test_mixed_column_grids_match_oracle(order, h, n, pair, triple):
+    """Pair/triple stages on column grids of length 16 m (m = 3, 5, 6, 9,
+    10, 12, 15) reproduce the oracle on the reference grid like the
+    power-of-two grids do (alias-free products have the same coefficients on
+    any period covering the box)."""
+    st = _box_state(order, h, n, seed=h)
+    t = 0.3
+    c = gl_engine.gl_spectral_coefficients(order, st["gravity"], st["depth"], st["a"], st["b"],
+                                           st["kx"], st["ky"], 0, 0, {"eta22_rank": 4})
+    _, _, _, _, comps, audit = gl_engine.gl_spectral_surface(c, st["lx"], st["ly"], n, n, t)
+    grids = audit["engine"]["column_grids"]
+    assert grids["pair"] == pair
+    if triple is not None:
+        assert grids["triple"] == triple
+    oc = O.spectral_coefficients(order, st["gravity"], st["depth"], st["a"], st["b"], st["kx"],
+                                 st["ky"], options={"eta22_rank": 4})
+    ref = O.spectral_surface(oc, st["lx"], st["ly"], n, n, t)
+    for name in COMPS[2: 2 * order]:
+        err = rel(comps[name + "_plus"], ref[name + "_plus"])
+        print(f"order {order} h {h} ({pair}/{triple}) {name}: {err:.3e}")
+        assert err < 1e-9, name
+
+
 def test_compact_and_reference_grids_agree():
     st = seastate.small_order3(seed=7, n=64, modes=12)
     c = gl_engine.gl_spectral_coefficients(3, st.gravity, st.depth, st.a, st.b, st.kx, st.ky,
