@@ -1072,7 +1072,9 @@ static gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, c
   if (!is_pow2(a.n) && !mixed_len(a.n)) return fail(GL_ERR_UNSUPPORTED, "column length %d has no transform", a.n);
   const int cw = fft_cols_per_block(a.n, a.box.w);
   const size_t smem = ((size_t)cw * padded_len(a.n) + (size_t)cw * a.box.h) * sizeof(cplx);
-  const int bpb = std::min(a.nbanks, 4);  // banks per block: grid.z spreads the rest
+  // banks per block: at most 4, spread evenly over grid.z (9 banks: 3 x 3)
+  const int nz = (a.nbanks + 3) / 4;
+  const int bpb = (a.nbanks + nz - 1) / nz;
   dim3 grid((a.box.w + cw - 1) / cw, njobs, (a.nbanks + bpb - 1) / bpb);
   const double bytes = (double)njobs * a.nbanks * a.box.w * a.n * sizeof(cplx) +
                        (double)njobs * a.box.w * a.box.h * sizeof(cplx);

@@ -289,6 +289,11 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
   int g, G;
   const FftGroup f = fft_group(n, a.log2n, g, G);
   const int iters = (ncol + G - 1) / G;
+  // with at least two columns per warp the last pass writes the columns
+  // straight to global memory (two adjacent columns fill each 32-byte
+  // sector) and the banks need no block-wide barrier; longer columns (one
+  // column per warp or more) are written back row-major through shared memory
+  const bool direct = f.T <= 16;
   for (int k = k_first; k < k_last; ++k) {
     const int mult = a.mult[k];
     const cplx* sk = a.spec + (long long)job * a.spec_job_stride + (long long)a.src_of[k] * a.spec_sub_stride;
@@ -297,10 +302,12 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
         !floor_it ? 0.0
                   : a.floor_rel * as_double(a.kind == COL_FLOORED ? a.floor_max[(size_t)job * a.floor_nsrc + a.src_of[k]]
                                                                   : a.floor_max[job]);
+    cplx* dst = a.out + ((size_t)job * a.nbanks + k) * n * a.box.w + x_first;
     for (int it = 0; it < iters; ++it) {
       const int c = it * G + g;
       const bool active = c < ncol;
       cplx* buf = bufs + (size_t)(active ? c : 0) * L;
+      cplx* dcol = dst + (active ? c : 0);
       auto load = [&](int yb) -> cplx {
         const int by = wrap_any(yb - a.box.y0, n);
         if (by >= h) return czero();
@@ -315,17 +322,23 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
         const cplx mv = apply_mult(mult, GeoRef{a.geo, plane, i}, v);
         return a.conj_io ? cconj(mv) : mv;
       };
-      auto store = [&](int yb, cplx v) { buf[phys(yb)] = v; };
+      auto store = [&](int yb, cplx v) {
+        if (direct)
+          dcol[(size_t)yb * a.box.w] = cscale(a.scale, a.conj_io ? cconj(v) : v);
+        else
+          buf[phys(yb)] = v;
+      };
       fft_row<+1, MIX>(buf, f, active, tw, load, store);
     }
-    __syncthreads();
-    cplx* dst = a.out + ((size_t)job * a.nbanks + k) * n * a.box.w + x_first;
-    for (int t = threadIdx.x; t < n * ncol; t += blockDim.x) {
-      const int y = t / ncol, c = t % ncol;
-      const cplx v = bufs[(size_t)c * L + phys(y)];
-      dst[(size_t)y * a.box.w + c] = cscale(a.scale, a.conj_io ? cconj(v) : v);
+    if (!direct) {
+      __syncthreads();
+      for (int t = threadIdx.x; t < n * ncol; t += blockDim.x) {
+        const int y = t / ncol, c = t % ncol;
+        const cplx v = bufs[(size_t)c * L + phys(y)];
+        dst[(size_t)y * a.box.w + c] = cscale(a.scale, a.conj_io ? cconj(v) : v);
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
 }
 
@@ -845,10 +858,21 @@ __global__ void __launch_bounds__(256, 2) col_fft_kernel(ColFftArgs a, const cpl
   const int L = padded_len(n);
   cplx* bufs = smem;  // cw * L
   const cplx* src = a.in + (size_t)js * n * a.box.w + x_first;
-  for (int t = threadIdx.x; t < n * ncol; t += blockDim.x) {
-    const int y = t / ncol, c = t % ncol;
-    const cplx v = src[(size_t)y * a.box.w + c];
-    bufs[(size_t)c * L + phys(y)] = a.conj_io ? cconj(v) : v;
+  // stage the kept columns ([y][col] rows in global memory) with eight
+  // independent loads in flight per thread
+  const int total = n * ncol;
+  for (int t0 = threadIdx.x; t0 < total; t0 += 8 * blockDim.x) {
+    cplx v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < total) v[u] = src[(size_t)(t / ncol) * a.box.w + t % ncol];
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < total) bufs[(size_t)(t % ncol) * L + phys(t / ncol)] = a.conj_io ? cconj(v[u]) : v[u];
+    }
   }
   __syncthreads();
   int g, G;
