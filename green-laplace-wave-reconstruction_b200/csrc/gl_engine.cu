@@ -719,6 +719,8 @@ struct Bump {
 
 static const int ROW_GMAX = 4;
 static const size_t SMEM_LIMIT = 227 * 1024;
+// row kernels also hold a static mbarrier: their dynamic budget leaves 1 KB
+static const size_t ROW_SMEM_LIMIT = SMEM_LIMIT - 1024;
 
 static size_t row_smem(int nbanks, int ncx) {
   return (size_t)nbanks * padded_len(ncx) * sizeof(cplx);
@@ -876,7 +878,7 @@ extern "C" gl_status gl_plan_create(gl_plan** out, const gl_plan_desc* desc) {
   p->lnx = ilog2(d.nx);
   p->lny = ilog2(d.ny);
   const int max_banks = o3 ? 21 : (p->want_psi22 ? 16 : 8);
-  if (deg > 1 && row_smem(max_banks, p->ncx) > SMEM_LIMIT) {
+  if (deg > 1 && row_smem(max_banks, p->ncx) > ROW_SMEM_LIMIT) {
     plan_free(p);
     return fail(GL_ERR_UNSUPPORTED,
                 "product grid %d x %d exceeds the shared-memory row budget (use the compact grid)",
@@ -1088,9 +1090,9 @@ template <int K>
 static void row_launch(dim3 grid, int threads, size_t smem, cudaStream_t st, const RowArgs& a,
                        const cplx* tw) {
   static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(row_kernel_t<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    attr = true;
+  if (!attr) {  // a failure here surfaces as the launch's own error
+    attr = cudaFuncSetAttribute(row_kernel_t<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)ROW_SMEM_LIMIT) == cudaSuccess;
   }
   row_kernel_t<K><<<grid, threads, smem, st>>>(a, tw);
 }
@@ -1100,6 +1102,8 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
   for (int g = 0; g < a.ngrp; ++g) nb += a.grp[g].nb;
   const bool e44 = a.kind >= ROW_E44_PAIR && a.kind <= ROW_E44_ORDER4_PSI;
   const size_t smem = row_smem(nb, a.nx);
+  if (smem > ROW_SMEM_LIMIT)
+    return fail(GL_ERR_UNSUPPORTED, "row stage of %d banks x %d exceeds the shared-memory budget", nb, a.nx);
   dim3 grid(a.ny, njobs);
   // 8 transform groups per block (n/16 threads each) when the row has at
   // most 12 banks (4 blocks fit per SM by shared memory), 16 for the wider
@@ -2008,7 +2012,7 @@ extern "C" gl_status gl_eta44_plan_create(gl_plan** out, const gl_eta44_desc* de
   p->lncy = ilog2(p->ncy);
   p->lnx = p->lny = ilog2(e.n);
   const int row_banks = want_psi ? 46 : 45;
-  if (row_smem(row_banks, p->ncx) > SMEM_LIMIT) {
+  if (row_smem(row_banks, p->ncx) > ROW_SMEM_LIMIT) {
     plan_free(p);
     return fail(GL_ERR_UNSUPPORTED,
                 "eta44 product grid width %d exceeds the shared-memory row budget (%d banks)", p->ncx,
@@ -2713,7 +2717,7 @@ static gl_status adj_check_plan(const gl_plan* p) {
   if (p->e44) return fail(GL_ERR_UNSUPPORTED, "the adjoint covers the eta11/eta22/eta33 graph only");
   if (!(p->comps & (GL_COMP_ETA11 | GL_COMP_ETA22 | GL_COMP_ETA33)))
     return fail(GL_ERR_INVALID_ARGUMENT, "the plan has no eta component to differentiate");
-  if (adj_eta33(p) && row_smem(23, p->ncx) > SMEM_LIMIT)
+  if (adj_eta33(p) && row_smem(23, p->ncx) > ROW_SMEM_LIMIT)
     return fail(GL_ERR_UNSUPPORTED, "the order-3 adjoint row exceeds the shared-memory budget at %d columns",
                 p->ncx);
   return GL_OK;

@@ -19,6 +19,7 @@
 //   out_row_kernel   final inverse FFT along x on the reference grid.
 #pragma once
 #include "gl_analysis.cuh"
+#include "gl_async.cuh"
 #include "gl_fft.cuh"
 #include "gl_fftreg.cuh"
 
@@ -367,7 +368,7 @@ struct RowArgs {
   cplx* out;               // [job][nout][out_w][n_y]
   int nx, log2nx;          // compact grid along x
   int ny;                  // compact grid along y (column length of inputs)
-  const UnitScalars* us;
+  UnitScalars* us;         // per-unit scalars; status word flagged on a timed-out copy
   int jobs_per_unit;
   int gmax;                // FFT group size (rows through tmp)
   // adjoint extensions (zero in the forward stages):
@@ -727,7 +728,8 @@ GL_D void row_products_adj(int kind, cplx* b, int L, int p) {
 template <int KIND>
 __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __restrict__ tw) {
   constexpr int FAMILY = KIND >= ROW_ADJ_ETA22 ? 1 : (KIND >= ROW_E44_PAIR && KIND <= ROW_E44_ORDER4_PSI ? 2 : 0);
-  extern __shared__ cplx smem[];
+  extern __shared__ __align__(128) cplx smem[];
+  __shared__ __align__(8) unsigned long long stage_bar;
   const int y = blockIdx.x;
   const int job = blockIdx.y;
   const int n = a.nx;
@@ -735,25 +737,37 @@ __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __
   int nb = 0;
   for (int q = 0; q < a.ngrp; ++q) nb += a.grp[q].nb;
   cplx* banks = smem;  // nb * L
-  constexpr bool PREFETCH = FAMILY == 2;
-  if constexpr (PREFETCH) {
-    // wide rows (the order-4 stages, > 24 banks): gather every bank's box
-    // columns first with coalesced loads, all in flight at once, since the
-    // transform loop takes several rounds of groups
-    for (int t = threadIdx.x; t < nb * L; t += blockDim.x) banks[t] = czero();
-    __syncthreads();
+  // Stage every bank's box row (w contiguous values) into the front of the
+  // bank's own row buffer with bulk async copies, all issued at block start,
+  // so the later transform rounds find their inputs in shared memory.  The
+  // first pass of a bank's transform reads its staged values into registers
+  // before the group writes the padded row over them.
+  const uint32_t bar = smem_u32(&stage_bar);
+  if (threadIdx.x == 0) mbar_init(bar, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t bytes = 0;
+    for (int q = 0; q < a.ngrp; ++q) bytes += (uint32_t)(a.grp[q].nb * a.grp[q].w * sizeof(cplx));
+    mbar_arrive_expect_tx(bar, bytes);
     int k0 = 0;
     for (int q = 0; q < a.ngrp; ++q) {
-      const BankGroup B = a.grp[q];
-      const int cnt = B.nb * B.w;
-      const cplx* src = B.data + ((size_t)job * B.nb * a.ny + y) * B.w;
-      for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
-        const int kk = t / B.w, xi = t % B.w;
-        banks[(size_t)(k0 + kk) * L + phys(wrap(B.x0 + xi, n))] = src[(size_t)kk * a.ny * B.w + xi];
-      }
+      const BankGroup& B = a.grp[q];
+      for (int kk = 0; kk < B.nb; ++kk)
+        bulk_g2s(smem_u32(banks + (size_t)(k0 + kk) * L), B.data + (((size_t)job * B.nb + kk) * a.ny + y) * B.w,
+                 (uint32_t)(B.w * sizeof(cplx)), bar);
       k0 += B.nb;
     }
-    __syncthreads();
+  }
+  {
+    bool late = !mbar_wait_bounded(bar, 0, BULK_WAIT_CYCLES);
+    if (__syncthreads_or(late)) {
+      // a copy never landed: flag the unit, give the copies one more bounded
+      // wait so none is left writing this block's shared memory, and leave
+      if (threadIdx.x == 0 && a.us && a.jobs_per_unit > 0)
+        atomicCAS(&a.us[job / a.jobs_per_unit].status, 0, (int)GL_ERR_TIMEOUT);
+      mbar_wait_bounded(bar, 0, BULK_WAIT_CYCLES);
+      return;
+    }
   }
   int g, G;
   const FftGroup f = fft_group(n, a.log2nx, g, G);
@@ -762,7 +776,6 @@ __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __
     const bool active = k < nb;
     cplx* buf = banks + (size_t)(active ? k : 0) * L;
     bool cj = false;
-    const cplx* srow = nullptr;
     int bx0 = 0, bw = 0;
     {
       const int kk0 = active ? k : 0;
@@ -771,7 +784,6 @@ __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __
         if (kk0 >= k0 && kk0 < k0 + a.grp[q].nb) {
           const BankGroup& B = a.grp[q];
           cj = FAMILY == 1 && B.conj != 0;
-          srow = B.data + (((size_t)job * B.nb + (kk0 - k0)) * a.ny + y) * B.w;
           bx0 = B.x0;
           bw = B.w;
         }
@@ -779,13 +791,8 @@ __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __
       }
     }
     auto load = [&](int xb) -> cplx {
-      cplx v;
-      if constexpr (PREFETCH) {
-        v = buf[phys(xb)];
-      } else {
-        const int xi = wrap(xb - bx0, n);
-        v = xi < bw ? srow[xi] : czero();
-      }
+      const int xi = wrap(xb - bx0, n);
+      const cplx v = xi < bw ? buf[xi] : czero();  // staged box row
       return cj ? cconj(v) : v;
     };
     auto store = [&](int xb, cplx v) { buf[phys(xb)] = cj ? cconj(v) : v; };
