@@ -10,8 +10,9 @@ across ranks: no collective on the data path).
 Arms:
 * default: the CUDA engine.  ``value`` times gl_execute on spectra already in
   HBM (CUDA events per step, L2 flushed between steps outside the events);
-  ``e2e`` times the public API with host inputs and a device->host read of
-  the real fields each step.
+  ``e2e`` times the public streaming API (``SurfaceStream``) with host inputs
+  and a device->host read of the real fields each step; each step's copy out
+  overlaps the next step's evaluation.
 * ``--impl reference``: the reference algorithm on the host CPU (the FP64
   NumPy oracle, one process per core), rank 0 only.
 
@@ -479,28 +480,31 @@ def run_engine(args, rank: int, world: int, local_rank: int) -> None:
     # ---- end to end through the public API, host inputs -> host fields
     e2e = None
     if not args.no_e2e:
-        host = torch.empty((U, 2, st.ny, st.nx), dtype=torch.float64, pin_memory=True)
-        e2e_out = torch.empty_like(out)
         h2d = dep.ab.nbytes + dep.omega.nbytes + dep.seg_offsets.nbytes + dep.seg_bins.nbytes + \
             times.nbytes
-        d2h = host.numel() * 8
+        d2h = U * 2 * st.ny * st.nx * 8
+        # the public streaming API: every step copies its inputs in and its
+        # real fields out to pinned host memory; step i's device->host copy
+        # overlaps step i+1's evaluation
+        sstream = api.SurfaceStream(coeffs, st.lx, st.ly, st.nx, st.ny,
+                                    components=["eta33", "psi33"], output="real", device=device,
+                                    max_units=args.group or U, check=False)
 
-        def e2e_step():
-            res = api.surface_batch_device(coeffs, st.lx, st.ly, st.nx, st.ny, times,
-                                           components=["eta33", "psi33"], output="real",
-                                           device=device, max_units=args.group or U,
-                                           out=e2e_out, check=False)
-            host.copy_(res.fields, non_blocking=True)
-            torch.cuda.current_stream(device).synchronize()
+        def e2e_steps(k):
+            pending = None
+            for _ in range(k):
+                ticket = sstream.submit(times)
+                if pending is not None:
+                    sstream.result(pending)
+                pending = ticket
+            sstream.result(pending)
 
-        for _ in range(2):
-            e2e_step()
+        e2e_steps(2)
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for _ in range(args.steps):
-            e2e_step()
+        e2e_steps(args.steps)
         torch.cuda.synchronize()
         e2e_s = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=device)
         if world > 1:

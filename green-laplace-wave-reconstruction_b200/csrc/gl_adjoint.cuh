@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(256, 2) col_combine_kernel(CmbArgs a, const cp
 // A bin's forward value survived the stage's mask and roundoff floor
 // (the forward's floored(): |v| < rel * max zeroes it).
 GL_D bool kept(cplx v, double rel, unsigned long long peak_bits, unsigned char in_mask) {
-  return in_mask && !(cabs_(v) < rel * as_double(peak_bits));
+  return in_mask && !abs_below(v, rel * as_double(peak_bits));
 }
 
 struct AdjArgs {

@@ -34,6 +34,16 @@ GL_HD cplx cconj(cplx a) { return cmk(a.x, -a.y); }
 // |z| as numpy computes it (hypot).
 GL_D double cabs_(cplx a) { return hypot(a.x, a.y); }
 
+// hypot(v) < t, numpy's |z| comparison (a squared-magnitude shortcut that
+// skips hypot away from t measured slower in the accumulation kernels).
+GL_D bool abs_below(cplx v, double t) { return cabs_(v) < t; }
+
+// Running max of |v| = hypot(v) with NaN propagation.
+GL_D double keep_max_abs(double cur, cplx v) {
+  const double m = cabs_(v);
+  return (m > cur || m != m) ? m : cur;
+}
+
 // Max of non-negative doubles through the integer order of their bit patterns.
 // NaN patterns order above +inf, so a NaN input propagates to the result.
 GL_D void atomic_max_nonneg(unsigned long long* slot, double v) {
@@ -48,6 +58,9 @@ GL_HD int wrap(int m, int n) { return m & (n - 1); }
 // of two); the power-of-two test is uniform across a launch.
 GL_HD int wrap_any(int m, int n) {
   if ((n & (n - 1)) == 0) return m & (n - 1);
+  if (m < 0) m += n;  // callers pass -n <= m < 2n: no division
+  else if (m >= n) m -= n;
+  if (m >= 0 && m < n) return m;
   const int r = m % n;
   return r < 0 ? r + n : r;
 }

@@ -1031,7 +1031,58 @@ static int grid_for(size_t n, int threads, int cap = 4096) {
 
 static int fft_cols_per_block(int n, int w) {
   const int T = is_pow2(n) ? n / 16 : 16;  // threads per column transform
-  return std::max(1, std::min(256 / T, w));
+  // a power of two (the kernels split thread indices with shifts)
+  return std::max(1, std::min(256 / T, next_pow2(w)));
+}
+
+// Twin banks: a bank whose multiplier is a column-constant factor times
+// another bank's on the same source (qx, i qx: constant along a column of a
+// box) is written by the column stage from that bank's transformed column
+// (see ColArgs::twins), so only the other banks are transformed.
+// set_banks() fills the column stage's bank lists from the stage's logical
+// list (mult[k], src[k]); the output keeps the logical layout.
+struct TwinRule {
+  int m, parent, fac;  // m = factor(fac) * parent
+};
+static const TwinRule kTwinRules[] = {
+    {M_QX, M_ONE, 1}, {M_NUQX, M_NU, 1}, {M_IQX, M_ONE, 2}, {M_NUQX, M_MI_NU, 2}};
+
+static void set_banks(ColArgs& a, int nb, const int* mult, const int* src) {
+  int parent_of[MAX_BANKS], fac_of[MAX_BANKS];
+  for (int k = 0; k < nb; ++k) {
+    parent_of[k] = -1;
+    fac_of[k] = 0;
+    for (const TwinRule& r : kTwinRules) {
+      if (mult[k] != r.m || parent_of[k] >= 0) continue;
+      for (int j = 0; j < nb; ++j) {
+        bool taken = false;  // one twin per transformed bank
+        for (int q = 0; q < k; ++q) taken = taken || parent_of[q] == j;
+        if (j != k && !taken && mult[j] == r.parent && src[j] == src[k]) {
+          parent_of[k] = j;
+          fac_of[k] = r.fac;
+          break;
+        }
+      }
+    }
+  }
+  a.twins = 1;
+  a.nout = nb;
+  int ns = 0;
+  for (int k = 0; k < nb; ++k) {
+    if (parent_of[k] >= 0) continue;
+    a.mult[ns] = mult[k];
+    a.src_of[ns] = src[k];
+    a.out_of[ns] = k;
+    a.twin[ns] = -1;
+    a.twin_fac[ns] = 0;
+    for (int q = 0; q < nb; ++q)
+      if (parent_of[q] == k) {
+        a.twin[ns] = q;
+        a.twin_fac[ns] = fac_of[q];
+      }
+    ++ns;
+  }
+  a.nbanks = ns;
 }
 
 // Column kernels are instantiated per mixed radix (MIX = n/16 for the mixed
@@ -1078,7 +1129,7 @@ static gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, c
   const int nz = (a.nbanks + 3) / 4;
   const int bpb = (a.nbanks + nz - 1) / nz;
   dim3 grid((a.box.w + cw - 1) / cw, njobs, (a.nbanks + bpb - 1) / bpb);
-  const double bytes = (double)njobs * a.nbanks * a.box.w * a.n * sizeof(cplx) +
+  const double bytes = (double)njobs * (a.twins ? a.nout : a.nbanks) * a.box.w * a.n * sizeof(cplx) +
                        (double)njobs * a.box.w * a.box.h * sizeof(cplx);
   LaunchScope ls("col_ifft_kernel", st, bytes);
   GL_MIX_DISPATCH(a.n, col_ifft_launch, grid, smem, st, a, tw, cw, bpb);
@@ -1436,9 +1487,9 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     ColArgs a;
     std::memset(&a, 0, sizeof a);
     a.kind = COL_ETA22;
-    a.nbanks = 8;
     const int m8[8] = {M_ONE, M_NU, M_NU2, M_QX_DIVNU, M_QY_DIVNU, M_Q2_DIVNU, M_QX, M_QY};
-    for (int k = 0; k < 8; ++k) a.mult[k] = m8[k];
+    const int z8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    set_banks(a, 8, m8, z8);
     a.box = B1;
     a.geo = p->geo1;
     a.spec = spec;
@@ -1645,10 +1696,10 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       ColArgs a;
       std::memset(&a, 0, sizeof a);
       a.kind = COL_INNER;
-      a.nbanks = 12;
       const int m12[12] = {M_ONE, M_NU, M_NU2, M_NU3, M_QX_SNU, M_QY_SNU,
                            M_QX, M_QY, M_Q2_SNU, M_Q2, M_NUQX, M_NUQY};
-      for (int k = 0; k < 12; ++k) a.mult[k] = m12[k];
+      const int z12[12] = {0};
+      set_banks(a, 12, m12, z12);
       a.box = B1;
       a.geo = p->geo1;
       a.spec = spec;
@@ -1725,10 +1776,10 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       ColArgs a;
       std::memset(&a, 0, sizeof a);
       a.kind = COL_OUTER1;
-      a.nbanks = 12;
       const int m12[12] = {M_ONE, M_IQX, M_IQY, M_QX_SNU, M_QY_SNU, M_MI_NU,
                            M_NUQX, M_NUQY, M_MI_Q2_SNU, M_MI_Q2NU, M_MINUS_A, M_MINUS_Q2};
-      for (int k = 0; k < 12; ++k) a.mult[k] = m12[k];
+      const int z12[12] = {0};
+      set_banks(a, 12, m12, z12);
       a.box = B1;
       a.geo = p->geo1;
       a.spec = spec;
@@ -1744,13 +1795,9 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       ColArgs a2;
       std::memset(&a2, 0, sizeof a2);
       a2.kind = COL_OUTER2;
-      a2.nbanks = 9;
       const int m9[9] = {M_ONE, M_IQX, M_IQY, M_IQX, M_IQY, M_A, M_Q2, M_A, M_ONE};
       const int src9[9] = {0, 0, 0, 2, 2, 2, 2, 3, 1};
-      for (int k = 0; k < 9; ++k) {
-        a2.mult[k] = m9[k];
-        a2.src_of[k] = src9[k];
-      }
+      set_banks(a2, 9, m9, src9);
       a2.box = B2;
       a2.geo = p->geo2;
       a2.spec = E;

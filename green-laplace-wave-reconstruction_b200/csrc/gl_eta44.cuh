@@ -43,10 +43,7 @@ GL_D void e44_max_reduce(double* v, int n, unsigned long long* slots) {
   }
 }
 
-GL_D double e44_keep_max(double cur, cplx v) {
-  const double m = cabs_(v);
-  return (m > cur || m != m) ? m : cur;
-}
+GL_D double e44_keep_max(double cur, cplx v) { return keep_max_abs(cur, v); }
 
 // Pair level: the five pair spectra of one group (gl_eta44_fftw.cpp:383-402).
 __global__ void acc_e44_pair_kernel(E44Acc a) {

@@ -188,6 +188,15 @@ struct ColArgs {
   // conj(F(conj x)) -- the transpose of a forward transform, used by the
   // adjoint to carry adjoint spectra to the grid
   int conj_io;
+  // Twin outputs (twins = 1): a bank whose multiplier is a column-constant
+  // factor times another bank's (qx, i qx along a box column) is written from
+  // that bank's transformed column instead of being transformed itself.  The
+  // output then holds nout banks; transformed bank k goes to bank out_of[k]
+  // and, when twin[k] >= 0, times twin_fac[k] (1: qx, 2: i qx of the column,
+  // from the geometry's qx plane) to bank twin[k].
+  int twins;
+  int nout;
+  int out_of[MAX_BANKS], twin[MAX_BANKS], twin_fac[MAX_BANKS];
 };
 
 // Damping base value of the job at box bin i (COL_ETA22/PSI22/INNER/OUTER1).
@@ -279,9 +288,11 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
   cplx* bufs = smem;                   // cw * L
   cplx* base = smem + (size_t)cw * L;  // cw * h
   const bool shared_base = a.kind != COL_PLAIN && a.kind != COL_OUTER2 && a.kind != COL_FLOORED;
+  const int lcw = 31 - __clz(cw);  // cw is a power of two
   if (shared_base) {
-    for (int t = threadIdx.x; t < ncol * h; t += blockDim.x) {
-      const int c = t / h, by = t % h;
+    for (int t = threadIdx.x; t < (h << lcw); t += blockDim.x) {
+      const int c = t & (cw - 1), by = t >> lcw;
+      if (c >= ncol) continue;
       const int i = by * a.box.w + x_first + c;
       base[c * h + by] = col_base(a, job, i, __ldg(a.geo + 3 * plane + i));
     }
@@ -303,12 +314,18 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
         !floor_it ? 0.0
                   : a.floor_rel * as_double(a.kind == COL_FLOORED ? a.floor_max[(size_t)job * a.floor_nsrc + a.src_of[k]]
                                                                   : a.floor_max[job]);
-    cplx* dst = a.out + ((size_t)job * a.nbanks + k) * n * a.box.w + x_first;
+    const int nout = a.twins ? a.nout : a.nbanks;
+    const int tb = a.twins ? a.twin[k] : -1;
+    const int tfac = tb >= 0 ? a.twin_fac[k] : 0;
+    cplx* dst = a.out + ((size_t)job * nout + (a.twins ? a.out_of[k] : k)) * n * a.box.w + x_first;
+    cplx* dst2 = tb >= 0 ? a.out + ((size_t)job * nout + tb) * n * a.box.w + x_first : nullptr;
     for (int it = 0; it < iters; ++it) {
       const int c = it * G + g;
       const bool active = c < ncol;
       cplx* buf = bufs + (size_t)(active ? c : 0) * L;
       cplx* dcol = dst + (active ? c : 0);
+      cplx* dcol2 = dst2 ? dst2 + (active ? c : 0) : nullptr;
+      const double qxc = (dst2 && active) ? __ldg(a.geo + x_first + c) : 0.0;  // qx plane, row 0
       auto load = [&](int yb) -> cplx {
         const int by = wrap_any(yb - a.box.y0, n);
         if (by >= h) return czero();
@@ -318,25 +335,37 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
           v = base[c * h + by];
         } else {
           v = sk[i];
-          if (floor_it && cabs_(v) < floor_abs) v = czero();
+          if (floor_it && abs_below(v, floor_abs)) v = czero();
         }
         const cplx mv = apply_mult(mult, GeoRef{a.geo, plane, i}, v);
         return a.conj_io ? cconj(mv) : mv;
       };
       auto store = [&](int yb, cplx v) {
-        if (direct)
-          dcol[(size_t)yb * a.box.w] = cscale(a.scale, a.conj_io ? cconj(v) : v);
-        else
+        if (direct) {
+          const cplx w = cscale(a.scale, a.conj_io ? cconj(v) : v);
+          dcol[(size_t)yb * a.box.w] = w;
+          if (dcol2) {
+            const cplx u = cscale(qxc, w);
+            dcol2[(size_t)yb * a.box.w] = tfac == 2 ? cmuli(u) : u;
+          }
+        } else {
           buf[phys(yb)] = v;
+        }
       };
       fft_row<+1, MIX>(buf, f, active, tw, load, store);
     }
     if (!direct) {
       __syncthreads();
-      for (int t = threadIdx.x; t < n * ncol; t += blockDim.x) {
-        const int y = t / ncol, c = t % ncol;
+      for (int t = threadIdx.x; t < (n << lcw); t += blockDim.x) {
+        const int y = t >> lcw, c = t & (cw - 1);
+        if (c >= ncol) continue;
         const cplx v = bufs[(size_t)c * L + phys(y)];
-        dst[(size_t)y * a.box.w + c] = cscale(a.scale, a.conj_io ? cconj(v) : v);
+        const cplx w = cscale(a.scale, a.conj_io ? cconj(v) : v);
+        dst[(size_t)y * a.box.w + c] = w;
+        if (dst2) {
+          const cplx u = cscale(__ldg(a.geo + x_first + c), w);
+          dst2[(size_t)y * a.box.w + c] = tfac == 2 ? cmuli(u) : u;
+        }
       }
       __syncthreads();
     }
@@ -867,18 +896,20 @@ __global__ void __launch_bounds__(256, 2) col_fft_kernel(ColFftArgs a, const cpl
   const cplx* src = a.in + (size_t)js * n * a.box.w + x_first;
   // stage the kept columns ([y][col] rows in global memory) with eight
   // independent loads in flight per thread
-  const int total = n * ncol;
+  const int lcw = 31 - __clz(cw);  // cw is a power of two: (y, c) = (t >> lcw, t & (cw - 1))
+  const int total = n << lcw;
   for (int t0 = threadIdx.x; t0 < total; t0 += 8 * blockDim.x) {
     cplx v[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int t = t0 + u * blockDim.x;
-      if (t < total) v[u] = src[(size_t)(t / ncol) * a.box.w + t % ncol];
+      if (t < total && (t & (cw - 1)) < ncol) v[u] = src[(size_t)(t >> lcw) * a.box.w + (t & (cw - 1))];
     }
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int t = t0 + u * blockDim.x;
-      if (t < total) bufs[(size_t)(t % ncol) * L + phys(t / ncol)] = a.conj_io ? cconj(v[u]) : v[u];
+      if (t < total && (t & (cw - 1)) < ncol)
+        bufs[(size_t)(t & (cw - 1)) * L + phys(t >> lcw)] = a.conj_io ? cconj(v[u]) : v[u];
     }
   }
   __syncthreads();
@@ -896,15 +927,15 @@ __global__ void __launch_bounds__(256, 2) col_fft_kernel(ColFftArgs a, const cpl
   const unsigned char* mask = a.mask ? a.mask + (size_t)unit * a.box.w * a.box.h : nullptr;
   cplx* dst = a.out + (size_t)js * a.box.w * a.box.h;
   double local = 0.0;
-  for (int t = threadIdx.x; t < ncol * a.box.h; t += blockDim.x) {
-    const int c = t % ncol, by = t / ncol;
+  for (int t = threadIdx.x; t < (a.box.h << lcw); t += blockDim.x) {
+    const int c = t & (cw - 1), by = t >> lcw;
+    if (c >= ncol) continue;
     const int i = by * a.box.w + x_first + c;
     const cplx raw = bufs[(size_t)c * L + phys(wrap_any(a.box.y0 + by, n))];
     cplx v = cscale(a.scale, a.conj_io ? cconj(raw) : raw);
     if (mask && !mask[i]) v = czero();
     dst[i] = v;
-    const double m = cabs_(v);
-    local = (m > local || m != m) ? m : local;
+    local = keep_max_abs(local, v);
   }
   if (a.maxslot) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -920,7 +951,7 @@ __global__ void __launch_bounds__(256, 2) col_fft_kernel(ColFftArgs a, const cpl
 // ---------------------------------------------------------------------------
 
 GL_D cplx floored(cplx v, double rel, unsigned long long peak_bits) {
-  return cabs_(v) < rel * as_double(peak_bits) ? czero() : v;
+  return abs_below(v, rel * as_double(peak_bits)) ? czero() : v;
 }
 
 struct AccArgs {
@@ -1060,8 +1091,7 @@ __global__ void acc_inner_kernel(AccArgs a) {
     dst[plane + i] = et;
     dst[2 * plane + i] = p;
     dst[3 * plane + i] = pt;
-    const double m = cabs_(et);
-    local = (m > local || m != m) ? m : local;
+    local = keep_max_abs(local, et);
   }
   for (int o = 16; o > 0; o >>= 1) {
     const double other = __shfl_xor_sync(0xffffffffu, local, o);
@@ -1091,9 +1121,8 @@ __global__ void acc_outer_combine_kernel(AccArgs a) {
     cplx* dst = a.out + (size_t)uj * 2 * plane;
     dst[i] = kpsi;
     dst[plane + i] = dpsi;
-    const double m0 = cabs_(kpsi), m1 = cabs_(dpsi);
-    l0 = (m0 > l0 || m0 != m0) ? m0 : l0;
-    l1 = (m1 > l1 || m1 != m1) ? m1 : l1;
+    l0 = keep_max_abs(l0, kpsi);
+    l1 = keep_max_abs(l1, dpsi);
   }
   for (int o = 16; o > 0; o >>= 1) {
     const double o0 = __shfl_xor_sync(0xffffffffu, l0, o);

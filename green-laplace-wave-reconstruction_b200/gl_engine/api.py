@@ -398,8 +398,10 @@ def surface_batch_device(coeffs: GLCoefficients, Lx, Ly, Nx, Ny, times, *,
     stream = stream or torch.cuda.current_stream(device)
     with torch.cuda.device(device), torch.cuda.stream(stream):
         def h2d(arr, dtype):
-            return torch.from_numpy(np.ascontiguousarray(arr)).to(device=device, dtype=dtype,
-                                                                  non_blocking=True)
+            # staged through pinned memory so the copy is asynchronous (a
+            # pageable source would synchronise the stream first)
+            host = torch.from_numpy(np.ascontiguousarray(arr)).to(dtype=dtype).pin_memory()
+            return host.to(device=device, non_blocking=True)
         seg_off = h2d(dep.seg_offsets, torch.int32)
         seg_bin = h2d(dep.seg_bins, torch.int32)
         ab = h2d(dep.ab, torch.float64)
@@ -419,6 +421,73 @@ def surface_batch_device(coeffs: GLCoefficients, Lx, Ly, Nx, Ny, times, *,
     if check:
         _check_status(status)
     return res
+
+
+class SurfaceStream:
+    """Batches of snapshots of one sea state streamed to pinned host memory.
+
+    ``submit(times)`` evaluates one batch through ``surface_batch_device``
+    (host inputs copied in, fields into one of two device buffers) and queues
+    the device->host copy of its fields on a separate copy stream, so the copy
+    of batch i overlaps the evaluation of batch i+1.  ``result(ticket)`` waits
+    for that batch's copy and returns its host fields; a host buffer is reused
+    two submissions later, so read (or copy) a result before submitting twice
+    more.
+    """
+
+    def __init__(self, coeffs: GLCoefficients, Lx, Ly, Nx, Ny, *,
+                 components: Sequence[str] | None = None, output: str = "real",
+                 grid: str = "compact", device=None, max_units: int | None = None,
+                 check: bool = True, order3_ranks=(4, 4)):
+        self._args = (coeffs, Lx, Ly, Nx, Ny)
+        self._kw = dict(components=components, output=output, grid=grid,
+                        max_units=max_units, order3_ranks=order3_ranks)
+        self.device = torch.device(device if device is not None else "cuda")
+        self.check = check
+        self._copy = torch.cuda.Stream(self.device)
+        self._dev: list[torch.Tensor | None] = [None, None]
+        self._host: list[torch.Tensor | None] = [None, None]
+        self._status: list[torch.Tensor | None] = [None, None]
+        self._computed = [torch.cuda.Event(), torch.cuda.Event()]
+        self._copied = [torch.cuda.Event(), torch.cuda.Event()]
+        self._names: list[str] = []
+        self._plan: Plan | None = None
+        self._submitted = 0
+
+    def submit(self, times) -> int:
+        slot = self._submitted % 2
+        comp = torch.cuda.current_stream(self.device)
+        dev = self._dev[slot]
+        if dev is not None:
+            comp.wait_event(self._copied[slot])  # the slot's previous copy has read it
+            if dev.shape[0] != np.atleast_1d(times).size:
+                dev = None
+        res = surface_batch_device(*self._args, times, device=self.device, check=False,
+                                   stream=comp, out=dev, **self._kw)
+        self._dev[slot] = res.fields
+        self._status[slot] = res.status
+        self._names, self._plan = res.names, res.plan
+        self._computed[slot].record(comp)
+        host = self._host[slot]
+        if host is None or host.shape != res.fields.shape:
+            host = torch.empty(res.fields.shape, dtype=res.fields.dtype, pin_memory=True)
+            self._host[slot] = host
+        self._copy.wait_event(self._computed[slot])
+        with torch.cuda.stream(self._copy):
+            host.copy_(res.fields, non_blocking=True)
+        self._copied[slot].record(self._copy)
+        self._submitted += 1
+        return self._submitted - 1
+
+    def result(self, ticket: int) -> SurfaceBatch:
+        if not 0 <= ticket < self._submitted or ticket < self._submitted - 2:
+            raise ValueError("ticket is not one of the last two submissions")
+        slot = ticket % 2
+        self._copied[slot].synchronize()
+        if self.check:
+            _check_status(self._status[slot])
+        return SurfaceBatch(fields=self._host[slot], names=self._names, status=self._status[slot],
+                            plan=self._plan)
 
 
 def _audit(coeffs: GLCoefficients, plan: Plan, names, Lx, Ly, Nx, Ny, t) -> dict[str, Any]:
