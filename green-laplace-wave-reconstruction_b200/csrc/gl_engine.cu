@@ -1121,6 +1121,18 @@ static void col_fft_launch(dim3 grid, size_t smem, cudaStream_t st, const ColFft
     default: launcher<0>(__VA_ARGS__); break;                              \
   }
 
+// Per-stage names of the column launches in the launch accounting.
+static const char* col_ifft_name(int kind) {
+  switch (kind) {
+    case COL_ETA22: case COL_PSI22: return "col_ifft_kernel[order2]";
+    case COL_INNER: return "col_ifft_kernel[inner]";
+    case COL_OUTER1: return "col_ifft_kernel[outer1]";
+    case COL_OUTER2: return "col_ifft_kernel[outer2]";
+    case COL_E44_PAIR: case COL_E44_FIRST3: case COL_E44_FIRST4: return "col_ifft_kernel[order4]";
+  }
+  return "col_ifft_kernel";
+}
+
 static gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
   if (!is_pow2(a.n) && !mixed_len(a.n)) return fail(GL_ERR_UNSUPPORTED, "column length %d has no transform", a.n);
   const int cw = fft_cols_per_block(a.n, a.box.w);
@@ -1131,7 +1143,7 @@ static gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, c
   dim3 grid((a.box.w + cw - 1) / cw, njobs, (a.nbanks + bpb - 1) / bpb);
   const double bytes = (double)njobs * (a.twins ? a.nout : a.nbanks) * a.box.w * a.n * sizeof(cplx) +
                        (double)njobs * a.box.w * a.box.h * sizeof(cplx);
-  LaunchScope ls("col_ifft_kernel", st, bytes);
+  LaunchScope ls(col_ifft_name(a.kind), st, bytes);
   GL_MIX_DISPATCH(a.n, col_ifft_launch, grid, smem, st, a, tw, cw, bpb);
   LAUNCH_CHECK("col_ifft_kernel");
   return GL_OK;
@@ -1190,13 +1202,14 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
   return GL_OK;
 }
 
-static gl_status launch_col_fft(const ColFftArgs& a, int njs, cudaStream_t st, const cplx* tw) {
+static gl_status launch_col_fft(const ColFftArgs& a, int njs, cudaStream_t st, const cplx* tw,
+                                const char* name = "col_fft_kernel") {
   if (!is_pow2(a.n) && !mixed_len(a.n)) return fail(GL_ERR_UNSUPPORTED, "column length %d has no transform", a.n);
   const int cw = fft_cols_per_block(a.n, a.box.w);
   const size_t smem = (size_t)cw * padded_len(a.n) * sizeof(cplx);
   dim3 grid((a.box.w + cw - 1) / cw, njs);
   const double bytes = (double)njs * a.box.w * (a.n + a.box.h) * sizeof(cplx);
-  LaunchScope ls("col_fft_kernel", st, bytes);
+  LaunchScope ls(name, st, bytes);
   GL_MIX_DISPATCH(a.n, col_fft_launch, grid, smem, st, a, tw, cw);
   LAUNCH_CHECK("col_fft_kernel");
   return GL_OK;
@@ -1742,7 +1755,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       f.mask = s2;
       f.maxslot = maxRI;
       f.scale = fwd_scale2;
-      if ((s = launch_col_fft(f, njobs * 4, st, p->tw)) != GL_OK) return s;
+      if ((s = launch_col_fft(f, njobs * 4, st, p->tw, "col_fft_kernel[inner]")) != GL_OK) return s;
       AccArgs c;
       std::memset(&c, 0, sizeof c);
       c.us = us;
@@ -1840,7 +1853,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       f.mask = s3;
       f.maxslot = maxRO;
       f.scale = fwd_scale3;
-      if ((s = launch_col_fft(f, nuj * 4, st, p->tw)) != GL_OK) return s;
+      if ((s = launch_col_fft(f, nuj * 4, st, p->tw, "col_fft_kernel[outer]")) != GL_OK) return s;
       AccArgs c;
       std::memset(&c, 0, sizeof c);
       c.us = us;

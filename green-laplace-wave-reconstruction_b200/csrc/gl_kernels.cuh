@@ -326,19 +326,28 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
       cplx* dcol = dst + (active ? c : 0);
       cplx* dcol2 = dst2 ? dst2 + (active ? c : 0) : nullptr;
       const double qxc = (dst2 && active) ? __ldg(a.geo + x_first + c) : 0.0;  // qx plane, row 0
+      // The group first writes its column's multiplied box rows to the front
+      // of the column's buffer (one copy of the multiplier code in a short
+      // loop, all loads independent); the first transform pass reads them
+      // back before it writes the padded column over them.
+      if (active) {
+        for (int by = f.t; by < h; by += f.T) {
+          const int i = by * a.box.w + x_first + c;
+          cplx v;
+          if (shared_base) {
+            v = base[c * h + by];
+          } else {
+            v = sk[i];
+            if (floor_it && abs_below(v, floor_abs)) v = czero();
+          }
+          const cplx mv = apply_mult(mult, GeoRef{a.geo, plane, i}, v);
+          buf[by] = a.conj_io ? cconj(mv) : mv;
+        }
+      }
+      f.sync();
       auto load = [&](int yb) -> cplx {
         const int by = wrap_any(yb - a.box.y0, n);
-        if (by >= h) return czero();
-        const int i = by * a.box.w + x_first + c;
-        cplx v;
-        if (shared_base) {
-          v = base[c * h + by];
-        } else {
-          v = sk[i];
-          if (floor_it && abs_below(v, floor_abs)) v = czero();
-        }
-        const cplx mv = apply_mult(mult, GeoRef{a.geo, plane, i}, v);
-        return a.conj_io ? cconj(mv) : mv;
+        return by < h ? buf[by] : czero();
       };
       auto store = [&](int yb, cplx v) {
         if (direct) {
