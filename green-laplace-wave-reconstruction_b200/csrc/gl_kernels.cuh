@@ -387,7 +387,7 @@ __global__ void __launch_bounds__(256, 2) col_ifft_kernel(ColArgs a, const cplx*
 
 enum RowKind : int { ROW_ETA22 = 0, ROW_PSI22, ROW_CONTACT22, ROW_INNER, ROW_OUTER,
                      ROW_E44_PAIR, ROW_E44_THIRD, ROW_E44_ORDER4, ROW_E44_ORDER4_PSI,
-                     // adjoint (transposed) products, row_kernel_t<1>
+                     // adjoint (transposed) products (row kernel family 1)
                      ROW_ADJ_ETA22, ROW_ADJ_INNER, ROW_ADJ_OUTER };
 
 struct BankGroup {
