@@ -30,6 +30,7 @@ struct UnitSlots {
   unsigned long long count;      // support size
   unsigned long long nonfinite;  // set when a non-finite value is met
   unsigned long long pad[3];   // [0] min q over S, [1] max |s| outside the box, [2] max sqrt(A) over the quartic support
+  unsigned long long dup;      // 1: the unit's support equals unit 0's (its Minkowski sums are copied)
 };
 
 constexpr int MAX_RANK = 16;

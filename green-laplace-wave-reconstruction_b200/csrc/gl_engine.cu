@@ -399,10 +399,12 @@ struct MinkArgs {
   const double* geoc;
   UnitSlots* slots;
   int which;                    // 2: sqa_max2, 3: sqa_max3, 0: none
+  int skip_dup;                 // 1: units flagged dup are filled by mink_copy_kernel instead
 };
 
 __global__ void minkowski_kernel(MinkArgs m) {
   const int job = blockIdx.y;
+  if (m.skip_dup && m.slots[job].dup) return;
   const unsigned long long* A = m.a + job * m.a_job_stride;
   const unsigned long long* B = m.brev + job * m.b_job_stride;
   unsigned char* C = m.c + job * m.c_job_stride;
@@ -419,6 +421,31 @@ __global__ void minkowski_kernel(MinkArgs m) {
     if ((threadIdx.x & 31) == 0)
       atomic_max_nonneg(m.which == 2 ? &m.slots[job].sqa_max2
                         : m.which == 3 ? &m.slots[job].sqa_max3 : &m.slots[job].pad[2], lmax);
+  }
+}
+
+// dup = 1 for a unit u >= 1 whose support rows equal unit 0's: then S2 = S+S
+// and S3 = S2+S equal unit 0's too (snapshots of one sea state share their
+// support), and the Minkowski sums are copied instead of recomputed.
+__global__ void support_dup_kernel(const unsigned long long* s1f, long long words, UnitSlots* slots) {
+  const int u = blockIdx.x + 1;
+  const unsigned long long* a = s1f + (size_t)u * words;
+  bool diff = false;
+  for (long long t = threadIdx.x; t < words; t += blockDim.x) diff |= a[t] != s1f[t];
+  diff = __syncthreads_or(diff);
+  if (threadIdx.x == 0) slots[u].dup = diff ? 0ull : 1ull;
+}
+
+// The Minkowski sum of unit 0 (mask plane and its sqrt(A) maximum) copied to
+// the units flagged dup.
+__global__ void mink_copy_kernel(unsigned char* c, long long plane, int which, UnitSlots* slots) {
+  const int u = blockIdx.y + 1;
+  if (!slots[u].dup) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane; i += (long long)gridDim.x * blockDim.x)
+    c[(size_t)u * plane + i] = c[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (which == 2) slots[u].sqa_max2 = slots[0].sqa_max2;
+    if (which == 3) slots[u].sqa_max3 = slots[0].sqa_max3;
   }
 }
 
@@ -1259,6 +1286,7 @@ static void mink_args(MinkArgs& m, const unsigned long long* a, int ha, int wa, 
   m.geoc = geoc;
   m.slots = slots;
   m.which = which;
+  m.skip_dup = 0;
 }
 
 // Final transform of box spectra `spec` ([unit][nb][box]) to the reference
@@ -1387,14 +1415,25 @@ static gl_status analyse_group(gl_plan* p, int gu, const void* spectra, int layo
       bitrows_kernel<<<g, T, 0, st>>>(s1, B1.h, B1.w, p->ww1, s1f, s1r);
     }
     LAUNCH_CHECK("bitrows_kernel");
+    if (gu > 1) {
+      LaunchScope ls_("support_dup_kernel", st, 0.0);
+      support_dup_kernel<<<gu - 1, T, 0, st>>>(s1f, (long long)B1.h * p->ww1, slots);
+    }
+    LAUNCH_CHECK("support_dup_kernel");
     MinkArgs m;
     mink_args(m, s1f, B1.h, B1.w, p->ww1, s1r, B1.h, B1.w, p->ww1, s2, p->geo2, slots, 2);
+    m.skip_dup = 1;
     dim3 g2(grid_for(pl2, T, 256), gu);
     {
       LaunchScope ls_("minkowski_kernel", st, 0.0);
       minkowski_kernel<<<g2, T, 0, st>>>(m);
     }
     LAUNCH_CHECK("minkowski_kernel");
+    if (gu > 1) {
+      LaunchScope ls_("mink_copy_kernel", st, 0.0);
+      mink_copy_kernel<<<dim3(grid_for(pl2, T, 64), gu - 1), T, 0, st>>>(s2, pl2, 2, slots);
+    }
+    LAUNCH_CHECK("mink_copy_kernel");
   }
   if (p->want_o3) {
     dim3 g(grid_for(B2.h * p->ww2, T, 64), gu);
@@ -1405,12 +1444,18 @@ static gl_status analyse_group(gl_plan* p, int gu, const void* spectra, int layo
     LAUNCH_CHECK("bitrows_kernel");
     MinkArgs m;
     mink_args(m, s2f, B2.h, B2.w, p->ww2, s1r, B1.h, B1.w, p->ww1, s3, p->geo3, slots, 3);
+    m.skip_dup = 1;
     dim3 g3(grid_for(pl3, T, 512), gu);
     {
       LaunchScope ls_("minkowski_kernel", st, 0.0);
       minkowski_kernel<<<g3, T, 0, st>>>(m);
     }
     LAUNCH_CHECK("minkowski_kernel");
+    if (gu > 1) {
+      LaunchScope ls_("mink_copy_kernel", st, 0.0);
+      mink_copy_kernel<<<dim3(grid_for(pl3, T, 64), gu - 1), T, 0, st>>>(s3, pl3, 3, slots);
+    }
+    LAUNCH_CHECK("mink_copy_kernel");
   }
   if (p->want_psi22) {
     dim3 g(grid_for(B1.h * p->ww1, T, 64), gu * 2);

@@ -291,3 +291,52 @@ def test_config2_deviation_is_within_oracle_roundoff_sensitivity():
     print(f"oracle self-spread eta33 {spread_e:.3e} psi33 {spread_p:.3e}; "
           f"engine deviation eta33 {dev_e:.3e} psi33 {dev_p:.3e}")
     assert dev_e < 3 * spread_e and dev_p < 3 * spread_p
+
+
+def test_units_with_different_supports_in_one_launch():
+    """One launch over units whose supports differ (all modes, half of them,
+    all again): each unit equals its own single-unit launch, so support
+    sums shared between equal-support units never leak across units."""
+    st = seastate.small_order3(seed=11, n=64, modes=20)
+    c = gl_engine.gl_spectral_coefficients(3, st.gravity, st.depth, st.a, st.b, st.kx, st.ky,
+                                           0, 0, {"eta22_rank": 4})
+    dep = api.prepare_deposit(c, st.lx, st.ly, 64, 64)
+    plan = api.get_plan(nx=64, ny=64, lx=st.lx, ly=st.ly, depth=c.h, gravity=c.g, order=3,
+                        components=api._components_for(3, None), eta22_rank=4,
+                        allow_below=False, box=dep.box, grid=api.GRID_COMPACT, max_units=3,
+                        output=api.OUT_COMPLEX, device=torch.device("cuda"), inner_rank=4,
+                        outer_rank=4)
+    pairs = dep.ab.reshape(-1, 2)  # (a, b) per mode
+    keep = np.ones((pairs.shape[0], 1))
+    keep[1::2] = 0.0
+    abs_ = [dep.ab, (pairs * keep).ravel(), dep.ab]
+    dev = torch.device("cuda")
+    w, h = dep.box[2], dep.box[3]
+
+    def box_spectra(ab_list, times):
+        out = []
+        for ab, t in zip(ab_list, times):
+            spec = torch.empty((1, h, w, 2), dtype=torch.float64, device=dev)
+            plan.deposit(1, torch.as_tensor(dep.seg_offsets, dtype=torch.int32, device=dev),
+                         torch.as_tensor(dep.seg_bins, dtype=torch.int32, device=dev),
+                         torch.as_tensor(ab, dtype=torch.float64, device=dev),
+                         torch.as_tensor(dep.omega, dtype=torch.float64, device=dev),
+                         torch.as_tensor([t], dtype=torch.float64, device=dev), spec,
+                         torch.cuda.current_stream().cuda_stream)
+            out.append(spec)
+        return torch.cat(out)
+
+    times = [0.3, 0.3, 1.7]
+    spec = box_spectra(abs_, times)
+    ncomp = plan.info.n_components
+    both = torch.empty((3, ncomp, 64, 64), dtype=torch.complex128, device=dev)
+    status = torch.zeros(3, dtype=torch.int32, device=dev)
+    plan.execute(3, spec, api.SPECTRA_BOX, both, status, torch.cuda.current_stream().cuda_stream)
+    assert int(status.abs().sum()) == 0
+    for u in range(3):
+        one = torch.empty((1, ncomp, 64, 64), dtype=torch.complex128, device=dev)
+        st1 = torch.zeros(1, dtype=torch.int32, device=dev)
+        plan.execute(1, spec[u:u + 1].contiguous(), api.SPECTRA_BOX, one, st1,
+                     torch.cuda.current_stream().cuda_stream)
+        assert torch.equal(both[u], one[0]), u
+    assert not torch.equal(both[0], both[1])
