@@ -681,6 +681,9 @@ struct gl_plan {
   // mixed lengths 16 m allowed (log2 0 for those); ncy (a power of two) is
   // the adjoint's grid and bounds both
   int ncy2, lncy2, ncy3, lncy3;
+  // forward row length of the pair stages (power of two or 144/160/192/240,
+  // <= ncx: their products need a period covering only the pair box)
+  int ncx2, lncx2;
   Box b1, b2, b3;
   int ww1, ww2;                 // bitset words per row (S1, S2)
   bool want_eta22, want_psi22, want_o3, want_first;
@@ -734,6 +737,16 @@ static int col_len(int v) {
   return best;
 }
 static int col_log2(int n) { return is_pow2(n) ? ilog2(n) : 0; }
+
+// Smallest row-transform length >= v: a power of two (>= 16) or one of the
+// mixed lengths the pair-stage row kernels are instantiated for.
+static int row_len(int v) {
+  int best = std::max(16, next_pow2(v));
+  const int mixed[4] = {144, 160, 192, 240};
+  for (int k = 0; k < 4; ++k)
+    if (mixed[k] >= v && mixed[k] < best) best = mixed[k];
+  return best;
+}
 
 struct Bump {
   size_t off = 0;
@@ -896,10 +909,13 @@ extern "C" gl_status gl_plan_create(gl_plan** out, const gl_plan_desc* desc) {
   p->lncx = ilog2(p->ncx);
   p->lncy = ilog2(p->ncy);
   p->ncy2 = p->ncy3 = p->ncy;
+  p->ncx2 = p->ncx;
   if (d.grid != GL_GRID_REFERENCE && deg > 1) {
     p->ncy2 = std::min(p->ncy, col_len(p->b2.h));
     if (deg == 3) p->ncy3 = std::min(p->ncy, col_len(p->b3.h));
+    p->ncx2 = std::min(p->ncx, row_len(p->b2.w));
   }
+  p->lncx2 = col_log2(p->ncx2);
   p->lncy2 = col_log2(p->ncy2);
   p->lncy3 = col_log2(p->ncy3);
   p->lnx = ilog2(d.nx);
@@ -1011,6 +1027,7 @@ extern "C" gl_status gl_plan_get_info(const gl_plan* p, gl_plan_info* info) {
   info->ncy = p->ncy;
   info->ncy_pair = p->e44 ? p->ncy : p->ncy2;
   info->ncy_triple = p->e44 ? p->ncy : p->ncy3;
+  info->ncx_pair = p->e44 ? p->ncx : p->ncx2;
   const Box* bs[3] = {&p->b1, &p->b2, &p->b3};
   int* dst[3] = {info->box1, info->box2, info->box3};
   for (int k = 0; k < 3; ++k) {
@@ -1176,15 +1193,30 @@ static gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, c
   return GL_OK;
 }
 
-template <int K>
+template <int K, int MIX = 0>
 static void row_launch(dim3 grid, int threads, size_t smem, cudaStream_t st, const RowArgs& a,
                        const cplx* tw) {
   static bool attr = false;
   if (!attr) {  // a failure here surfaces as the launch's own error
-    attr = cudaFuncSetAttribute(row_kernel_t<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    attr = cudaFuncSetAttribute(row_kernel_t<K, MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)ROW_SMEM_LIMIT) == cudaSuccess;
   }
-  row_kernel_t<K><<<grid, threads, smem, st>>>(a, tw);
+  row_kernel_t<K, MIX><<<grid, threads, smem, st>>>(a, tw);
+}
+
+// Pair-stage rows also run on the mixed row lengths 144, 160, 192, 240
+// (row_len); each is its own instantiation.
+template <int K>
+static bool row_launch_mixed(dim3 grid, int threads, size_t smem, cudaStream_t st, const RowArgs& a,
+                             const cplx* tw) {
+  switch (mixed_len(a.nx) ? a.nx / 16 : 0) {
+    case 0: row_launch<K, 0>(grid, threads, smem, st, a, tw); return true;
+    case 9: row_launch<K, 9>(grid, threads, smem, st, a, tw); return true;
+    case 10: row_launch<K, 10>(grid, threads, smem, st, a, tw); return true;
+    case 12: row_launch<K, 12>(grid, threads, smem, st, a, tw); return true;
+    case 15: row_launch<K, 15>(grid, threads, smem, st, a, tw); return true;
+  }
+  return false;
 }
 
 static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
@@ -1198,7 +1230,12 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
   // 8 transform groups per block (n/16 threads each) when the row has at
   // most 12 banks (4 blocks fit per SM by shared memory), 16 for the wider
   // outer stage (2 blocks per SM); at least one warp
-  const int threads = std::max(32, std::min(256, (nb <= 12 ? 8 : 16) * (a.nx / 16)));
+  const int T = is_pow2(a.nx) ? a.nx / 16 : 16;  // threads per row transform
+  const int threads = std::max(32, std::min(256, (nb <= 12 ? 8 : 16) * T));
+  const bool pair_kind = a.kind == ROW_ETA22 || a.kind == ROW_PSI22 || a.kind == ROW_CONTACT22 ||
+                         a.kind == ROW_INNER;
+  if (!is_pow2(a.nx) && !pair_kind)
+    return fail(GL_ERR_UNSUPPORTED, "row kind %d runs power-of-two rows only (got %d)", a.kind, a.nx);
   double bytes = (double)njobs * a.nout * a.out_w * a.ny * sizeof(cplx);
   for (int g = 0; g < a.ngrp; ++g) bytes += (double)njobs * a.grp[g].nb * a.grp[g].w * a.ny * sizeof(cplx);
   const bool adj = a.kind >= ROW_ADJ_ETA22;
@@ -1210,11 +1247,12 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
                      : a.kind >= ROW_E44_PAIR    ? "row_kernel[order4]"
                                                  : "row_kernel[order2]";
   LaunchScope ls(name, st, bytes);
+  bool ok = true;
   switch (a.kind) {
-    case ROW_ETA22: row_launch<ROW_ETA22>(grid, threads, smem, st, a, tw); break;
-    case ROW_PSI22: row_launch<ROW_PSI22>(grid, threads, smem, st, a, tw); break;
-    case ROW_CONTACT22: row_launch<ROW_CONTACT22>(grid, threads, smem, st, a, tw); break;
-    case ROW_INNER: row_launch<ROW_INNER>(grid, threads, smem, st, a, tw); break;
+    case ROW_ETA22: ok = row_launch_mixed<ROW_ETA22>(grid, threads, smem, st, a, tw); break;
+    case ROW_PSI22: ok = row_launch_mixed<ROW_PSI22>(grid, threads, smem, st, a, tw); break;
+    case ROW_CONTACT22: ok = row_launch_mixed<ROW_CONTACT22>(grid, threads, smem, st, a, tw); break;
+    case ROW_INNER: ok = row_launch_mixed<ROW_INNER>(grid, threads, smem, st, a, tw); break;
     case ROW_OUTER: row_launch<ROW_OUTER>(grid, threads, smem, st, a, tw); break;
     case ROW_E44_PAIR: row_launch<ROW_E44_PAIR>(grid, threads, smem, st, a, tw); break;
     case ROW_E44_THIRD: row_launch<ROW_E44_THIRD>(grid, threads, smem, st, a, tw); break;
@@ -1225,6 +1263,7 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
     case ROW_ADJ_OUTER: row_launch<ROW_ADJ_OUTER>(grid, threads, smem, st, a, tw); break;
     default: return fail(GL_ERR_INVALID_ARGUMENT, "unknown row kind %d", a.kind);
   }
+  if (!ok) return fail(GL_ERR_UNSUPPORTED, "row length %d has no transform", a.nx);
   LAUNCH_CHECK("row_kernel");
   return GL_OK;
 }
@@ -1529,7 +1568,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
   const double inv_scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
   const double nn = (double)p->d.nx * (double)p->d.ny;
   const int ncy2 = p->ncy2, ncy3 = p->ncy3;
-  const double fwd_scale2 = nn / ((double)p->ncx * (double)ncy2);
+  const double fwd_scale2 = nn / ((double)p->ncx2 * (double)ncy2);
   const double fwd_scale3 = nn / ((double)p->ncx * (double)ncy3);
 
   // ---------------- eta22 (spatial.py:156-231) ----------------
@@ -1569,8 +1608,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     r.out_x0 = B2.x0;
     r.out_w = B2.w;
     r.out = Q;
-    r.nx = p->ncx;
-    r.log2nx = p->lncx;
+    r.nx = p->ncx2;
+    r.log2nx = p->lncx2;
     r.ny = ncy2;
     r.us = us;
     r.jobs_per_unit = J;
@@ -1650,8 +1689,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     r.out_x0 = B2.x0;
     r.out_w = B2.w;
     r.out = Q;
-    r.nx = p->ncx;
-    r.log2nx = p->lncx;
+    r.nx = p->ncx2;
+    r.log2nx = p->lncx2;
     r.ny = ncy2;
     r.us = us;
     r.jobs_per_unit = 4;
@@ -1697,8 +1736,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     rc.out_x0 = B2.x0;
     rc.out_w = B2.w;
     rc.out = Qc;
-    rc.nx = p->ncx;
-    rc.log2nx = p->lncx;
+    rc.nx = p->ncx2;
+    rc.log2nx = p->lncx2;
     rc.ny = ncy2;
     rc.us = us;
     rc.jobs_per_unit = 1;
@@ -1782,8 +1821,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       r.out_x0 = B2.x0;
       r.out_w = B2.w;
       r.out = QI;
-      r.nx = p->ncx;
-      r.log2nx = p->lncx;
+      r.nx = p->ncx2;
+      r.log2nx = p->lncx2;
       r.ny = ncy2;
       r.us = us;
       r.jobs_per_unit = J * I;

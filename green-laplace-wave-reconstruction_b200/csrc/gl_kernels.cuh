@@ -763,7 +763,9 @@ GL_D void row_products_adj(int kind, cplx* b, int L, int p) {
 // (and get registers) on their own.  FAMILY 0: order-2/3 stages, 1: adjoint
 // stages, 2: order-4 stages (their rows are wider than 24 banks and are
 // staged in shared memory first).
-template <int KIND>
+// MIX = m > 0: the row length is the mixed length 16 m (pair stages on a
+// product grid narrower than a power of two); 0: a power of two.
+template <int KIND, int MIX = 0>
 __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __restrict__ tw) {
   constexpr int FAMILY = KIND >= ROW_ADJ_ETA22 ? 1 : (KIND >= ROW_E44_PAIR && KIND <= ROW_E44_ORDER4_PSI ? 2 : 0);
   extern __shared__ __align__(128) cplx smem[];
@@ -829,12 +831,12 @@ __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __
       }
     }
     auto load = [&](int xb) -> cplx {
-      const int xi = wrap(xb - bx0, n);
+      const int xi = MIX ? wrap_any(xb - bx0, n) : wrap(xb - bx0, n);
       const cplx v = xi < bw ? buf[xi] : czero();  // staged box row
       return cj ? cconj(v) : v;
     };
     auto store = [&](int xb, cplx v) { buf[phys(xb)] = cj ? cconj(v) : v; };
-    fft_row<+1>(buf, f, active, tw, load, store);
+    fft_row<+1, MIX>(buf, f, active, tw, load, store);
   }
   __syncthreads();
   if constexpr (FAMILY == 0) {
@@ -863,10 +865,10 @@ __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __
       return oc ? cconj(v) : v;
     };
     auto store = [&](int xb, cplx v) {
-      const int xo = wrap(xb - ox0, n);
+      const int xo = MIX ? wrap_any(xb - ox0, n) : wrap(xb - ox0, n);
       if (xo < ow) orow[xo] = oc ? cconj(v) : v;
     };
-    fft_row<-1>(buf, f, active, tw, load, store);
+    fft_row<-1, MIX>(buf, f, active, tw, load, store);
   }
 }
 

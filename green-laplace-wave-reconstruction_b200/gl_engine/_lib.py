@@ -79,7 +79,7 @@ class PlanInfo(C.Structure):
         ("box1", C.c_int * 4), ("box2", C.c_int * 4), ("box3", C.c_int * 4),
         ("n_components", C.c_int), ("component_ids", C.c_int * 6),
         ("transforms_per_unit", C.c_double),
-        ("ncy_pair", C.c_int), ("ncy_triple", C.c_int),
+        ("ncy_pair", C.c_int), ("ncy_triple", C.c_int), ("ncx_pair", C.c_int),
     ]
 
 

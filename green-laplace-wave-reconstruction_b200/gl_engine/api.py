@@ -521,6 +521,7 @@ def _audit(coeffs: GLCoefficients, plan: Plan, names, Lx, Ly, Nx, Ny, t) -> dict
             "precision": "fp64",
             "product_grid": [info.ncy, info.ncx],
             "column_grids": {"pair": info.ncy_pair, "triple": info.ncy_triple},
+            "pair_row_length": info.ncx_pair,
             "parent_box": list(info.box1),
             "reference_transforms_per_unit": info.transforms_per_unit,
         },

@@ -104,6 +104,7 @@ typedef struct gl_plan_info {
   double transforms_per_unit; /* 2-D transforms of the reference graph      */
   int ncy_pair, ncy_triple;   /* column lengths of the pair and triple stages
                                  (ncy or a mixed length 16 m <= ncy)         */
+  int ncx_pair;               /* row length of the pair stages (<= ncx)     */
 } gl_plan_info;
 
 /* Create a plan: validates the descriptor, picks the product grid, builds

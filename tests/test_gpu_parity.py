@@ -183,6 +183,34 @@ def test_mixed_column_grids_match_oracle(order, h, n, pair, triple):
         assert err < 1e-9, name
 
 
+# (order, parent box width, grid, expected pair row length): the mixed row
+# lengths of the pair-stage row kernels (144, 160, 192, 240), reached through
+# wide parent boxes (the pair box is 2w - 1 wide).
+MIXED_ROW_CASES = [
+    (2, 70, 512, 144), (2, 76, 512, 160), (2, 90, 512, 192), (2, 110, 512, 240),
+    (3, 70, 512, 144), (3, 76, 512, 160),
+]
+
+
+@pytest.mark.parametrize("order,w,n,pair_row", MIXED_ROW_CASES)
+def test_mixed_row_grids_match_oracle(order, w, n, pair_row):
+    """Pair-stage rows on the mixed lengths 16 m reproduce the oracle on the
+    reference grid."""
+    st = _box_state(order, 5, n, seed=w, w=w)
+    t = 0.3
+    c = gl_engine.gl_spectral_coefficients(order, st["gravity"], st["depth"], st["a"], st["b"],
+                                           st["kx"], st["ky"], 0, 0, {"eta22_rank": 4})
+    _, _, _, _, comps, audit = gl_engine.gl_spectral_surface(c, st["lx"], st["ly"], n, n, t)
+    assert audit["engine"]["pair_row_length"] == pair_row
+    oc = O.spectral_coefficients(order, st["gravity"], st["depth"], st["a"], st["b"], st["kx"],
+                                 st["ky"], options={"eta22_rank": 4})
+    ref = O.spectral_surface(oc, st["lx"], st["ly"], n, n, t)
+    for name in COMPS[2: 2 * order]:
+        err = rel(comps[name + "_plus"], ref[name + "_plus"])
+        print(f"order {order} w {w} (rows {pair_row}) {name}: {err:.3e}")
+        assert err < 1e-9, name
+
+
 def test_compact_and_reference_grids_agree():
     st = seastate.small_order3(seed=7, n=64, modes=12)
     c = gl_engine.gl_spectral_coefficients(3, st.gravity, st.depth, st.a, st.b, st.kx, st.ky,
