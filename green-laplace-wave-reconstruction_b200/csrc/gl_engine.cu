@@ -1194,27 +1194,42 @@ static gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, c
 }
 
 template <int K, int MIX = 0>
-static void row_launch(dim3 grid, int threads, size_t smem, cudaStream_t st, const RowArgs& a,
+static void row_launch(dim3 grid, int T, size_t smem, cudaStream_t st, const RowArgs& a,
                        const cplx* tw) {
   static bool attr = false;
   if (!attr) {  // a failure here surfaces as the launch's own error
     attr = cudaFuncSetAttribute(row_kernel_t<K, MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)ROW_SMEM_LIMIT) == cudaSuccess;
   }
+  int nb = 0;
+  for (int g = 0; g < a.ngrp; ++g) nb += a.grp[g].nb;
+  // 8 transform groups per block when the row has at most 12 banks (4
+  // blocks fit per SM), 16 for wider rows (2 per SM by shared memory); a
+  // forward row with more than 16 banks (the order-3 outer row: 21) gets the
+  // fewest whole-warp groups that keep its rounds (12: the same rounds with
+  // fewer idle groups measured 6 % faster; more resident blocks for the
+  // 12-bank rows measured slower)
+  int G = nb <= 12 ? 8 : 16;
+  if (K == ROW_OUTER && nb > 16) {
+    const int rounds = (nb + 15) / 16;
+    G = (nb + rounds - 1) / rounds;
+    while ((G * T) % 32 != 0) ++G;
+  }
+  const int threads = std::max(32, std::min(256, G * T));
   row_kernel_t<K, MIX><<<grid, threads, smem, st>>>(a, tw);
 }
 
 // Pair-stage rows also run on the mixed row lengths 144, 160, 192, 240
 // (row_len); each is its own instantiation.
 template <int K>
-static bool row_launch_mixed(dim3 grid, int threads, size_t smem, cudaStream_t st, const RowArgs& a,
+static bool row_launch_mixed(dim3 grid, int T, size_t smem, cudaStream_t st, const RowArgs& a,
                              const cplx* tw) {
   switch (mixed_len(a.nx) ? a.nx / 16 : 0) {
-    case 0: row_launch<K, 0>(grid, threads, smem, st, a, tw); return true;
-    case 9: row_launch<K, 9>(grid, threads, smem, st, a, tw); return true;
-    case 10: row_launch<K, 10>(grid, threads, smem, st, a, tw); return true;
-    case 12: row_launch<K, 12>(grid, threads, smem, st, a, tw); return true;
-    case 15: row_launch<K, 15>(grid, threads, smem, st, a, tw); return true;
+    case 0: row_launch<K, 0>(grid, T, smem, st, a, tw); return true;
+    case 9: row_launch<K, 9>(grid, T, smem, st, a, tw); return true;
+    case 10: row_launch<K, 10>(grid, T, smem, st, a, tw); return true;
+    case 12: row_launch<K, 12>(grid, T, smem, st, a, tw); return true;
+    case 15: row_launch<K, 15>(grid, T, smem, st, a, tw); return true;
   }
   return false;
 }
@@ -1227,11 +1242,8 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
   if (smem > ROW_SMEM_LIMIT)
     return fail(GL_ERR_UNSUPPORTED, "row stage of %d banks x %d exceeds the shared-memory budget", nb, a.nx);
   dim3 grid(a.ny, njobs);
-  // 8 transform groups per block (n/16 threads each) when the row has at
-  // most 12 banks (4 blocks fit per SM by shared memory), 16 for the wider
-  // outer stage (2 blocks per SM); at least one warp
-  const int T = is_pow2(a.nx) ? a.nx / 16 : 16;  // threads per row transform
-  const int threads = std::max(32, std::min(256, (nb <= 12 ? 8 : 16) * T));
+  // threads per row transform; row_launch() sets the groups per block
+  const int T = is_pow2(a.nx) ? a.nx / 16 : 16;
   const bool pair_kind = a.kind == ROW_ETA22 || a.kind == ROW_PSI22 || a.kind == ROW_CONTACT22 ||
                          a.kind == ROW_INNER;
   if (!is_pow2(a.nx) && !pair_kind)
@@ -1249,18 +1261,18 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
   LaunchScope ls(name, st, bytes);
   bool ok = true;
   switch (a.kind) {
-    case ROW_ETA22: ok = row_launch_mixed<ROW_ETA22>(grid, threads, smem, st, a, tw); break;
-    case ROW_PSI22: ok = row_launch_mixed<ROW_PSI22>(grid, threads, smem, st, a, tw); break;
-    case ROW_CONTACT22: ok = row_launch_mixed<ROW_CONTACT22>(grid, threads, smem, st, a, tw); break;
-    case ROW_INNER: ok = row_launch_mixed<ROW_INNER>(grid, threads, smem, st, a, tw); break;
-    case ROW_OUTER: row_launch<ROW_OUTER>(grid, threads, smem, st, a, tw); break;
-    case ROW_E44_PAIR: row_launch<ROW_E44_PAIR>(grid, threads, smem, st, a, tw); break;
-    case ROW_E44_THIRD: row_launch<ROW_E44_THIRD>(grid, threads, smem, st, a, tw); break;
-    case ROW_E44_ORDER4: row_launch<ROW_E44_ORDER4>(grid, threads, smem, st, a, tw); break;
-    case ROW_E44_ORDER4_PSI: row_launch<ROW_E44_ORDER4_PSI>(grid, threads, smem, st, a, tw); break;
-    case ROW_ADJ_ETA22: row_launch<ROW_ADJ_ETA22>(grid, threads, smem, st, a, tw); break;
-    case ROW_ADJ_INNER: row_launch<ROW_ADJ_INNER>(grid, threads, smem, st, a, tw); break;
-    case ROW_ADJ_OUTER: row_launch<ROW_ADJ_OUTER>(grid, threads, smem, st, a, tw); break;
+    case ROW_ETA22: ok = row_launch_mixed<ROW_ETA22>(grid, T, smem, st, a, tw); break;
+    case ROW_PSI22: ok = row_launch_mixed<ROW_PSI22>(grid, T, smem, st, a, tw); break;
+    case ROW_CONTACT22: ok = row_launch_mixed<ROW_CONTACT22>(grid, T, smem, st, a, tw); break;
+    case ROW_INNER: ok = row_launch_mixed<ROW_INNER>(grid, T, smem, st, a, tw); break;
+    case ROW_OUTER: row_launch<ROW_OUTER>(grid, T, smem, st, a, tw); break;
+    case ROW_E44_PAIR: row_launch<ROW_E44_PAIR>(grid, T, smem, st, a, tw); break;
+    case ROW_E44_THIRD: row_launch<ROW_E44_THIRD>(grid, T, smem, st, a, tw); break;
+    case ROW_E44_ORDER4: row_launch<ROW_E44_ORDER4>(grid, T, smem, st, a, tw); break;
+    case ROW_E44_ORDER4_PSI: row_launch<ROW_E44_ORDER4_PSI>(grid, T, smem, st, a, tw); break;
+    case ROW_ADJ_ETA22: row_launch<ROW_ADJ_ETA22>(grid, T, smem, st, a, tw); break;
+    case ROW_ADJ_INNER: row_launch<ROW_ADJ_INNER>(grid, T, smem, st, a, tw); break;
+    case ROW_ADJ_OUTER: row_launch<ROW_ADJ_OUTER>(grid, T, smem, st, a, tw); break;
     default: return fail(GL_ERR_INVALID_ARGUMENT, "unknown row kind %d", a.kind);
   }
   if (!ok) return fail(GL_ERR_UNSUPPORTED, "row length %d has no transform", a.nx);
