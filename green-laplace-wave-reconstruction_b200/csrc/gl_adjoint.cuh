@@ -110,6 +110,8 @@ GL_D double cmb_damping(const CmbArgs& a, int job, double nu) {
 // sign by groups of n/16 threads in parallel, and each box bin then sums its
 // banks' multiplied values in bank order (deterministic) into the bank's
 // output spectrum, with the job's damping, the scale and the mask applied.
+// MIX = m > 0: columns of the mixed length 16 m.
+template <int MIX>
 __global__ void __launch_bounds__(256, 2) col_combine_kernel(CmbArgs a, const cplx* __restrict__ tw,
                                                             int cw) {
   extern __shared__ cplx smem[];
@@ -140,7 +142,7 @@ __global__ void __launch_bounds__(256, 2) col_combine_kernel(CmbArgs a, const cp
     cplx* buf = smem + (size_t)((rr / ncol) * cw + rr % ncol) * L;
     auto load = [&](int yb) -> cplx { return buf[phys(yb)]; };
     auto store = [&](int yb, cplx v) { buf[phys(yb)] = v; };
-    fft_row<+1>(buf, f, active, tw, load, store);
+    fft_row<+1, MIX>(buf, f, active, tw, load, store);
   }
   __syncthreads();
   const unsigned char* mask = a.mask ? a.mask + (size_t)unit * plane : nullptr;
@@ -148,7 +150,7 @@ __global__ void __launch_bounds__(256, 2) col_combine_kernel(CmbArgs a, const cp
   for (int t = threadIdx.x; t < ncol * h; t += blockDim.x) {
     const int c = t % ncol, by = t / ncol;
     const int i = by * a.box.w + x_first + c;
-    const int yb = phys(wrap(a.box.y0 + by, n));
+    const int yb = phys(wrap_any(a.box.y0 + by, n));
     const GeoRef geo{a.geo, plane, i};
     cplx acc0 = czero(), acc1 = czero(), acc2 = czero(), acc3 = czero();
     for (int k = 0; k < nb; ++k) {

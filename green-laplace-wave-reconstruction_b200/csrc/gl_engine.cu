@@ -1245,7 +1245,7 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
   // threads per row transform; row_launch() sets the groups per block
   const int T = is_pow2(a.nx) ? a.nx / 16 : 16;
   const bool pair_kind = a.kind == ROW_ETA22 || a.kind == ROW_PSI22 || a.kind == ROW_CONTACT22 ||
-                         a.kind == ROW_INNER;
+                         a.kind == ROW_INNER || a.kind == ROW_ADJ_ETA22 || a.kind == ROW_ADJ_INNER;
   if (!is_pow2(a.nx) && !pair_kind)
     return fail(GL_ERR_UNSUPPORTED, "row kind %d runs power-of-two rows only (got %d)", a.kind, a.nx);
   double bytes = (double)njobs * a.nout * a.out_w * a.ny * sizeof(cplx);
@@ -1270,8 +1270,8 @@ static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const 
     case ROW_E44_THIRD: row_launch<ROW_E44_THIRD>(grid, T, smem, st, a, tw); break;
     case ROW_E44_ORDER4: row_launch<ROW_E44_ORDER4>(grid, T, smem, st, a, tw); break;
     case ROW_E44_ORDER4_PSI: row_launch<ROW_E44_ORDER4_PSI>(grid, T, smem, st, a, tw); break;
-    case ROW_ADJ_ETA22: row_launch<ROW_ADJ_ETA22>(grid, T, smem, st, a, tw); break;
-    case ROW_ADJ_INNER: row_launch<ROW_ADJ_INNER>(grid, T, smem, st, a, tw); break;
+    case ROW_ADJ_ETA22: ok = row_launch_mixed<ROW_ADJ_ETA22>(grid, T, smem, st, a, tw); break;
+    case ROW_ADJ_INNER: ok = row_launch_mixed<ROW_ADJ_INNER>(grid, T, smem, st, a, tw); break;
     case ROW_ADJ_OUTER: row_launch<ROW_ADJ_OUTER>(grid, T, smem, st, a, tw); break;
     default: return fail(GL_ERR_INVALID_ARGUMENT, "unknown row kind %d", a.kind);
   }
@@ -2903,6 +2903,16 @@ static gl_status launch_seed_rows(const SeedArgs& a, int nunits, cudaStream_t st
   return GL_OK;
 }
 
+template <int MIX>
+static void combine_launch(dim3 grid, size_t smem, cudaStream_t st, const CmbArgs& a, const cplx* tw, int cw) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(col_combine_kernel<MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    attr = true;
+  }
+  col_combine_kernel<MIX><<<grid, 256, smem, st>>>(a, tw, cw);
+}
+
 static gl_status launch_combine(const CmbArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
   // columns per block: all banks of `cw` columns staged at once, within
   // ~110 KB of shared memory (two blocks per SM)
@@ -2911,16 +2921,12 @@ static gl_status launch_combine(const CmbArgs& a, int njobs, cudaStream_t st, co
   const size_t smem = (size_t)cw * col_bytes;
   if (smem > SMEM_LIMIT) return fail(GL_ERR_UNSUPPORTED, "adjoint column stage exceeds shared memory");
   if (a.nout < 1 || a.nout > 4) return fail(GL_ERR_INVALID_ARGUMENT, "adjoint column stage: 1..4 outputs");
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(col_combine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    attr = true;
-  }
+  if (!is_pow2(a.n) && !mixed_len(a.n)) return fail(GL_ERR_UNSUPPORTED, "column length %d has no transform", a.n);
   dim3 grid((a.box.w + cw - 1) / cw, njobs);
   const double bytes = (double)njobs * a.nbanks * a.box.w * a.n * sizeof(cplx) +
                        (double)njobs * a.nout * a.box.w * a.box.h * sizeof(cplx);
   LaunchScope ls("col_combine_kernel", st, bytes);
-  col_combine_kernel<<<grid, 256, smem, st>>>(a, tw, cw);
+  GL_MIX_DISPATCH(a.n, combine_launch, grid, smem, st, a, tw, cw);
   LAUNCH_CHECK("col_combine_kernel");
   return GL_OK;
 }
@@ -2955,8 +2961,15 @@ static gl_status adj_seed(gl_plan* p, int gu, const double* resid, const Box& bo
 
 // Adjoint column stage: + or - sign column transforms of `nb` adjoint
 // spectra per job (COL_PLAIN, the transposed forward transform).
-static gl_status adj_cols(gl_plan* p, const Box& box, const double* geo, const cplx* spec, int nb,
-                          int njobs, cplx* out, cudaStream_t st) {
+// Product grid of one adjoint segment (column transform -> rows -> column
+// combine): the pair stages run on (ncx2, ncy2), the triple stage on
+// (ncx, ncy3), like the forward stages they transpose.
+struct AdjGrid {
+  int nx, lnx, ny, lny;
+};
+
+static gl_status adj_cols(gl_plan* p, const AdjGrid& gr, const Box& box, const double* geo,
+                          const cplx* spec, int nb, int njobs, cplx* out, cudaStream_t st) {
   ColArgs a;
   std::memset(&a, 0, sizeof a);
   a.kind = COL_PLAIN;
@@ -2972,16 +2985,16 @@ static gl_status adj_cols(gl_plan* p, const Box& box, const double* geo, const c
   a.spec_sub_stride = (long long)box.w * box.h;
   a.jobs_per_unit = 1;
   a.out = out;
-  a.n = p->ncy;
-  a.log2n = p->lncy;
-  a.scale = ((double)p->d.nx * (double)p->d.ny) / ((double)p->ncx * (double)p->ncy);
+  a.n = gr.ny;
+  a.log2n = gr.lny;
+  a.scale = ((double)p->d.nx * (double)p->d.ny) / ((double)gr.nx * (double)gr.ny);
   a.conj_io = 1;
   return launch_col_ifft(a, njobs, st, p->tw);
 }
 
-static CmbArgs cmb_args(gl_plan* p, int kind, int nb, const int* mults, const int* dsts, int nout,
-                        const Box& box, const double* geo, const cplx* in, cplx* out,
-                        const UnitScalars* us, int jobs_per_unit) {
+static CmbArgs cmb_args(gl_plan* p, const AdjGrid& gr, int kind, int nb, const int* mults,
+                        const int* dsts, int nout, const Box& box, const double* geo, const cplx* in,
+                        cplx* out, const UnitScalars* us, int jobs_per_unit) {
   CmbArgs a;
   std::memset(&a, 0, sizeof a);
   a.kind = kind;
@@ -2995,8 +3008,8 @@ static CmbArgs cmb_args(gl_plan* p, int kind, int nb, const int* mults, const in
   a.geo = geo;
   a.in = in;
   a.out = out;
-  a.n = p->ncy;
-  a.log2n = p->lncy;
+  a.n = gr.ny;
+  a.log2n = gr.lny;
   a.scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
   a.us = us;
   a.jobs_per_unit = jobs_per_unit;
@@ -3014,9 +3027,12 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
   unsigned char* s3 = at<unsigned char>(ws, p->o_s3);
   char* base = at<char>(ws, p->o_scratch);
   const double* dn = p->nodes;
-  const int ncy = p->ncy;
-  const double fwd_scale = ((double)p->d.nx * (double)p->d.ny) / ((double)p->ncx * (double)p->ncy);
   const double inv_scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
+  // pair segments on (ncx2, ncy2), the triple segment on (ncx, ncy3)
+  const AdjGrid G2{p->ncx2, p->lncx2, p->ncy2, p->lncy2};
+  const AdjGrid G3{p->ncx, p->lncx, p->ncy3, p->lncy3};
+  const double fwd2 = ((double)p->d.nx * (double)p->d.ny) / ((double)G2.nx * (double)G2.ny);
+  const double fwd3 = ((double)p->d.nx * (double)p->d.ny) / ((double)G3.nx * (double)G3.ny);
   const AdjLayout L = adj_layout(p, p->group);
   cplx* E1 = reinterpret_cast<cplx*>(base + L.e1);
   cplx* E2 = reinterpret_cast<cplx*>(base + L.e2);
@@ -3062,8 +3078,8 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
     a.us = us;
     a.nodes = dn + 0 * MAX_RANK;
     a.out = P;
-    a.n = ncy;
-    a.log2n = p->lncy;
+    a.n = G2.ny;
+    a.log2n = G2.lny;
     a.scale = inv_scale;
     if ((s = launch_col_ifft(a, nj, st, p->tw)) != GL_OK) return s;
     RowArgs r;
@@ -3075,9 +3091,9 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
     r.out_x0 = B2.x0;
     r.out_w = B2.w;
     r.out = Q;
-    r.nx = p->ncx;
-    r.log2nx = p->lncx;
-    r.ny = ncy;
+    r.nx = G2.nx;
+    r.log2nx = G2.lnx;
+    r.ny = G2.ny;
     r.us = us;
     r.jobs_per_unit = J;
     r.gmax = ROW_GMAX;
@@ -3086,13 +3102,13 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
     f.in = Q;
     f.out = R;
     f.box = B2;
-    f.n = ncy;
-    f.log2n = p->lncy;
+    f.n = G2.ny;
+    f.log2n = G2.lny;
     f.nsrc = 2;
     f.jobs_per_unit = J;
     f.mask = s2;
     f.maxslot = mx;
-    f.scale = fwd_scale;
+    f.scale = fwd2;
     if ((s = launch_col_fft(f, nj * 2, st, p->tw)) != GL_OK) return s;
     // adjoint node spectra -> adjoint fields -> transposed products
     AdjArgs aa;
@@ -3115,7 +3131,7 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
       adj_eta22_kernel<<<g, T, 0, st>>>(aa);
     }
     LAUNCH_CHECK("adj_eta22_kernel");
-    if ((s = adj_cols(p, B2, p->geo2, RA, 2, nj, Q, st)) != GL_OK) return s;
+    if ((s = adj_cols(p, G2, B2, p->geo2, RA, 2, nj, Q, st)) != GL_OK) return s;
     RowArgs ra;
     std::memset(&ra, 0, sizeof ra);
     ra.kind = ROW_ADJ_ETA22;
@@ -3127,14 +3143,14 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
     ra.out_w = B1.w;
     ra.out = QA;
     ra.out_conj = 1;
-    ra.nx = p->ncx;
-    ra.log2nx = p->lncx;
-    ra.ny = ncy;
+    ra.nx = G2.nx;
+    ra.log2nx = G2.lnx;
+    ra.ny = G2.ny;
     ra.us = us;
     ra.jobs_per_unit = J;
     ra.gmax = ROW_GMAX;
     if ((s = launch_row(ra, nj, st, p->tw)) != GL_OK) return s;
-    CmbArgs c = cmb_args(p, CMB_ETA22, 8, m8, nullptr, 1, B1, p->geo1, QA, DA22, us, J);
+    CmbArgs c = cmb_args(p, G2, CMB_ETA22, 8, m8, nullptr, 1, B1, p->geo1, QA, DA22, us, J);
     c.nodes = dn + 0 * MAX_RANK;
     if ((s = launch_combine(c, nj, st, p->tw)) != GL_OK) return s;
   }
@@ -3187,8 +3203,8 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
       a.n_inner = I;
       a.n_outer = Jo;
       a.out = PI;
-      a.n = ncy;
-      a.log2n = p->lncy;
+      a.n = G2.ny;
+      a.log2n = G2.lny;
       a.scale = inv_scale;
       if ((s = launch_col_ifft(a, nj, st, p->tw)) != GL_OK) return s;
       RowArgs r;
@@ -3200,9 +3216,9 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
       r.out_x0 = B2.x0;
       r.out_w = B2.w;
       r.out = QI;
-      r.nx = p->ncx;
-      r.log2nx = p->lncx;
-      r.ny = ncy;
+      r.nx = G2.nx;
+      r.log2nx = G2.lnx;
+      r.ny = G2.ny;
       r.us = us;
       r.jobs_per_unit = Jo * I;
       r.gmax = ROW_GMAX;
@@ -3211,13 +3227,13 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
       f.in = QI;
       f.out = RI;
       f.box = B2;
-      f.n = ncy;
-      f.log2n = p->lncy;
+      f.n = G2.ny;
+      f.log2n = G2.lny;
       f.nsrc = 4;
       f.jobs_per_unit = Jo * I;
       f.mask = s2;
       f.maxslot = maxRI;
-      f.scale = fwd_scale;
+      f.scale = fwd2;
       if ((s = launch_col_fft(f, nj * 4, st, p->tw)) != GL_OK) return s;
       AccArgs c;
       std::memset(&c, 0, sizeof c);
@@ -3257,8 +3273,8 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
       a.us = us;
       a.nodes = dn + 3 * MAX_RANK;
       a.out = P1;
-      a.n = ncy;
-      a.log2n = p->lncy;
+      a.n = G3.ny;
+      a.log2n = G3.lny;
       a.scale = inv_scale;
       if ((s = launch_col_ifft(a, nuj, st, p->tw)) != GL_OK) return s;
       ColArgs a2;
@@ -3279,8 +3295,8 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
       a2.floor_max = maxEt;
       a2.floor_rel = p->floor_rel;
       a2.out = P2;
-      a2.n = ncy;
-      a2.log2n = p->lncy;
+      a2.n = G3.ny;
+      a2.log2n = G3.lny;
       a2.scale = inv_scale;
       if ((s = launch_col_ifft(a2, nuj, st, p->tw)) != GL_OK) return s;
       RowArgs r;
@@ -3293,9 +3309,9 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
       r.out_x0 = B3.x0;
       r.out_w = B3.w;
       r.out = QO;
-      r.nx = p->ncx;
-      r.log2nx = p->lncx;
-      r.ny = ncy;
+      r.nx = G3.nx;
+      r.log2nx = G3.lnx;
+      r.ny = G3.ny;
       r.us = us;
       r.jobs_per_unit = Jo;
       r.gmax = ROW_GMAX;
@@ -3304,13 +3320,13 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
       f.in = QO;
       f.out = RO;
       f.box = B3;
-      f.n = ncy;
-      f.log2n = p->lncy;
+      f.n = G3.ny;
+      f.log2n = G3.lny;
       f.nsrc = 2;
       f.jobs_per_unit = Jo;
       f.mask = s3;
       f.maxslot = maxRO;
-      f.scale = fwd_scale;
+      f.scale = fwd3;
       if ((s = launch_col_fft(f, nuj * 2, st, p->tw)) != GL_OK) return s;
     }
     // adjoint outer stage: forcing adjoints -> first-order and pair adjoints
@@ -3335,7 +3351,7 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
         adj_outer_kernel<<<g, T, 0, st>>>(aa);
       }
       LAUNCH_CHECK("adj_outer_kernel");
-      if ((s = adj_cols(p, B3, p->geo3, RAo, 2, nuj, QO, st)) != GL_OK) return s;
+      if ((s = adj_cols(p, G3, B3, p->geo3, RAo, 2, nuj, QO, st)) != GL_OK) return s;
       RowArgs ra;
       std::memset(&ra, 0, sizeof ra);
       ra.kind = ROW_ADJ_OUTER;
@@ -3352,17 +3368,17 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
       ra.out2_w = B2.w;
       ra.out2 = QA2;
       ra.out_conj = 1;
-      ra.nx = p->ncx;
-      ra.log2nx = p->lncx;
-      ra.ny = ncy;
+      ra.nx = G3.nx;
+      ra.log2nx = G3.lnx;
+      ra.ny = G3.ny;
       ra.us = us;
       ra.jobs_per_unit = Jo;
       ra.gmax = ROW_GMAX;
       if ((s = launch_row(ra, nuj, st, p->tw)) != GL_OK) return s;
-      CmbArgs c1 = cmb_args(p, CMB_FIRST3, 12, m1, nullptr, 1, B1, p->geo1, QA1, DA1, us, Jo);
+      CmbArgs c1 = cmb_args(p, G3, CMB_FIRST3, 12, m1, nullptr, 1, B1, p->geo1, QA1, DA1, us, Jo);
       c1.nodes = dn + 3 * MAX_RANK;
       if ((s = launch_combine(c1, nuj, st, p->tw)) != GL_OK) return s;
-      CmbArgs c2 = cmb_args(p, CMB_PAIR, 8, m9, src9, 4, B2, p->geo2, QA2, EA, us, Jo);
+      CmbArgs c2 = cmb_args(p, G3, CMB_PAIR, 8, m9, src9, 4, B2, p->geo2, QA2, EA, us, Jo);
       c2.mask = s2;
       if ((s = launch_combine(c2, nuj, st, p->tw)) != GL_OK) return s;
     }
@@ -3389,7 +3405,7 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
         adj_inner_kernel<<<g, T, 0, st>>>(aa);
       }
       LAUNCH_CHECK("adj_inner_kernel");
-      if ((s = adj_cols(p, B2, p->geo2, RAi, 4, nj, QI, st)) != GL_OK) return s;
+      if ((s = adj_cols(p, G2, B2, p->geo2, RAi, 4, nj, QI, st)) != GL_OK) return s;
       RowArgs ra;
       std::memset(&ra, 0, sizeof ra);
       ra.kind = ROW_ADJ_INNER;
@@ -3401,14 +3417,14 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
       ra.out_w = B1.w;
       ra.out = QAi;
       ra.out_conj = 1;
-      ra.nx = p->ncx;
-      ra.log2nx = p->lncx;
-      ra.ny = ncy;
+      ra.nx = G2.nx;
+      ra.log2nx = G2.lnx;
+      ra.ny = G2.ny;
       ra.us = us;
       ra.jobs_per_unit = Jo * I;
       ra.gmax = ROW_GMAX;
       if ((s = launch_row(ra, nj, st, p->tw)) != GL_OK) return s;
-      CmbArgs c = cmb_args(p, CMB_INNER, 12, mi, nullptr, 1, B1, p->geo1, QAi, DAI, us, Jo * I);
+      CmbArgs c = cmb_args(p, G2, CMB_INNER, 12, mi, nullptr, 1, B1, p->geo1, QAi, DAI, us, Jo * I);
       c.nodes = dn + 3 * MAX_RANK;
       c.nodes2 = dn + 2 * MAX_RANK;
       c.n_inner = I;
