@@ -684,6 +684,7 @@ struct gl_plan {
   // forward row length of the pair stages (power of two or 144/160/192/240,
   // <= ncx: their products need a period covering only the pair box)
   int ncx2, lncx2;
+  int ncx3 = 0;  // eta44 third-level row length (power of two covering B3)
   Box b1, b2, b3;
   int ww1, ww2;                 // bitset words per row (S1, S2)
   bool want_eta22, want_psi22, want_o3, want_first;
@@ -1025,9 +1026,9 @@ extern "C" gl_status gl_plan_get_info(const gl_plan* p, gl_plan_info* info) {
   std::memset(info, 0, sizeof *info);
   info->ncx = p->ncx;
   info->ncy = p->ncy;
-  info->ncy_pair = p->e44 ? p->ncy : p->ncy2;
-  info->ncy_triple = p->e44 ? p->ncy : p->ncy3;
-  info->ncx_pair = p->e44 ? p->ncx : p->ncx2;
+  info->ncy_pair = p->ncy2;
+  info->ncy_triple = p->ncy3;
+  info->ncx_pair = p->ncx2;
   const Box* bs[3] = {&p->b1, &p->b2, &p->b3};
   int* dst[3] = {info->box1, info->box2, info->box3};
   for (int k = 0; k < 3; ++k) {
@@ -2167,6 +2168,16 @@ extern "C" gl_status gl_eta44_plan_create(gl_plan** out, const gl_eta44_desc* de
   p->lncx = ilog2(p->ncx);
   p->lncy = ilog2(p->ncy);
   p->lnx = p->lny = ilog2(e.n);
+  // pair and third stages: rows a power of two covering B2 / B3 (the order-4
+  // row kernels run powers of two), columns the shortest length covering
+  // B2 / B3 that the column kernels run
+  p->ncx2 = std::min(p->ncx, std::max(16, next_pow2(p->b2.w)));
+  p->ncy2 = std::min(p->ncy, col_len(p->b2.h));
+  p->ncx3 = std::min(p->ncx, std::max(16, next_pow2(p->b3.w)));
+  p->ncy3 = std::min(p->ncy, col_len(p->b3.h));
+  p->lncx2 = col_log2(p->ncx2);
+  p->lncy2 = col_log2(p->ncy2);
+  p->lncy3 = col_log2(p->ncy3);
   const int row_banks = want_psi ? 46 : 45;
   if (row_smem(row_banks, p->ncx) > ROW_SMEM_LIMIT) {
     plan_free(p);
@@ -2464,9 +2475,20 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     }
     LAUNCH_CHECK("scalars_kernel");
   }
-  const double fwd_scale = ((double)p->d.nx * (double)p->d.ny) / ((double)p->ncx * (double)p->ncy);
   const double inv_scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
-  const int ncy = p->ncy;
+  // Product grid of each stage: the pair stage only forms products of two
+  // first-order fields and the third stage of three, so they run on grids
+  // covering B2 and B3 (rows a power of two, columns a power of two or a
+  // mixed length 16 m); the order-4 stage on the plan's grid covering B4.
+  struct StageGrid {
+    int nx, lnx, ny, lny;
+    double fwd;  // (Nx Ny)/(nx ny): forward-transform scale
+  };
+  auto stage_grid = [&](int nx, int ny) {
+    return StageGrid{nx, col_log2(nx), ny, col_log2(ny),
+                     ((double)p->d.nx * (double)p->d.ny) / ((double)nx * (double)ny)};
+  };
+  StageGrid cur = stage_grid(p->ncx, p->ncy);
   const int JP = Ro * R * R + Ro * R, GP = Ro * R + Ro;
   const bool psi = p->e44_psi;
   const int nts = psi ? 4 : 3;   // third-state spectra: es, ps, pts [, ets]
@@ -2500,8 +2522,8 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     a.outer0 = o0;
     a.floor_rel = p->floor_rel;
     a.out = outp;
-    a.n = ncy;
-    a.log2n = p->lncy;
+    a.n = cur.ny;
+    a.log2n = cur.lny;
     a.scale = inv_scale;
     return a;
   };
@@ -2513,9 +2535,9 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     r.out_x0 = outbox.x0;
     r.out_w = outbox.w;
     r.out = outp;
-    r.nx = p->ncx;
-    r.log2nx = p->lncx;
-    r.ny = ncy;
+    r.nx = cur.nx;
+    r.log2nx = cur.lnx;
+    r.ny = cur.ny;
     r.us = us;
     r.jobs_per_unit = 1;
     r.gmax = ROW_GMAX;
@@ -2527,22 +2549,23 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     f.in = in;
     f.out = outp;
     f.box = box;
-    f.n = ncy;
-    f.log2n = p->lncy;
+    f.n = cur.ny;
+    f.log2n = cur.lny;
     f.nsrc = nsrc;
     f.jobs_per_unit = jobs_per_unit;
     f.mask = mask;
     f.maxslot = mx;
-    f.scale = fwd_scale;
+    f.scale = cur.fwd;
     return launch_col_fft(f, njs, st, p->tw);
   };
 
   // ---- stage 1: every pair level (Ro R^2 third-level + Ro R order-4 pair jobs)
+  cur = stage_grid(p->ncx2, p->ncy2);
   {
     const int nj = gu * JP;
     Bump b;
-    cplx* P = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 16 * B1.w * ncy * sizeof(cplx)));
-    cplx* Q = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 6 * B2.w * ncy * sizeof(cplx)));
+    cplx* P = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 16 * B1.w * cur.ny * sizeof(cplx)));
+    cplx* Q = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 6 * B2.w * cur.ny * sizeof(cplx)));
     cplx* RP = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 6 * pl2 * sizeof(cplx)));
     unsigned long long* mRP = reinterpret_cast<unsigned long long*>(tr + b.take((size_t)nj * 6 * 8));
     CUDA_TRY(cudaMemsetAsync(mRP, 0, (size_t)nj * 6 * 8, st));
@@ -2578,12 +2601,13 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     LAUNCH_CHECK("acc_e44_pair_kernel");
   }
   // ---- stage 2: third level (Ro R jobs per unit)
+  cur = stage_grid(p->ncx3, p->ncy3);
   {
     const int nj = gu * Ro * R;
     Bump b;
-    cplx* PF = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 16 * B1.w * ncy * sizeof(cplx)));
-    cplx* PP = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 15 * B2.w * ncy * sizeof(cplx)));
-    cplx* Q = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 4 * B3.w * ncy * sizeof(cplx)));
+    cplx* PF = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 16 * B1.w * cur.ny * sizeof(cplx)));
+    cplx* PP = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 15 * B2.w * cur.ny * sizeof(cplx)));
+    cplx* Q = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 4 * B3.w * cur.ny * sizeof(cplx)));
     cplx* R3 = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 4 * pl3 * sizeof(cplx)));
     unsigned long long* mR3 = reinterpret_cast<unsigned long long*>(tr + b.take((size_t)nj * 4 * 8));
     CUDA_TRY(cudaMemsetAsync(mR3, 0, (size_t)nj * 4 * 8, st));
@@ -2594,7 +2618,7 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     for (int u = 0; u < gu; ++u) {
       ColArgs a2 = colargs(COL_FLOORED, 15, E44_POUT_MULT, E44_POUT_SRC, B2, p->geo2,
                            E + (size_t)u * GP * 5 * pl2, 5LL * pl2, pl2, Ro * R,
-                           PP + (size_t)u * Ro * R * 15 * B2.w * ncy);
+                           PP + (size_t)u * Ro * R * 15 * B2.w * cur.ny);
       a2.floor_max = maxE + (size_t)u * GP * 5;
       a2.floor_nsrc = 5;
       if ((s = launch_col_ifft(a2, Ro * R, st, p->tw)) != GL_OK) return s;
@@ -2630,14 +2654,15 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     LAUNCH_CHECK("acc_e44_third_kernel");
   }
   // ---- stage 3: order-4 forcing (Ro jobs per unit)
+  cur = stage_grid(p->ncx, p->ncy);
   {
     const int nj = gu * Ro;
     Bump b;
-    cplx* PF = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 19 * B1.w * ncy * sizeof(cplx)));
-    cplx* PP = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 18 * B2.w * ncy * sizeof(cplx)));
+    cplx* PF = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 19 * B1.w * cur.ny * sizeof(cplx)));
+    cplx* PP = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 18 * B2.w * cur.ny * sizeof(cplx)));
     const int ntb = nts + 5;  // third-state banks (8, or 9 with eta_t)
-    cplx* PT = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * ntb * B3.w * ncy * sizeof(cplx)));
-    cplx* Q = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * nf4 * B4.w * ncy * sizeof(cplx)));
+    cplx* PT = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * ntb * B3.w * cur.ny * sizeof(cplx)));
+    cplx* Q = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * nf4 * B4.w * cur.ny * sizeof(cplx)));
     cplx* R4 = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * nf4 * pl4 * sizeof(cplx)));
     unsigned long long* mR4 = reinterpret_cast<unsigned long long*>(tr + b.take((size_t)nj * nf4 * 8));
     CUDA_TRY(cudaMemsetAsync(mR4, 0, (size_t)nj * nf4 * 8, st));
@@ -2646,7 +2671,7 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     for (int u = 0; u < gu; ++u) {
       ColArgs a2 = colargs(COL_FLOORED, 18, E44_POUT_MULT, E44_POUT_SRC, B2, p->geo2,
                            E + ((size_t)u * GP + Ro * R) * 5 * pl2, 5LL * pl2, pl2, Ro,
-                           PP + (size_t)u * Ro * 18 * B2.w * ncy);
+                           PP + (size_t)u * Ro * 18 * B2.w * cur.ny);
       a2.floor_max = maxE + ((size_t)u * GP + Ro * R) * 5;
       a2.floor_nsrc = 5;
       if ((s = launch_col_ifft(a2, Ro, st, p->tw)) != GL_OK) return s;

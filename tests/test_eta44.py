@@ -6,7 +6,9 @@ from pathlib import Path
 
 import numpy as np
 import pytest
+import torch
 
+from gl_engine import _lib
 from gl_engine import eta44 as E44
 from gl_engine import wit
 from oracle import gl_eta44 as OE
@@ -58,6 +60,45 @@ def test_eta44_matches_cpu_restatement(seed, rank):
     err = rel(got, ref)
     print(f"seed {seed} GL{rank}: rel L2 {err:.3e}")
     assert err < 1e-9
+
+
+def _tall(seed, h, n=128, w=8, m=12):
+    """Modes filling a parent box w columns (mx = 1..w) by h rows."""
+    rng = np.random.default_rng(seed)
+    lo = -((h - 1) // 2)
+    cells = {(1, lo), (w, lo + h - 1)}
+    while len(cells) < m:
+        cells.add((int(rng.integers(1, w + 1)), int(rng.integers(lo, lo + h))))
+    modes = np.array(sorted(cells))
+    c = 0.01 * (rng.standard_normal(len(modes)) + 1j * rng.standard_normal(len(modes)))
+    return E44.spectrum_from_modes(modes, c, n, 1.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("h,pair_cols,third_cols", [(20, 48, 64), (25, 64, 80)])
+def test_eta44_stage_grids_match_cpu_restatement(h, pair_cols, third_cols):
+    """The pair and third stages on their own grids (columns of the mixed
+    lengths 48 = 3 x 16 and 80 = 5 x 16 here; the order-4 stage on 128)
+    reproduce the CPU restatement on the 128^2 grid."""
+    s = _tall(h, h)
+    box = E44._box(np.abs(s))
+    desc = _lib.Eta44Desc(n=128, dk=0.25, depth=1.0, peak_depth=1.0, rank=2, nodes=None,
+                          weights=None, box_x0=box[0], box_y0=box[1], box_w=box[2], box_h=box[3],
+                          max_units=1, output=_lib.OUT_COMPLEX, components=_lib.COMP_ETA44,
+                          gravity=1.0)
+    info = E44.Eta44Plan(desc, torch.device("cuda")).info
+    assert (info.ncy_pair, info.ncy_triple, info.ncy) == (pair_cols, third_cols, 128)
+    nodes, weights = O.gauss_laguerre(2)
+    ref = OE.eta44(s, 0.25, 1.0, 1.0, nodes, weights)
+    # the oracle's own answer under a 1-ulp change of its input: where the
+    # roundoff floor sits near some bins (h = 20 here) FP64 implementations
+    # that differ only in FFT roundoff spread by ~1e-9, the grid used or not
+    spread = rel(OE.eta44(s * (1 + 2.2e-16), 0.25, 1.0, 1.0, nodes, weights), ref)
+    got = E44.eta44(s, dk=0.25, depth=1.0, peak_depth=1.0, rank=2)
+    err = rel(got, ref)
+    print(f"h {h} (pair cols {pair_cols}, third cols {third_cols}): rel L2 {err:.3e}, "
+          f"oracle 1-ulp spread {spread:.3e}")
+    assert err < max(1e-9, 8 * spread)
 
 
 @pytest.mark.gpu
