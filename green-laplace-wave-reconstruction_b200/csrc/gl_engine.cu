@@ -1201,6 +1201,9 @@ static void row_launch(dim3 grid, int T, size_t smem, cudaStream_t st, const Row
   if (!attr) {  // a failure here surfaces as the launch's own error
     attr = cudaFuncSetAttribute(row_kernel_t<K, MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)ROW_SMEM_LIMIT) == cudaSuccess;
+    if constexpr (MIX == 0)
+      attr = attr && cudaFuncSetAttribute(row_kernel_t<K, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)ROW_SMEM_LIMIT) == cudaSuccess;
   }
   int nb = 0;
   for (int g = 0; g < a.ngrp; ++g) nb += a.grp[g].nb;
@@ -1216,8 +1219,27 @@ static void row_launch(dim3 grid, int T, size_t smem, cudaStream_t st, const Row
     G = (nb + rounds - 1) / rounds;
     while ((G * T) % 32 != 0) ++G;
   }
-  const int threads = std::max(32, std::min(256, G * T));
-  row_kernel_t<K, MIX><<<grid, threads, smem, st>>>(a, tw);
+  // Short rows (fewer than 16 threads per transform) carry little work per
+  // block, so a block takes several rows (one team of G groups each) while it
+  // stays within 256 threads and ~76 KB of shared memory (3 blocks per SM).
+  const int team = G * T;
+  int rpb = 1;
+  if (MIX == 0 && T < 16) {
+    int r = std::min(256 / std::max(1, team), (int)((76 * 1024) / std::max<size_t>(1, smem)));
+    while (r > 1 && (team * r) % 32 != 0) --r;
+    rpb = std::max(1, r);
+  }
+  const int threads = rpb > 1 ? team * rpb : std::max(32, std::min(256, team));
+  RowArgs b = a;
+  b.rpb = rpb;
+  dim3 g2((a.ny + rpb - 1) / rpb, grid.y);
+  if constexpr (MIX == 0) {
+    if (rpb > 1) {
+      row_kernel_t<K, 0, true><<<g2, threads, smem * rpb, st>>>(b, tw);
+      return;
+    }
+  }
+  row_kernel_t<K, MIX><<<g2, threads, smem, st>>>(b, tw);
 }
 
 // Pair-stage rows also run on the mixed row lengths 144, 160, 192, 240

@@ -337,6 +337,22 @@ struct FftGroup {
   GroupSync sync;
 };
 
+// Group geometry of thread tl of a team of `team` threads (a block, or one
+// row's share of a block that carries several rows) doing length-n
+// transforms; named barriers of the team's groups start at id_base.
+GL_D FftGroup fft_group_team(int n, int log2n, int tl, int team, int id_base, int& g, int& G) {
+  FftGroup f;
+  f.n = n;
+  f.log2n = log2n;
+  f.m = mixed_len(n) ? n >> 4 : 0;
+  f.T = f.m ? 16 : n >> 4;
+  G = team / f.T;
+  g = tl / f.T;
+  f.t = tl % f.T;
+  f.sync = GroupSync{f.T, id_base + g};
+  return f;
+}
+
 // Group geometry for a block of `threads` threads doing length-n transforms.
 GL_D FftGroup fft_group(int n, int log2n, int& g, int& G) {
   FftGroup f;

@@ -414,6 +414,7 @@ struct RowArgs {
   int nout_a;              // > 0: outputs [nout_a, nout) go to out2 instead
   int out2_x0, out2_w;
   cplx* out2;              // [job][nout - nout_a][out2_w][n_y]
+  int rpb;                 // rows per block (> 1 for short rows; 0 or 1: one)
 };
 
 // Pointwise products of each stage; `b` points at the bank rows (bank k at
@@ -764,19 +765,28 @@ GL_D void row_products_adj(int kind, cplx* b, int L, int p) {
 // stages, 2: order-4 stages (their rows are wider than 24 banks and are
 // staged in shared memory first).
 // MIX = m > 0: the row length is the mixed length 16 m (pair stages on a
-// product grid narrower than a power of two); 0: a power of two.
-template <int KIND, int MIX = 0>
+// product grid narrower than a power of two); 0: a power of two.  MULTI:
+// several short rows per block (RowArgs::rpb).
+template <int KIND, int MIX = 0, bool MULTI = false>
 __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __restrict__ tw) {
   constexpr int FAMILY = KIND >= ROW_ADJ_ETA22 ? 1 : (KIND >= ROW_E44_PAIR && KIND <= ROW_E44_ORDER4_PSI ? 2 : 0);
   extern __shared__ __align__(128) cplx smem[];
   __shared__ __align__(8) unsigned long long stage_bar;
-  const int y = blockIdx.x;
+  // MULTI: a.rpb rows per block, each row with its own team of
+  // blockDim.x / rpb threads and its own nb bank rows of shared memory
+  const int rpb = MULTI && a.rpb > 1 ? a.rpb : 1;
+  const int team = blockDim.x / rpb;
+  const int rr = MULTI ? threadIdx.x / team : 0;
+  const int tl = MULTI ? threadIdx.x % team : threadIdx.x;
+  const int y0 = blockIdx.x * rpb;
+  const int y = y0 + rr;
+  const bool row_ok = !MULTI || y < a.ny;
   const int job = blockIdx.y;
   const int n = a.nx;
   const int L = padded_len(n);
   int nb = 0;
   for (int q = 0; q < a.ngrp; ++q) nb += a.grp[q].nb;
-  cplx* banks = smem;  // nb * L
+  cplx* banks = smem + (size_t)rr * nb * L;  // this row's nb * L
   // Stage every bank's box row (w contiguous values) into the front of the
   // bank's own row buffer with bulk async copies, all issued at block start,
   // so the later transform rounds find their inputs in shared memory.  The
@@ -786,16 +796,21 @@ __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __
   if (threadIdx.x == 0) mbar_init(bar, 1);
   __syncthreads();
   if (threadIdx.x == 0) {
+    const int nrows = MULTI ? min(rpb, a.ny - y0) : 1;
     uint32_t bytes = 0;
     for (int q = 0; q < a.ngrp; ++q) bytes += (uint32_t)(a.grp[q].nb * a.grp[q].w * sizeof(cplx));
-    mbar_arrive_expect_tx(bar, bytes);
-    int k0 = 0;
-    for (int q = 0; q < a.ngrp; ++q) {
-      const BankGroup& B = a.grp[q];
-      for (int kk = 0; kk < B.nb; ++kk)
-        bulk_g2s(smem_u32(banks + (size_t)(k0 + kk) * L), B.data + (((size_t)job * B.nb + kk) * a.ny + y) * B.w,
-                 (uint32_t)(B.w * sizeof(cplx)), bar);
-      k0 += B.nb;
+    mbar_arrive_expect_tx(bar, bytes * (uint32_t)nrows);
+    for (int r = 0; r < nrows; ++r) {
+      cplx* rb = smem + (size_t)r * nb * L;
+      int k0 = 0;
+      for (int q = 0; q < a.ngrp; ++q) {
+        const BankGroup& B = a.grp[q];
+        for (int kk = 0; kk < B.nb; ++kk)
+          bulk_g2s(smem_u32(rb + (size_t)(k0 + kk) * L),
+                   B.data + (((size_t)job * B.nb + kk) * a.ny + y0 + r) * B.w, (uint32_t)(B.w * sizeof(cplx)),
+                   bar);
+        k0 += B.nb;
+      }
     }
   }
   {
@@ -810,10 +825,10 @@ __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __
     }
   }
   int g, G;
-  const FftGroup f = fft_group(n, a.log2nx, g, G);
+  const FftGroup f = fft_group_team(n, a.log2nx, tl, team, 1 + rr * (team / (MIX ? 16 : (n >> 4))), g, G);
   for (int it = 0; it < (nb + G - 1) / G; ++it) {
     const int k = it * G + g;
-    const bool active = k < nb;
+    const bool active = k < nb && row_ok;
     cplx* buf = banks + (size_t)(active ? k : 0) * L;
     bool cj = false;
     int bx0 = 0, bw = 0;
@@ -839,27 +854,30 @@ __global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __
     fft_row<+1, MIX>(buf, f, active, tw, load, store);
   }
   __syncthreads();
-  if constexpr (FAMILY == 0) {
-    const int chan_count = KIND == ROW_PSI22 ? a.us[job / a.jobs_per_unit].chan_count : 0;
-    for (int p = threadIdx.x; p < n; p += blockDim.x) row_products(KIND, banks, L, phys(p), chan_count);
-  } else if constexpr (FAMILY == 2) {
-    for (int p = threadIdx.x; p < n; p += blockDim.x) row_products_e44(KIND, banks, L, phys(p));
-  } else {
-    for (int p = threadIdx.x; p < n; p += blockDim.x) row_products_adj(KIND, banks, L, phys(p));
+  if (row_ok) {
+    if constexpr (FAMILY == 0) {
+      const int chan_count = KIND == ROW_PSI22 ? a.us[job / a.jobs_per_unit].chan_count : 0;
+      for (int p = tl; p < n; p += team) row_products(KIND, banks, L, phys(p), chan_count);
+    } else if constexpr (FAMILY == 2) {
+      for (int p = tl; p < n; p += team) row_products_e44(KIND, banks, L, phys(p));
+    } else {
+      for (int p = tl; p < n; p += team) row_products_adj(KIND, banks, L, phys(p));
+    }
   }
   __syncthreads();
   const int na = a.nout_a > 0 ? a.nout_a : a.nout;
   const bool oc = FAMILY == 1 && a.out_conj != 0;
   for (int it = 0; it < (a.nout + G - 1) / G; ++it) {
     const int o = it * G + g;
-    const bool active = o < a.nout;
+    const bool active = o < a.nout && row_ok;
     const int oo = active ? o : 0;
     cplx* buf = banks + (size_t)oo * L;
     const bool second = oo >= na;
     const int ox0 = second ? a.out2_x0 : a.out_x0;
     const int ow = second ? a.out2_w : a.out_w;
-    cplx* orow = second ? a.out2 + (((size_t)job * (a.nout - na) + (oo - na)) * a.ny + y) * ow
-                        : a.out + (((size_t)job * na + oo) * a.ny + y) * ow;
+    const int yr = row_ok ? y : 0;
+    cplx* orow = second ? a.out2 + (((size_t)job * (a.nout - na) + (oo - na)) * a.ny + yr) * ow
+                        : a.out + (((size_t)job * na + oo) * a.ny + yr) * ow;
     auto load = [&](int xb) -> cplx {
       const cplx v = buf[phys(xb)];
       return oc ? cconj(v) : v;
