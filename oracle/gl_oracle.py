@@ -320,7 +320,7 @@ def psi22(spectrum: np.ndarray, qx: np.ndarray, qy: np.ndarray, *,
 
 
 # ---------------------------------------------------------------------------
-# order three (north-star graph)
+# order three (the eta33 + psi33 graph)
 # ---------------------------------------------------------------------------
 
 INNER_RANKS = (4, 6, 8, 10, 12)
