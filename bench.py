@@ -571,6 +571,12 @@ def run_config3(args, rank: int, world: int, local_rank: int) -> None:
     graph_s = timed(runner.replay)
     units = runner.units
     grids = sorted({it.nx for it in items})
+    # per-kernel breakdown: one profiled eager pass (events per launch)
+    _lib.profile_begin()
+    runner.run_eager()
+    torch.cuda.synchronize()
+    kstats = sorted(_lib.profile_end(), key=lambda r: -r["ms_total"])
+    ktot = sum(r["ms_total"] for r in kstats) or 1.0
     line = {
         "metric": "config-3 uneven batch units/s (captured graph)", "value": units * args.steps / graph_s,
         "unit": "units/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -581,6 +587,8 @@ def run_config3(args, rank: int, world: int, local_rank: int) -> None:
                    "units_per_step_per_gpu": units},
         "eager": {"value": units * args.steps / eager_s, "ms_per_step": 1e3 * eager_s / args.steps,
                   "kernel_launches_per_step": int(launches)},
+        "kernel_shares": [{"name": r["name"], "launches": r["launches"],
+                           "share": round(r["ms_total"] / ktot, 4)} for r in kstats[:10]],
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
