@@ -48,9 +48,22 @@ struct WitModel {
       default: return m2 * m2;
     }
   }
+  // zd from a cached |k| = hypot(x, y) and q(x, y): the same operations
+  GL_D double zdc(double m, double qv, int o) const {
+    const double m2 = m * m;
+    switch (o) {
+      case 0: return 1.0;
+      case 1: return qv;
+      case 2: return m2;
+      case 3: return m2 * qv;
+      default: return m2 * m2;
+    }
+  }
   // (eta, psi) response of the free surface to a (kinematic, dynamic) source
   GL_D void solve(cplx s0, cplx s1, double x, double y, double w, cplx& e, cplx& p) const {
-    const double qv = q(x, y);
+    solve_q(s0, s1, q(x, y), w, e, p);
+  }
+  GL_D void solve_q(cplx s0, cplx s1, double qv, double w, cplx& e, cplx& p) const {
     const double den = w * w - g * qv;
     const cplx a = csub(cmul(cmk(0.0, w), s0), cscale(qv, s1));
     const cplx b = cadd(cscale(g, s0), cmul(cmk(0.0, w), s1));
@@ -110,6 +123,13 @@ __device__ __noinline__ void wit_evaluate(const WitModel& M, const double* pkx, 
       }
     }
   }
+  // |k| and q of every subset wavenumber, once per quartet (the calls they
+  // replace take exactly these arguments, so the values are identical)
+  double HK[16], QK[16];
+  for (int m = 0; m < 16; ++m) {
+    HK[m] = hypot(S.kx[m], S.ky[m]);
+    QK[m] = HK[m] * tanh(M.h * HK[m]);
+  }
   cplx eff0 = czero(), eff1 = czero(), co0 = czero(), co1 = czero();
   int strict_count = 0;
   double strict_src = 0.0;
@@ -119,7 +139,7 @@ __device__ __noinline__ void wit_evaluate(const WitModel& M, const double* pkx, 
       cplx taylor = czero();
       if (d == 1) {
         S.eta[m] = cmk(0.5, 0.0);
-        S.phi[m] = cmk(0.0, -S.om[m] / (2.0 * M.q(S.kx[m], S.ky[m])));
+        S.phi[m] = cmk(0.0, -S.om[m] / (2.0 * QK[m]));
         S.psi[m] = S.phi[m];
       } else {
         // ordinary source: horizontal advection and kinetic terms over the
@@ -139,9 +159,9 @@ __device__ __noinline__ void wit_evaluate(const WitModel& M, const double* pkx, 
             const unsigned int pt = c_wit_parts[c_wit_off[m][o + 1] + e];
             const int pm = pt & 0xFF;
             const cplx pe = wit_eta_product(S, pt, o + 1);
-            lower_v = cadd(lower_v, cdiv_real(cmul(cscale(M.zd(S.kx[pm], S.ky[pm], o + 1), S.phi[pm]), pe),
+            lower_v = cadd(lower_v, cdiv_real(cmul(cscale(M.zdc(HK[pm], QK[pm], o + 1), S.phi[pm]), pe),
                                               fact[o]));
-            const double zo = M.zd(S.kx[pm], S.ky[pm], o);
+            const double zo = M.zdc(HK[pm], QK[pm], o);
             lower_t = cadd(lower_t, cdiv_real(cmul(cmul(cmk(0.0, -S.om[pm] * zo), S.phi[pm]), pe), fact[o]));
           }
         }
@@ -151,14 +171,14 @@ __device__ __noinline__ void wit_evaluate(const WitModel& M, const double* pkx, 
           for (int e = 0; e < c_wit_cnt[m][o + 1]; ++e) {
             const unsigned int pt = c_wit_parts[c_wit_off[m][o + 1] + e];
             const int pm = pt & 0xFF;
-            taylor = cadd(taylor, cdiv_real(cmul(cscale(M.zd(S.kx[pm], S.ky[pm], o), S.phi[pm]),
+            taylor = cadd(taylor, cdiv_real(cmul(cscale(M.zdc(HK[pm], QK[pm], o), S.phi[pm]),
                                                  wit_eta_product(S, pt, o + 1)), fact[o]));
           }
         }
-        const double qm = M.q(S.kx[m], S.ky[m]);
+        const double qm = QK[m];
         const cplx src0 = csub(cmk(-ord0.x, -ord0.y), cscale(qm, taylor));
         const cplx src1 = csub(cmk(-ord1.x, -ord1.y), cmul(cmk(0.0, S.om[m]), taylor));
-        const double mag = hypot(S.kx[m], S.ky[m]);
+        const double mag = HK[m];
         const bool strict_zero = mag <= 100.0 * 2.220446049250313e-16 * fmax(mag, 1.0);
         if (strict_zero) {
           S.eta[m] = czero();
@@ -166,9 +186,9 @@ __device__ __noinline__ void wit_evaluate(const WitModel& M, const double* pkx, 
           strict_count += 1;
           strict_src = fmax(strict_src, hypot(cabs_(src0), cabs_(src1)));
         } else if (d == 2 || (d == 3 && abs(S.chg[m]) == 3)) {
-          M.solve(src0, src1, S.kx[m], S.ky[m], S.om[m], S.eta[m], S.psi[m]);
+          M.solve_q(src0, src1, QK[m], S.om[m], S.eta[m], S.psi[m]);
         } else if (d == 3) {
-          const double wo = M.omega(S.kx[m], S.ky[m]);
+          const double wo = sqrt(M.g * QK[m]);
           const double ms = sqrt(wo / (2.0 * M.g)), ns = sqrt(M.g / (2.0 * wo));
           const int ts = S.chg[m] > 0 ? 1 : -1;
           const cplx a = cdiv_real(src0, 2.0 * ms);
@@ -188,8 +208,8 @@ __device__ __noinline__ void wit_evaluate(const WitModel& M, const double* pkx, 
             // quadratic normal map of (cubic subset, singleton)
             const double ax = S.kx[cm], ay = S.ky[cm], bx = skx[sgl], by = sky[sgl];
             const int sa = S.chg[cm] > 0 ? 1 : -1, sb = sign[sgl];
-            const double qa = M.q(ax, ay), qb = M.q(bx, by);
-            const double wa = M.omega(ax, ay), wb = M.omega(bx, by);
+            const double qa = QK[cm], qb = QK[1 << sgl];  // (ax, ay), (bx, by) of subsets cm, {sgl}
+            const double wa = sqrt(M.g * qa), wb = sqrt(M.g * qb);
             const double ma = sqrt(wa / (2.0 * M.g)), na = sqrt(M.g / (2.0 * wa));
             const cplx ea = cmk(ma, 0.0), psa = cmk(0.0, -sa * na);
             const cplx eb = cmk(0.5, 0.0), psb = cmk(0.0, -sb * wb / (2.0 * qb));
@@ -210,22 +230,22 @@ __device__ __noinline__ void wit_evaluate(const WitModel& M, const double* pkx, 
             const int cc = S.chg[cm];
             if (abs(cc) != 1) continue;
             if (cabs_(S.eta[cm]) + cabs_(S.psi[cm]) == 0.0) continue;
-            const double cf = M.omega(S.kx[cm], S.ky[cm]);
+            const double cf = sqrt(M.g * QK[cm]);
             const cplx rot = cmul(cmk(0.0, cc * cf / M.g), S.psi[cm]);
             const cplx ae = cscale(0.5, cadd(S.eta[cm], rot));
             const cplx oe = cscale(0.5, csub(S.eta[cm], rot));
             const cplx ap = cmul(cmk(0.0, -M.g * cc / cf), ae);
             const cplx op = cmul(cmk(0.0, M.g * cc / cf), oe);
-            const double sq = M.q(skx[sgl], sky[sgl]);
+            const double sq = QK[1 << sgl];
             const cplx se = cmk(0.5, 0.0);
-            const cplx sp = cmk(0.0, -sign[sgl] * M.omega(pkx[sgl], pky[sgl]) / (2.0 * sq));
+            const cplx sp = cmk(0.0, -sign[sgl] * sqrt(M.g * QK[1 << sgl]) / (2.0 * sq));
             cplx al0 = czero(), al1 = czero();
             for (int pass = 0; pass < 2; ++pass) {
               const double wa = pass == 0 ? cc * cf : -cc * cf;
               const cplx ea = pass == 0 ? ae : oe, pa = pass == 0 ? ap : op;
               const double ax = S.kx[cm], ay = S.ky[cm], bx = skx[sgl], by = sky[sgl];
               const cplx x0 = cadd(cmul(cscale(M.g1(ax, ay, bx, by), ea), sp), cmul(cscale(M.g1(bx, by, ax, ay), se), pa));
-              const cplx x1 = cmul(cscale((ax * bx + ay * by) + M.q(ax, ay) * sq, pa), sp);
+              const cplx x1 = cmul(cscale((ax * bx + ay * by) + QK[cm] * sq, pa), sp);
               cplx re = czero(), rp = czero();
               if (hypot(ax + bx, ay + by) != 0.0) M.solve(x0, x1, ax + bx, ay + by, wa + som[sgl], re, rp);
               if (pass == 0) {
@@ -237,11 +257,11 @@ __device__ __noinline__ void wit_evaluate(const WitModel& M, const double* pkx, 
               }
             }
           }
-          const double qo = M.q(S.kx[m], S.ky[m]);
+          const double qo = QK[m];
           const double lin = M.g * qo, tem = S.om[m] * S.om[m];
           const double rho = fabs(lin - tem) / fmax(lin + tem, 2.2250738585072014e-308);
           if (rho < thr) {
-            const double wo = M.omega(S.kx[m], S.ky[m]);
+            const double wo = sqrt(M.g * QK[m]);
             const double ms = sqrt(wo / (2.0 * M.g)), ns = sqrt(M.g / (2.0 * wo));
             const int ts = S.om[m] >= 0.0 ? 1 : -1;
             const cplx a = cdiv_real(eff0, 2.0 * ms);
@@ -252,7 +272,7 @@ __device__ __noinline__ void wit_evaluate(const WitModel& M, const double* pkx, 
             S.eta[m] = cdiv_real(cmul(cmk(0.0, ms), comp), den);
             S.psi[m] = cdiv_real(cscale(-ts * ns, comp), den);
           } else {
-            M.solve(eff0, eff1, S.kx[m], S.ky[m], S.om[m], S.eta[m], S.psi[m]);
+            M.solve_q(eff0, eff1, QK[m], S.om[m], S.eta[m], S.psi[m]);
           }
         }
         S.phi[m] = csub(S.psi[m], taylor);
@@ -266,10 +286,10 @@ __device__ __noinline__ void wit_evaluate(const WitModel& M, const double* pkx, 
             const int pm = pt & 0xFF;
             const cplx pe = wit_eta_product(S, pt, o + 1);
             const cplx common = cdiv_real(cmul(S.phi[pm], pe), fact[o]);
-            const double vert = M.zd(S.kx[pm], S.ky[pm], o);
+            const double vert = M.zdc(HK[pm], QK[pm], o);
             h0 = cadd(h0, cmul(cmk(0.0, S.kx[pm] * vert), common));
             h1 = cadd(h1, cmul(cmk(0.0, S.ky[pm] * vert), common));
-            v = cadd(v, cdiv_real(cmul(cscale(M.zd(S.kx[pm], S.ky[pm], o + 1), S.phi[pm]), pe), fact[o]));
+            v = cadd(v, cdiv_real(cmul(cscale(M.zdc(HK[pm], QK[pm], o + 1), S.phi[pm]), pe), fact[o]));
           }
         }
         S.sh0[m] = h0;
@@ -278,13 +298,13 @@ __device__ __noinline__ void wit_evaluate(const WitModel& M, const double* pkx, 
       }
     }
   }
-  const double qo = M.q(S.kx[15], S.ky[15]);
+  const double qo = QK[15];
   const double lin = M.g * qo, tem = S.om[15] * S.om[15];
   const double rho = fabs(lin - tem) / fmax(lin + tem, 2.2250738585072014e-308);
   cplx er = csub(csub(cmul(cmk(0.0, -S.om[15]), S.eta[15]), cscale(qo, S.psi[15])), eff0);
   cplx pr = csub(cadd(cmul(cmk(0.0, -S.om[15]), S.psi[15]), cscale(M.g, S.eta[15])), eff1);
   if (rho < thr) {
-    const double wo = M.omega(S.kx[15], S.ky[15]);
+    const double wo = sqrt(M.g * QK[15]);
     const double ms = sqrt(wo / (2.0 * M.g)), ns = sqrt(M.g / (2.0 * wo));
     const int ts = S.om[15] >= 0.0 ? 1 : -1;
     er = cadd(er, cscale(ms, S.ret[15]));
