@@ -1090,7 +1090,8 @@ struct TwinRule {
   int m, parent, fac;  // m = factor(fac) * parent
 };
 static const TwinRule kTwinRules[] = {
-    {M_QX, M_ONE, 1}, {M_NUQX, M_NU, 1}, {M_IQX, M_ONE, 2}, {M_NUQX, M_MI_NU, 2}};
+    {M_QX, M_ONE, 1},   {M_NUQX, M_NU, 1}, {M_IQX, M_ONE, 2}, {M_NUQX, M_MI_NU, 2},
+    {M_NU2QX, M_NU2, 1}, {M_IQXA, M_A, 2}};
 
 static void set_banks(ColArgs& a, int nb, const int* mult, const int* src) {
   int parent_of[MAX_BANKS], fac_of[MAX_BANKS];
@@ -2526,11 +2527,9 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     ColArgs a;
     std::memset(&a, 0, sizeof a);
     a.kind = kind;
-    a.nbanks = nb;
-    for (int k = 0; k < nb; ++k) {
-      a.mult[k] = mults[k];
-      a.src_of[k] = srcs ? srcs[k] : 0;
-    }
+    int src[MAX_BANKS];
+    for (int k = 0; k < nb; ++k) src[k] = srcs ? srcs[k] : 0;
+    set_banks(a, nb, mults, src);  // qx-multiple banks become twins
     a.box = box;
     a.geo = geo;
     a.spec = sp;
