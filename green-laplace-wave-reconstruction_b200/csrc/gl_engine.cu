@@ -3114,8 +3114,8 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
     ColArgs a;
     std::memset(&a, 0, sizeof a);
     a.kind = COL_ETA22;
-    a.nbanks = 8;
-    for (int k = 0; k < 8; ++k) a.mult[k] = m8[k];
+    const int z8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    set_banks(a, 8, m8, z8);  // qx-multiple banks become twins
     a.box = B1;
     a.geo = p->geo1;
     a.spec = spec;
@@ -3236,8 +3236,8 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
       ColArgs a;
       std::memset(&a, 0, sizeof a);
       a.kind = COL_INNER;
-      a.nbanks = 12;
-      for (int k = 0; k < 12; ++k) a.mult[k] = mi[k];
+      const int z12[12] = {0};
+      set_banks(a, 12, mi, z12);
       a.box = B1;
       a.geo = p->geo1;
       a.spec = spec;
@@ -3309,8 +3309,8 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
       ColArgs a;
       std::memset(&a, 0, sizeof a);
       a.kind = COL_OUTER1;
-      a.nbanks = 12;
-      for (int k = 0; k < 12; ++k) a.mult[k] = m1[k];
+      const int z12[12] = {0};
+      set_banks(a, 12, m1, z12);
       a.box = B1;
       a.geo = p->geo1;
       a.spec = spec;
@@ -3326,11 +3326,7 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
       ColArgs a2;
       std::memset(&a2, 0, sizeof a2);
       a2.kind = COL_OUTER2;
-      a2.nbanks = 9;
-      for (int k = 0; k < 9; ++k) {
-        a2.mult[k] = m9[k];
-        a2.src_of[k] = src9[k];
-      }
+      set_banks(a2, 9, m9, src9);
       a2.box = B2;
       a2.geo = p->geo2;
       a2.spec = E;
