@@ -824,6 +824,13 @@ static size_t stage_scratch(const gl_plan* p, int g) {
   return need;
 }
 
+// The inner accumulation: blocks of 256 threads over (ACC_TILE-bin tiles,
+// units); each block covers every outer node of its unit.
+static void launch_acc_inner(const AccArgs& c, size_t plane, int units, cudaStream_t st) {
+  const int ntiles = (int)((plane + ACC_TILE - 1) / ACC_TILE);
+  acc_inner_kernel<<<dim3(std::min(ntiles, 4096), units), 256, 0, st>>>(c);
+}
+
 static void plan_free(gl_plan* p) {
   if (!p) return;
   cudaFree(p->geo4);
@@ -1891,10 +1898,9 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       c.nnodes = I;
       c.nsub = J;
       c.floor_rel = p->floor_rel;
-      dim3 g(grid_for(pl2, T, 128), nuj);
       {
         LaunchScope ls_("acc_inner_kernel", st, 0.0);
-        acc_inner_kernel<<<g, T, 0, st>>>(c);
+        launch_acc_inner(c, pl2, nuj / c.nsub, st);
       }
       LAUNCH_CHECK("acc_inner_kernel");
     }
@@ -3296,10 +3302,9 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
       c.nnodes = I;
       c.nsub = Jo;
       c.floor_rel = p->floor_rel;
-      dim3 g(grid_for(pl2, T, 128), nuj);
       {
         LaunchScope ls_("acc_inner_kernel", st, 0.0);
-        acc_inner_kernel<<<g, T, 0, st>>>(c);
+        launch_acc_inner(c, pl2, nuj / c.nsub, st);
       }
       LAUNCH_CHECK("acc_inner_kernel");
     }

@@ -1080,53 +1080,79 @@ __global__ void acc_psi22_kernel(AccArgs a) {
 
 // order-3 inner accumulation into the four pair spectra of each outer node
 // (_order3.py:240-259); the eta_t max feeds its floor in the outer stage.
-__global__ void acc_inner_kernel(AccArgs a) {
-  const int uj = blockIdx.y;  // unit * n_outer + j
-  const int unit = uj / a.nsub;
+// One block takes ACC_TILE bins of one unit for all of its outer nodes
+// (AccArgs::nsub of them).  The node responses sinh(sqrt(A) tau)/sqrt(A) and
+// cosh(sqrt(A) tau) depend on the unit, the inner node and the bin only, so
+// each is evaluated once per block into shared memory; the block's threads
+// then accumulate the (outer node, bin) items from there.
+constexpr int ACC_TILE = 64;  // a multiple of 32: each warp's items share one outer node
+__global__ void __launch_bounds__(256, 4) acc_inner_kernel(AccArgs a) {
+  const int unit = blockIdx.y;
+  const int J = a.nsub, I = a.nnodes;
   const int plane = a.box.w * a.box.h;
   const UnitScalars& u = a.us[unit];
-  double local = 0.0;
   __shared__ double s_tau[MAX_RANK], s_coef[MAX_RANK];
-  if (threadIdx.x < a.nnodes) {
+  __shared__ double s_sh[MAX_RANK][ACC_TILE], s_ch[MAX_RANK][ACC_TILE];
+  if (threadIdx.x < I) {
     const double x = a.nodes[threadIdx.x], w = a.weights[threadIdx.x];
     const double tau = x / u.lam2;
     s_tau[threadIdx.x] = tau;
     s_coef[threadIdx.x] = w * exp(x) / u.lam2 * exp(-2.0 * u.shift2 * tau) / 4.0;
   }
-  __syncthreads();
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
-    BinGeo g = load_geo(a.geo, plane, i);
-    cplx e = czero(), et = czero(), p = czero(), pt = czero();
-    for (int ii = 0; ii < a.nnodes; ++ii) {
-      const int js = uj * a.nnodes + ii;
-      const double tau = s_tau[ii];
-      const double coef = s_coef[ii];
-      const double sh = sinh_over_root(g.sqa, tau);
-      const double ch = cosh(g.sqa * tau);
-      const cplx* src = a.in + (size_t)js * 4 * plane;
-      cplx sd = floored(src[i], a.floor_rel, a.maxin[js * 4 + 0]);
-      cplx sk = floored(src[plane + i], a.floor_rel, a.maxin[js * 4 + 1]);
-      cplx sdt = floored(src[2 * plane + i], a.floor_rel, a.maxin[js * 4 + 2]);
-      cplx skt = floored(src[3 * plane + i], a.floor_rel, a.maxin[js * 4 + 3]);
-      const double mash = -g.a * sh;
-      e = cadd(e, cscale(coef, cadd(cscale(mash, sd), cscale(ch, sk))));
-      et = csub(et, cmul(cmk(0.0, coef), cadd(cscale(mash, sdt), cscale(ch, skt))));
-      p = cadd(p, cmul(cmk(0.0, coef), csub(cscale(ch, sd), cscale(sh, sk))));
-      pt = cadd(pt, cscale(coef, csub(cscale(ch, sdt), cscale(sh, skt))));
+  const int ntiles = (plane + ACC_TILE - 1) / ACC_TILE;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int i0 = tile * ACC_TILE;
+    __syncthreads();  // s_tau written, the previous tile's responses read
+    for (int w = threadIdx.x; w < I * ACC_TILE; w += blockDim.x) {
+      const int ii = w / ACC_TILE, b = w % ACC_TILE;
+      if (i0 + b < plane) {
+        const double sqa = a.geo[5 * plane + i0 + b];
+        s_sh[ii][b] = sinh_over_root(sqa, s_tau[ii]);
+        s_ch[ii][b] = cosh(sqa * s_tau[ii]);
+      }
     }
-    if (!a.mask[(size_t)unit * plane + i]) { e = czero(); et = czero(); p = czero(); pt = czero(); }
-    cplx* dst = a.out + (size_t)uj * 4 * plane;
-    dst[i] = e;
-    dst[plane + i] = et;
-    dst[2 * plane + i] = p;
-    dst[3 * plane + i] = pt;
-    local = keep_max_abs(local, et);
+    __syncthreads();
+    for (int w = threadIdx.x; w < J * ACC_TILE; w += blockDim.x) {
+      const int j = w / ACC_TILE, b = w % ACC_TILE;
+      const int i = i0 + b;
+      const int uj = unit * J + j;
+      double local = 0.0;
+      if (i < plane) {
+        const double ga = a.geo[4 * plane + i];
+        cplx e = czero(), et = czero(), p = czero(), pt = czero();
+        for (int ii = 0; ii < I; ++ii) {
+          const int js = uj * I + ii;
+          const double coef = s_coef[ii];
+          const double sh = s_sh[ii][b];
+          const double ch = s_ch[ii][b];
+          const cplx* src = a.in + (size_t)js * 4 * plane;
+          cplx sd = floored(src[i], a.floor_rel, a.maxin[js * 4 + 0]);
+          cplx sk = floored(src[plane + i], a.floor_rel, a.maxin[js * 4 + 1]);
+          cplx sdt = floored(src[2 * plane + i], a.floor_rel, a.maxin[js * 4 + 2]);
+          cplx skt = floored(src[3 * plane + i], a.floor_rel, a.maxin[js * 4 + 3]);
+          const double mash = -ga * sh;
+          e = cadd(e, cscale(coef, cadd(cscale(mash, sd), cscale(ch, sk))));
+          et = csub(et, cmul(cmk(0.0, coef), cadd(cscale(mash, sdt), cscale(ch, skt))));
+          p = cadd(p, cmul(cmk(0.0, coef), csub(cscale(ch, sd), cscale(sh, sk))));
+          pt = cadd(pt, cscale(coef, csub(cscale(ch, sdt), cscale(sh, skt))));
+        }
+        if (!a.mask[(size_t)unit * plane + i]) { e = czero(); et = czero(); p = czero(); pt = czero(); }
+        cplx* dst = a.out + (size_t)uj * 4 * plane;
+        dst[i] = e;
+        dst[plane + i] = et;
+        dst[2 * plane + i] = p;
+        dst[3 * plane + i] = pt;
+        local = keep_max_abs(0.0, et);
+      }
+      // whole warps take this loop's iterations together (blockDim.x and
+      // J * ACC_TILE are multiples of 32), and a warp's items share uj
+      for (int o = 16; o > 0; o >>= 1) {
+        const double other = __shfl_xor_sync(0xffffffffu, local, o);
+        local = (other > local || other != other) ? other : local;
+      }
+      if ((threadIdx.x & 31) == 0) atomic_max_nonneg(a.maxout + uj, local);
+    }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    const double other = __shfl_xor_sync(0xffffffffu, local, o);
-    local = (other > local || other != other) ? other : local;
-  }
-  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(a.maxout + uj, local);
 }
 
 // order-3 outer combine: floors of the four forcing spectra, then the psi
