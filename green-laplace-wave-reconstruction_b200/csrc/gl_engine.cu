@@ -1331,14 +1331,18 @@ static gl_status launch_out_rows(const OutArgs& a0, int nuc, cudaStream_t st, co
   const size_t smem = (size_t)G * padded_len(a.nx) * sizeof(cplx);
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(out_row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    cudaFuncSetAttribute(out_row_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    cudaFuncSetAttribute(out_row_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
     attr = true;
   }
   dim3 grid((a.ny + G - 1) / G, nuc);
   const double bytes = (double)nuc * a.w * a.ny * sizeof(cplx) +
                        (double)nuc * a.nx * a.ny * (a.real_only ? sizeof(double) : sizeof(cplx));
   LaunchScope ls("out_row_kernel", st, bytes);
-  out_row_kernel<<<grid, 256, smem, st>>>(a, tw);
+  if (a.real_only)
+    out_row_kernel<true><<<grid, 256, smem, st>>>(a, tw);
+  else
+    out_row_kernel<false><<<grid, 256, smem, st>>>(a, tw);
   LAUNCH_CHECK("out_row_kernel");
   return GL_OK;
 }

@@ -1250,7 +1250,10 @@ struct OutArgs {
 
 // Final inverse transform along x on the reference grid: each group of n/16
 // threads takes one output row (inputs [uc][y][col], zero outside the box
-// columns) and writes scaled complex values or real parts.
+// columns) and writes scaled complex values or (REAL, OutArgs::real_only)
+// real parts; one instantiation per output type keeps one store path per
+// kernel.
+template <bool REAL>
 __global__ void __launch_bounds__(256, 2) out_row_kernel(OutArgs a, const cplx* __restrict__ tw) {
   extern __shared__ cplx smem[];
   const int n = a.nx;
@@ -1272,7 +1275,7 @@ __global__ void __launch_bounds__(256, 2) out_row_kernel(OutArgs a, const cplx* 
     return xi < a.w ? row[xi] : czero();
   };
   bool bad = false;  // the output check of the unit's status, folded into the store
-  if (a.real_only) {
+  if constexpr (REAL) {
     double* o = reinterpret_cast<double*>(a.out) + base;
     auto store = [&](int xb, cplx v) {
       const double r = s * v.x;
