@@ -1212,6 +1212,10 @@ static void row_launch(dim3 grid, int T, size_t smem, cudaStream_t st, const Row
     if constexpr (MIX == 0)
       attr = attr && cudaFuncSetAttribute(row_kernel_t<K, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)ROW_SMEM_LIMIT) == cudaSuccess;
+    if constexpr (K == ROW_OUTER && MIX == 0)
+      attr = attr && cudaFuncSetAttribute(row_kernel_t<K, 0, false, true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)ROW_SMEM_LIMIT) == cudaSuccess;
   }
   int nb = 0;
   for (int g = 0; g < a.ngrp; ++g) nb += a.grp[g].nb;
@@ -1244,6 +1248,12 @@ static void row_launch(dim3 grid, int T, size_t smem, cudaStream_t st, const Row
   if constexpr (MIX == 0) {
     if (rpb > 1) {
       row_kernel_t<K, 0, true><<<g2, threads, smem * rpb, st>>>(b, tw);
+      return;
+    }
+  }
+  if constexpr (K == ROW_OUTER && MIX == 0) {
+    if (threads <= 192) {
+      row_kernel_t<K, 0, false, true><<<g2, threads, smem, st>>>(b, tw);
       return;
     }
   }

@@ -767,8 +767,11 @@ GL_D void row_products_adj(int kind, cplx* b, int L, int p) {
 // MIX = m > 0: the row length is the mixed length 16 m (pair stages on a
 // product grid narrower than a power of two); 0: a power of two.  MULTI:
 // several short rows per block (RowArgs::rpb).
-template <int KIND, int MIX = 0, bool MULTI = false>
-__global__ void __launch_bounds__(256, 2) row_kernel_t(RowArgs a, const cplx* __restrict__ tw) {
+// B192: launched with at most 192 threads (the order-3 outer row of 256
+// points: 12 groups of 16, 92 KB of shared memory, 2 blocks per SM), so 2
+// blocks per SM leave it 168 registers instead of the 128 of 2 x 256.
+template <int KIND, int MIX = 0, bool MULTI = false, bool B192 = false>
+__global__ void __launch_bounds__(B192 ? 192 : 256, 2) row_kernel_t(RowArgs a, const cplx* __restrict__ tw) {
   constexpr int FAMILY = KIND >= ROW_ADJ_ETA22 ? 1 : (KIND >= ROW_E44_PAIR && KIND <= ROW_E44_ORDER4_PSI ? 2 : 0);
   extern __shared__ __align__(128) cplx smem[];
   __shared__ __align__(8) unsigned long long stage_bar;
