@@ -828,7 +828,8 @@ static size_t stage_scratch(const gl_plan* p, int g) {
 // units); each block covers every outer node of its unit.
 static void launch_acc_inner(const AccArgs& c, size_t plane, int units, cudaStream_t st) {
   const int ntiles = (int)((plane + ACC_TILE - 1) / ACC_TILE);
-  acc_inner_kernel<<<dim3(std::min(ntiles, 4096), units), 256, 0, st>>>(c);
+  // at least one block (an empty box runs no tile)
+  acc_inner_kernel<<<dim3(std::max(1, std::min(ntiles, 4096)), units), 256, 0, st>>>(c);
 }
 
 static void plan_free(gl_plan* p) {
