@@ -3,7 +3,8 @@
 * MATLAB fixtures of the reference (python/tests/test_spatial.py:16-65),
   with the reference's own tolerances;
 * outputs of the reference Python package on seeded inputs
-  (tests/golden/make_golden.py).
+  (tests/golden/make_golden.py), and of its order-3 graph at inner / outer
+  GL rank pairs other than GL4/GL4 (tests/golden/make_rank_pairs.py).
 """
 
 import math
@@ -30,6 +31,11 @@ def matlab():
 @pytest.fixture(scope="module")
 def refpy():
     return dict(np.load(GOLD / "reference_python.npz"))
+
+
+@pytest.fixture(scope="module")
+def rank_pairs():
+    return dict(np.load(GOLD / "order3_rank_pairs.npz"))
 
 
 def _fixture_run(m, tag, order):
@@ -121,3 +127,19 @@ def test_minkowski_support_matches_direct_sum():
         for y2, x2 in zip(ys, xs):
             direct[(y1 + y2) % n, (x1 + x2) % n] = True
     assert np.array_equal(s2, direct)
+
+
+@pytest.mark.parametrize("inner,outer", [(6, 3), (8, 6), (4, 10), (12, 4)])
+def test_oracle_order3_rank_pairs_match_reference(rank_pairs, inner, outer):
+    """_order3.py:18-26 takes the inner and outer ranks as arguments; the
+    oracle's order3 reproduces it at unequal rank pairs."""
+    g, h, lx, ly, nx, ny, t = rank_pairs["meta"]
+    a, b, kx, ky = rank_pairs["modes"]
+    nx, ny = int(nx), int(ny)
+    oc = O.spectral_coefficients(3, g, h, a, b, kx, ky)
+    s = O.deposit_modes(oc["a"], oc["b"], oc["kx"], oc["ky"], oc["omega"], h, lx, ly, nx, ny, t)
+    kxg, kyg = O.fft_wavenumber_grid(lx, ly, nx, ny)
+    e33, p33, audit = O.order3(s, h * kxg, h * kyg, inner_rank=inner, outer_rank=outer)
+    assert audit["inner_quadrature_rank"] == inner and audit["outer_quadrature_rank"] == outer
+    assert rel(e33, rank_pairs[f"gl{inner}_{outer}/eta33"]) < 1e-14
+    assert rel(p33, rank_pairs[f"gl{inner}_{outer}/psi33"]) < 1e-14
