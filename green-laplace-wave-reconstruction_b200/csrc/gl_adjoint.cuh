@@ -37,6 +37,7 @@ struct SeedArgs {
 
 // + sign transform along x of each residual row; only the box columns are
 // kept.  The column pass is col_fft_kernel with conj_io = 1.
+#ifdef GL_TRANSFORM_TU  // launched by gl_launch_cols.cu
 __global__ void __launch_bounds__(256, 2) seed_row_kernel(SeedArgs a, const cplx* __restrict__ tw) {
   extern __shared__ cplx smem[];
   const int n = a.nx;
@@ -57,6 +58,7 @@ __global__ void __launch_bounds__(256, 2) seed_row_kernel(SeedArgs a, const cplx
   };
   fft_row<+1>(buf, f, active, tw, load, store);
 }
+#endif  // GL_TRANSFORM_TU
 
 // ---------------------------------------------------------------------------
 // column + transform of adjoint bank fields, multipliers, damping, combine
@@ -175,6 +177,7 @@ __global__ void __launch_bounds__(256, 2) col_combine_kernel(CmbArgs a, const cp
 // adjoint spectra of the accumulated node products (elementwise)
 // ---------------------------------------------------------------------------
 
+#ifndef GL_TRANSFORM_TU  // elementwise kernels: compiled by gl_engine.cu only
 // A bin's forward value survived the stage's mask and roundoff floor
 // (the forward's floored(): |v| < rel * max zeroes it).
 GL_D bool kept(cplx v, double rel, unsigned long long peak_bits, unsigned char in_mask) {
@@ -326,5 +329,6 @@ __global__ void deposit_adjoint_kernel(int n_units, int n_seg, const int* seg_of
     }
   }
 }
+#endif  // GL_TRANSFORM_TU
 
 }  // namespace gl

@@ -18,16 +18,19 @@
 #include "gl_eta44.cuh"
 #include "gl_adjoint.cuh"
 #include "gl_modal.cuh"
+#include "gl_host.h"
 
 using namespace gl;
 
 // ---------------------------------------------------------------------------
-// error plumbing
+// error plumbing and launch accounting (declared in gl_host.h)
 // ---------------------------------------------------------------------------
 
 static thread_local std::string g_last_error;
 
-static gl_status fail(gl_status s, const char* fmt, ...) {
+namespace gl {
+
+gl_status fail(gl_status s, const char* fmt, ...) {
   char buf[512];
   va_list ap;
   va_start(ap, fmt);
@@ -37,58 +40,26 @@ static gl_status fail(gl_status s, const char* fmt, ...) {
   return s;
 }
 
-#define CUDA_TRY(expr)                                                               \
-  do {                                                                               \
-    cudaError_t e_ = (expr);                                                         \
-    if (e_ != cudaSuccess)                                                           \
-      return fail(GL_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(e_));      \
-  } while (0)
+std::atomic<unsigned long long> g_launches{0};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<ProfRecord> g_prof;
 
-#define LAUNCH_CHECK(what)                                                           \
-  do {                                                                               \
-    cudaError_t e_ = cudaGetLastError();                                             \
-    if (e_ != cudaSuccess)                                                           \
-      return fail(GL_ERR_CUDA, "launch of %s failed: %s", what, cudaGetErrorString(e_)); \
-  } while (0)
+cudaError_t ensure_smem_attr(const void* kernel, int bytes) {
+  static std::mutex mu;
+  static std::vector<std::pair<std::pair<int, const void*>, int>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  for (const auto& d : done)
+    if (d.first.first == dev && d.first.second == kernel && d.second >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done.push_back({{dev, kernel}, bytes});
+  return e;
+}
 
-// ---------------------------------------------------------------------------
-// launch accounting: a launch counter and optional per-kernel event timing
-// ---------------------------------------------------------------------------
-
-static std::atomic<unsigned long long> g_launches{0};
-
-struct ProfRecord {
-  const char* name;
-  cudaEvent_t start, stop;
-  double bytes;
-};
-static std::mutex g_prof_mu;
-static bool g_prof_on = false;
-static std::vector<ProfRecord> g_prof;
-
-// Wraps one kernel launch: counts it and, while profiling, brackets it with
-// events on its own stream.  `bytes` is the launch's algorithmic traffic.
-struct LaunchScope {
-  const char* name;
-  cudaStream_t st;
-  double bytes;
-  cudaEvent_t a = nullptr, b = nullptr;
-  LaunchScope(const char* n, cudaStream_t s, double by) : name(n), st(s), bytes(by) {
-    g_launches.fetch_add(1, std::memory_order_relaxed);
-    if (g_prof_on) {
-      cudaEventCreate(&a);
-      cudaEventCreate(&b);
-      cudaEventRecord(a, st);
-    }
-  }
-  ~LaunchScope() {
-    if (a) {
-      cudaEventRecord(b, st);
-      std::lock_guard<std::mutex> lk(g_prof_mu);
-      g_prof.push_back(ProfRecord{name, a, b, bytes});
-    }
-  }
-};
+}  // namespace gl
 
 extern "C" unsigned long long gl_launch_count(void) { return g_launches.load(); }
 
@@ -715,19 +686,6 @@ struct gl_plan {
   size_t o_s3f = 0, o_s3r = 0, o_s4 = 0, o_e44 = 0;
 };
 
-static int ilog2(int v) {
-  int l = 0;
-  while ((1 << l) < v) ++l;
-  return l;
-}
-static bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
-static int next_pow2(int v) {
-  int p = 1;
-  while (p < v) p <<= 1;
-  return p;
-}
-static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
-
 // Smallest column-transform length >= v: a power of two (>= 16) or one of the
 // mixed lengths 16 m the column kernels run.
 static int col_len(int v) {
@@ -757,15 +715,6 @@ struct Bump {
     return o;
   }
 };
-
-static const int ROW_GMAX = 4;
-static const size_t SMEM_LIMIT = 227 * 1024;
-// row kernels also hold a static mbarrier: their dynamic budget leaves 1 KB
-static const size_t ROW_SMEM_LIMIT = SMEM_LIMIT - 1024;
-
-static size_t row_smem(int nbanks, int ncx) {
-  return (size_t)nbanks * padded_len(ncx) * sizeof(cplx);
-}
 
 // Scratch bytes of each stage, for `g` units.
 static size_t stage_scratch(const gl_plan* p, int g) {
@@ -1075,19 +1024,6 @@ extern "C" gl_status gl_workspace_size(const gl_plan* p, size_t* bytes) {
 // launch helpers
 // ---------------------------------------------------------------------------
 
-static int grid_for(size_t n, int threads, int cap = 4096) {
-  size_t b = (n + threads - 1) / threads;
-  if (b < 1) b = 1;
-  if (b > (size_t)cap) b = cap;
-  return (int)b;
-}
-
-static int fft_cols_per_block(int n, int w) {
-  const int T = is_pow2(n) ? n / 16 : 16;  // threads per column transform
-  // a power of two (the kernels split thread indices with shifts)
-  return std::max(1, std::min(256 / T, next_pow2(w)));
-}
-
 // Twin banks: a bank whose multiplier is a column-constant factor times
 // another bank's on the same source (qx, i qx: constant along a column of a
 // box) is written by the column stage from that bank's transformed column
@@ -1137,225 +1073,6 @@ static void set_banks(ColArgs& a, int nb, const int* mult, const int* src) {
     ++ns;
   }
   a.nbanks = ns;
-}
-
-// Column kernels are instantiated per mixed radix (MIX = n/16 for the mixed
-// lengths, 0 for powers of two).
-template <int MIX>
-static void col_ifft_launch(dim3 grid, size_t smem, cudaStream_t st, const ColArgs& a, const cplx* tw,
-                            int cw, int bpb) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(col_ifft_kernel<MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    attr = true;
-  }
-  col_ifft_kernel<MIX><<<grid, 256, smem, st>>>(a, tw, cw, bpb);
-}
-
-template <int MIX>
-static void col_fft_launch(dim3 grid, size_t smem, cudaStream_t st, const ColFftArgs& a, const cplx* tw,
-                           int cw) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(col_fft_kernel<MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    attr = true;
-  }
-  col_fft_kernel<MIX><<<grid, 256, smem, st>>>(a, tw, cw);
-}
-
-#define GL_MIX_DISPATCH(n, launcher, ...)                                   \
-  switch (mixed_len(n) ? (n) / 16 : 0) {                                   \
-    case 3: launcher<3>(__VA_ARGS__); break;                               \
-    case 5: launcher<5>(__VA_ARGS__); break;                               \
-    case 6: launcher<6>(__VA_ARGS__); break;                               \
-    case 9: launcher<9>(__VA_ARGS__); break;                               \
-    case 10: launcher<10>(__VA_ARGS__); break;                             \
-    case 12: launcher<12>(__VA_ARGS__); break;                             \
-    case 15: launcher<15>(__VA_ARGS__); break;                             \
-    default: launcher<0>(__VA_ARGS__); break;                              \
-  }
-
-// Per-stage names of the column launches in the launch accounting.
-static const char* col_ifft_name(int kind) {
-  switch (kind) {
-    case COL_ETA22: case COL_PSI22: return "col_ifft_kernel[order2]";
-    case COL_INNER: return "col_ifft_kernel[inner]";
-    case COL_OUTER1: return "col_ifft_kernel[outer1]";
-    case COL_OUTER2: return "col_ifft_kernel[outer2]";
-    case COL_E44_PAIR: case COL_E44_FIRST3: case COL_E44_FIRST4: return "col_ifft_kernel[order4]";
-  }
-  return "col_ifft_kernel";
-}
-
-static gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
-  if (!is_pow2(a.n) && !mixed_len(a.n)) return fail(GL_ERR_UNSUPPORTED, "column length %d has no transform", a.n);
-  const int cw = fft_cols_per_block(a.n, a.box.w);
-  const size_t smem = ((size_t)cw * padded_len(a.n) + (size_t)cw * a.box.h) * sizeof(cplx);
-  // banks per block: at most 4, spread evenly over grid.z (9 banks: 3 x 3)
-  const int nz = (a.nbanks + 3) / 4;
-  const int bpb = (a.nbanks + nz - 1) / nz;
-  dim3 grid((a.box.w + cw - 1) / cw, njobs, (a.nbanks + bpb - 1) / bpb);
-  const double bytes = (double)njobs * (a.twins ? a.nout : a.nbanks) * a.box.w * a.n * sizeof(cplx) +
-                       (double)njobs * a.box.w * a.box.h * sizeof(cplx);
-  LaunchScope ls(col_ifft_name(a.kind), st, bytes);
-  GL_MIX_DISPATCH(a.n, col_ifft_launch, grid, smem, st, a, tw, cw, bpb);
-  LAUNCH_CHECK("col_ifft_kernel");
-  return GL_OK;
-}
-
-template <int K, int MIX = 0>
-static void row_launch(dim3 grid, int T, size_t smem, cudaStream_t st, const RowArgs& a,
-                       const cplx* tw) {
-  static bool attr = false;
-  if (!attr) {  // a failure here surfaces as the launch's own error
-    attr = cudaFuncSetAttribute(row_kernel_t<K, MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)ROW_SMEM_LIMIT) == cudaSuccess;
-    if constexpr (MIX == 0)
-      attr = attr && cudaFuncSetAttribute(row_kernel_t<K, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)ROW_SMEM_LIMIT) == cudaSuccess;
-    if constexpr (K == ROW_OUTER && MIX == 0)
-      attr = attr && cudaFuncSetAttribute(row_kernel_t<K, 0, false, true>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)ROW_SMEM_LIMIT) == cudaSuccess;
-  }
-  int nb = 0;
-  for (int g = 0; g < a.ngrp; ++g) nb += a.grp[g].nb;
-  // 8 transform groups per block when the row has at most 12 banks (4
-  // blocks fit per SM), 16 for wider rows (2 per SM by shared memory); a
-  // forward row with more than 16 banks (the order-3 outer row: 21) gets the
-  // fewest whole-warp groups that keep its rounds (12: the same rounds with
-  // fewer idle groups measured 6 % faster; more resident blocks for the
-  // 12-bank rows measured slower)
-  int G = nb <= 12 ? 8 : 16;
-  if (K == ROW_OUTER && nb > 16) {
-    const int rounds = (nb + 15) / 16;
-    G = (nb + rounds - 1) / rounds;
-    while ((G * T) % 32 != 0) ++G;
-  }
-  // Short rows (fewer than 16 threads per transform) carry little work per
-  // block, so a block takes several rows (one team of G groups each) while it
-  // stays within 256 threads and ~76 KB of shared memory (3 blocks per SM).
-  const int team = G * T;
-  int rpb = 1;
-  if (MIX == 0 && T < 16) {
-    int r = std::min(256 / std::max(1, team), (int)((76 * 1024) / std::max<size_t>(1, smem)));
-    while (r > 1 && (team * r) % 32 != 0) --r;
-    rpb = std::max(1, r);
-  }
-  const int threads = rpb > 1 ? team * rpb : std::max(32, std::min(256, team));
-  RowArgs b = a;
-  b.rpb = rpb;
-  dim3 g2((a.ny + rpb - 1) / rpb, grid.y);
-  if constexpr (MIX == 0) {
-    if (rpb > 1) {
-      row_kernel_t<K, 0, true><<<g2, threads, smem * rpb, st>>>(b, tw);
-      return;
-    }
-  }
-  if constexpr (K == ROW_OUTER && MIX == 0) {
-    if (threads <= 192) {
-      row_kernel_t<K, 0, false, true><<<g2, threads, smem, st>>>(b, tw);
-      return;
-    }
-  }
-  row_kernel_t<K, MIX><<<g2, threads, smem, st>>>(b, tw);
-}
-
-// Pair-stage rows also run on the mixed row lengths 144, 160, 192, 240
-// (row_len); each is its own instantiation.
-template <int K>
-static bool row_launch_mixed(dim3 grid, int T, size_t smem, cudaStream_t st, const RowArgs& a,
-                             const cplx* tw) {
-  switch (mixed_len(a.nx) ? a.nx / 16 : 0) {
-    case 0: row_launch<K, 0>(grid, T, smem, st, a, tw); return true;
-    case 9: row_launch<K, 9>(grid, T, smem, st, a, tw); return true;
-    case 10: row_launch<K, 10>(grid, T, smem, st, a, tw); return true;
-    case 12: row_launch<K, 12>(grid, T, smem, st, a, tw); return true;
-    case 15: row_launch<K, 15>(grid, T, smem, st, a, tw); return true;
-  }
-  return false;
-}
-
-static gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
-  int nb = 0;
-  for (int g = 0; g < a.ngrp; ++g) nb += a.grp[g].nb;
-  const bool e44 = a.kind >= ROW_E44_PAIR && a.kind <= ROW_E44_ORDER4_PSI;
-  const size_t smem = row_smem(nb, a.nx);
-  if (smem > ROW_SMEM_LIMIT)
-    return fail(GL_ERR_UNSUPPORTED, "row stage of %d banks x %d exceeds the shared-memory budget", nb, a.nx);
-  dim3 grid(a.ny, njobs);
-  // threads per row transform; row_launch() sets the groups per block
-  const int T = is_pow2(a.nx) ? a.nx / 16 : 16;
-  const bool pair_kind = a.kind == ROW_ETA22 || a.kind == ROW_PSI22 || a.kind == ROW_CONTACT22 ||
-                         a.kind == ROW_INNER || a.kind == ROW_ADJ_ETA22 || a.kind == ROW_ADJ_INNER;
-  if (!is_pow2(a.nx) && !pair_kind)
-    return fail(GL_ERR_UNSUPPORTED, "row kind %d runs power-of-two rows only (got %d)", a.kind, a.nx);
-  double bytes = (double)njobs * a.nout * a.out_w * a.ny * sizeof(cplx);
-  for (int g = 0; g < a.ngrp; ++g) bytes += (double)njobs * a.grp[g].nb * a.grp[g].w * a.ny * sizeof(cplx);
-  const bool adj = a.kind >= ROW_ADJ_ETA22;
-  const char* name = a.kind == ROW_INNER         ? "row_kernel[inner]"
-                     : a.kind == ROW_OUTER       ? "row_kernel[outer]"
-                     : a.kind == ROW_ADJ_INNER   ? "row_kernel[adj_inner]"
-                     : a.kind == ROW_ADJ_OUTER   ? "row_kernel[adj_outer]"
-                     : a.kind == ROW_ADJ_ETA22   ? "row_kernel[adj_eta22]"
-                     : a.kind >= ROW_E44_PAIR    ? "row_kernel[order4]"
-                                                 : "row_kernel[order2]";
-  LaunchScope ls(name, st, bytes);
-  bool ok = true;
-  switch (a.kind) {
-    case ROW_ETA22: ok = row_launch_mixed<ROW_ETA22>(grid, T, smem, st, a, tw); break;
-    case ROW_PSI22: ok = row_launch_mixed<ROW_PSI22>(grid, T, smem, st, a, tw); break;
-    case ROW_CONTACT22: ok = row_launch_mixed<ROW_CONTACT22>(grid, T, smem, st, a, tw); break;
-    case ROW_INNER: ok = row_launch_mixed<ROW_INNER>(grid, T, smem, st, a, tw); break;
-    case ROW_OUTER: row_launch<ROW_OUTER>(grid, T, smem, st, a, tw); break;
-    case ROW_E44_PAIR: row_launch<ROW_E44_PAIR>(grid, T, smem, st, a, tw); break;
-    case ROW_E44_THIRD: row_launch<ROW_E44_THIRD>(grid, T, smem, st, a, tw); break;
-    case ROW_E44_ORDER4: row_launch<ROW_E44_ORDER4>(grid, T, smem, st, a, tw); break;
-    case ROW_E44_ORDER4_PSI: row_launch<ROW_E44_ORDER4_PSI>(grid, T, smem, st, a, tw); break;
-    case ROW_ADJ_ETA22: ok = row_launch_mixed<ROW_ADJ_ETA22>(grid, T, smem, st, a, tw); break;
-    case ROW_ADJ_INNER: ok = row_launch_mixed<ROW_ADJ_INNER>(grid, T, smem, st, a, tw); break;
-    case ROW_ADJ_OUTER: row_launch<ROW_ADJ_OUTER>(grid, T, smem, st, a, tw); break;
-    default: return fail(GL_ERR_INVALID_ARGUMENT, "unknown row kind %d", a.kind);
-  }
-  if (!ok) return fail(GL_ERR_UNSUPPORTED, "row length %d has no transform", a.nx);
-  LAUNCH_CHECK("row_kernel");
-  return GL_OK;
-}
-
-static gl_status launch_col_fft(const ColFftArgs& a, int njs, cudaStream_t st, const cplx* tw,
-                                const char* name = "col_fft_kernel") {
-  if (!is_pow2(a.n) && !mixed_len(a.n)) return fail(GL_ERR_UNSUPPORTED, "column length %d has no transform", a.n);
-  const int cw = fft_cols_per_block(a.n, a.box.w);
-  const size_t smem = (size_t)cw * padded_len(a.n) * sizeof(cplx);
-  dim3 grid((a.box.w + cw - 1) / cw, njs);
-  const double bytes = (double)njs * a.box.w * (a.n + a.box.h) * sizeof(cplx);
-  LaunchScope ls(name, st, bytes);
-  GL_MIX_DISPATCH(a.n, col_fft_launch, grid, smem, st, a, tw, cw);
-  LAUNCH_CHECK("col_fft_kernel");
-  return GL_OK;
-}
-
-static gl_status launch_out_rows(const OutArgs& a0, int nuc, cudaStream_t st, const cplx* tw) {
-  OutArgs a = a0;
-  const int G = 256 / (a.nx / 16);
-  a.rows = G;
-  const size_t smem = (size_t)G * padded_len(a.nx) * sizeof(cplx);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(out_row_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    cudaFuncSetAttribute(out_row_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    attr = true;
-  }
-  dim3 grid((a.ny + G - 1) / G, nuc);
-  const double bytes = (double)nuc * a.w * a.ny * sizeof(cplx) +
-                       (double)nuc * a.nx * a.ny * (a.real_only ? sizeof(double) : sizeof(cplx));
-  LaunchScope ls("out_row_kernel", st, bytes);
-  if (a.real_only)
-    out_row_kernel<true><<<grid, 256, smem, st>>>(a, tw);
-  else
-    out_row_kernel<false><<<grid, 256, smem, st>>>(a, tw);
-  LAUNCH_CHECK("out_row_kernel");
-  return GL_OK;
 }
 
 template <class T>
@@ -2954,50 +2671,6 @@ extern "C" gl_status gl_adjoint_workspace_size(const gl_plan* p, size_t* bytes) 
   return GL_OK;
 }
 
-static gl_status launch_seed_rows(const SeedArgs& a, int nunits, cudaStream_t st, const cplx* tw) {
-  const int G = 256 / (a.nx / 16);
-  const size_t smem = (size_t)G * padded_len(a.nx) * sizeof(cplx);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(seed_row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    attr = true;
-  }
-  dim3 grid((a.ny + G - 1) / G, nunits);
-  const double bytes = (double)nunits * a.ny * ((double)a.nx * sizeof(double) + (double)a.w * sizeof(cplx));
-  LaunchScope ls("seed_row_kernel", st, bytes);
-  seed_row_kernel<<<grid, 256, smem, st>>>(a, tw);
-  LAUNCH_CHECK("seed_row_kernel");
-  return GL_OK;
-}
-
-template <int MIX>
-static void combine_launch(dim3 grid, size_t smem, cudaStream_t st, const CmbArgs& a, const cplx* tw, int cw) {
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(col_combine_kernel<MIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    attr = true;
-  }
-  col_combine_kernel<MIX><<<grid, 256, smem, st>>>(a, tw, cw);
-}
-
-static gl_status launch_combine(const CmbArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
-  // columns per block: all banks of `cw` columns staged at once, within
-  // ~110 KB of shared memory (two blocks per SM)
-  const size_t col_bytes = (size_t)a.nbanks * padded_len(a.n) * sizeof(cplx);
-  const int cw = (int)std::max<size_t>(1, std::min<size_t>((size_t)a.box.w, (110 * 1024) / col_bytes));
-  const size_t smem = (size_t)cw * col_bytes;
-  if (smem > SMEM_LIMIT) return fail(GL_ERR_UNSUPPORTED, "adjoint column stage exceeds shared memory");
-  if (a.nout < 1 || a.nout > 4) return fail(GL_ERR_INVALID_ARGUMENT, "adjoint column stage: 1..4 outputs");
-  if (!is_pow2(a.n) && !mixed_len(a.n)) return fail(GL_ERR_UNSUPPORTED, "column length %d has no transform", a.n);
-  dim3 grid((a.box.w + cw - 1) / cw, njobs);
-  const double bytes = (double)njobs * a.nbanks * a.box.w * a.n * sizeof(cplx) +
-                       (double)njobs * a.nout * a.box.w * a.box.h * sizeof(cplx);
-  LaunchScope ls("col_combine_kernel", st, bytes);
-  GL_MIX_DISPATCH(a.n, combine_launch, grid, smem, st, a, tw, cw);
-  LAUNCH_CHECK("col_combine_kernel");
-  return GL_OK;
-}
-
 // Ebar of one output box from the residual: + sign transforms, h/(Nx Ny).
 static gl_status adj_seed(gl_plan* p, int gu, const double* resid, const Box& box, cplx* rows,
                           cplx* out, cudaStream_t st) {
@@ -3685,15 +3358,15 @@ extern "C" gl_status gl_fft2(int batch, int nx, int ny, const void* d_in, void* 
   const cplx* in = reinterpret_cast<const cplx*>(d_in);
   cplx* out = reinterpret_cast<cplx*>(d_out);
   if (inverse) {
-    cudaFuncSetAttribute(fft2_rows_kernel<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    cudaFuncSetAttribute(fft2_cols_kernel<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    ensure_smem_attr((const void*)fft2_rows_kernel<+1>, (int)SMEM_LIMIT);
+    ensure_smem_attr((const void*)fft2_cols_kernel<+1>, (int)SMEM_LIMIT);
     fft2_rows_kernel<+1><<<gr, 256, smr, st>>>(in, out, nx, ilog2(nx), ny, rows, scale, tw);
     LAUNCH_CHECK("fft2_rows_kernel");
     fft2_cols_kernel<+1><<<gc, 256, smc, st>>>(out, nx, ny, ilog2(ny), cw, tw);
     LAUNCH_CHECK("fft2_cols_kernel");
   } else {
-    cudaFuncSetAttribute(fft2_rows_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    cudaFuncSetAttribute(fft2_cols_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
+    ensure_smem_attr((const void*)fft2_rows_kernel<-1>, (int)SMEM_LIMIT);
+    ensure_smem_attr((const void*)fft2_cols_kernel<-1>, (int)SMEM_LIMIT);
     fft2_rows_kernel<-1><<<gr, 256, smr, st>>>(in, out, nx, ilog2(nx), ny, rows, scale, tw);
     LAUNCH_CHECK("fft2_rows_kernel");
     fft2_cols_kernel<-1><<<gc, 256, smc, st>>>(out, nx, ny, ilog2(ny), cw, tw);
@@ -3705,26 +3378,6 @@ extern "C" gl_status gl_fft2(int batch, int nx, int ny, const void* d_in, void* 
 // ---------------------------------------------------------------------------
 // single-direction time path (modal GL resolvent and eta20)
 // ---------------------------------------------------------------------------
-
-static gl_status launch_sfft(const SFft& a, int outer, int sign, cudaStream_t st, const cplx* tw) {
-  const int T = a.n / 16;
-  const int cw = std::max(1, 256 / T);
-  const size_t smem = (size_t)cw * padded_len(a.n) * sizeof(cplx);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(strided_fft_kernel<+1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    cudaFuncSetAttribute(strided_fft_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_LIMIT);
-    attr = true;
-  }
-  dim3 grid((unsigned)((a.ncount + cw - 1) / cw), (unsigned)outer);
-  LaunchScope ls("strided_fft_kernel", st, 2.0 * a.n * (double)a.ncount * outer * sizeof(cplx));
-  if (sign > 0)
-    strided_fft_kernel<+1><<<grid, 256, smem, st>>>(a, tw, cw);
-  else
-    strided_fft_kernel<-1><<<grid, 256, smem, st>>>(a, tw, cw);
-  LAUNCH_CHECK("strided_fft_kernel");
-  return GL_OK;
-}
 
 static SFft sfft(cplx* d, int n, long long stride, long long cstride, int ncount, long long ostride,
                  double scale) {

@@ -1004,6 +1004,9 @@ struct AccArgs {
   double floor_rel;
 };
 
+constexpr int ACC_TILE = 64;  // a multiple of 32: each warp's items share one outer node
+
+#ifndef GL_TRANSFORM_TU  // elementwise kernels: compiled by gl_engine.cu only
 // eta22: sum_n coef_n (-A sh_n sd_n + ch_n sk_n)   (spatial.py:206-221)
 __global__ void acc_eta22_kernel(AccArgs a) {
   const int unit = blockIdx.y;
@@ -1088,7 +1091,6 @@ __global__ void acc_psi22_kernel(AccArgs a) {
 // cosh(sqrt(A) tau) depend on the unit, the inner node and the bin only, so
 // each is evaluated once per block into shared memory; the block's threads
 // then accumulate the (outer node, bin) items from there.
-constexpr int ACC_TILE = 64;  // a multiple of 32: each warp's items share one outer node
 __global__ void __launch_bounds__(256, 4) acc_inner_kernel(AccArgs a) {
   const int unit = blockIdx.y;
   const int J = a.nsub, I = a.nnodes;
@@ -1232,6 +1234,7 @@ __global__ void acc_outer_kernel(AccArgs a, const unsigned long long* maxpsi) {
     a.out[((size_t)unit * 2 + 1) * plane + i] = psi;
   }
 }
+#endif  // GL_TRANSFORM_TU
 
 // ---------------------------------------------------------------------------
 // final inverse FFT along x on the reference grid

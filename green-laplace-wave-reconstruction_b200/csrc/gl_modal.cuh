@@ -83,6 +83,7 @@ __global__ void __launch_bounds__(256, 2) strided_fft_kernel(SFft a, const cplx*
 // joint arrays: deposit, bank multipliers, products
 // ---------------------------------------------------------------------------
 
+#ifndef GL_TRANSFORM_TU  // elementwise kernels: compiled by gl_engine.cu only
 // joint[row][col] = val for idx = row * W + col (distinct indices; the joint
 // [rows][M] is zeroed first by the caller).
 __global__ void modal_scatter_kernel(const long long* idx, const double* val, int nnz, cplx* joint,
@@ -441,5 +442,6 @@ __global__ void series_synth_kernel(const int* bins, const cplx* coef, int nb, i
       reinterpret_cast<cplx*>(out)[n] = acc;
   }
 }
+#endif  // GL_TRANSFORM_TU
 
 }  // namespace gl
