@@ -914,6 +914,22 @@ def run_timeseries(args, rank: int, world: int, local_rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def _relaunch_ranks(n: int) -> None:
+    """``--gpus N`` without a launcher: start N ranks of this script on this
+    node through torch.distributed.run (one process per GPU, 127.0.0.1
+    rendezvous), which then sets RANK / LOCAL_RANK / WORLD_SIZE."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__),
+           *sys.argv[1:]]
+    sys.stdout.flush()
+    os.execv(sys.executable, cmd)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -932,10 +948,20 @@ def main() -> None:
                          "config4: adjoint fit; config5: order 4 (eta44 GL, WIT) on the reference's "
                          "runtime inputs; timeseries: the single-direction modal time path")
     ap.add_argument("--states", type=int, default=64, help="config3: sea states per GPU")
+    ap.add_argument("--launch-check", action="store_true",
+                    help="print each rank's RANK / WORLD_SIZE as JSON and exit (checks the "
+                         "multi-rank launch without touching a GPU)")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        _relaunch_ranks(args.gpus)  # does not return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if world != max(1, args.gpus):
+        raise SystemExit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}")
+    if args.launch_check:
+        print(json.dumps({"rank": rank, "local_rank": local_rank, "world": world}), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

@@ -34,6 +34,11 @@ GL_D void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) 
       : "memory");
 }
 
+// Completes `bytes` of the expected transaction count without a copy.
+GL_D void mbar_complete_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
 GL_D bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   uint32_t done;
   asm volatile(

@@ -18,6 +18,7 @@
 #include "gl_eta44.cuh"
 #include "gl_adjoint.cuh"
 #include "gl_modal.cuh"
+#include "gl_gen.cuh"
 #include "gl_host.h"
 
 using namespace gl;
@@ -162,6 +163,16 @@ __global__ void twiddle_kernel(cplx* tw, int count) {
   }
 }
 
+// W_n^e = exp(-2 pi i e / n), e < n, for the final transforms of reference
+// grids that are not powers of two.
+__global__ void gen_twiddle_kernel(cplx* tw, int n) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    double s, c;
+    sincospi(2.0 * (double)e / (double)n, &s, &c);
+    tw[e] = cmk(c, -s);
+  }
+}
+
 __global__ void slots_init_kernel(UnitSlots* slots, int n) {
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= n) return;
@@ -290,7 +301,7 @@ __global__ void peak_kernel(const cplx* boxv, const double* geo, Box box, int nx
       if (m * m == amax) {
         const int mx = box.x0 + i % box.w, my = box.y0 + i / box.w;
         const unsigned long long flat =
-            (unsigned long long)wrap(my, ny) * (unsigned long long)nx + (unsigned long long)wrap(mx, nx);
+            (unsigned long long)wrap_any(my, ny) * (unsigned long long)nx + (unsigned long long)wrap_any(mx, nx);
         best = flat < best ? flat : best;
       }
       if (want_channels) {
@@ -684,6 +695,15 @@ struct gl_plan {
   int ww3 = 0;
   double* geo4 = nullptr;
   size_t o_s3f = 0, o_s3r = 0, o_s4 = 0, o_e44 = 0;
+  // reference grids that are not powers of two: the final transforms run the
+  // generic-length kernels of gl_gen.cuh with these radix plans and tables
+  bool gen = false;
+  GenPlan genx, geny;
+  cplx* twx = nullptr;
+  cplx* twy = nullptr;
+  // failure-path test hook of the order-2/3 row stages (gl_plan_set_wait_test)
+  unsigned int wait_surplus = 0;
+  long long wait_cycles = 0;
 };
 
 // Smallest column-transform length >= v: a power of two (>= 16) or one of the
@@ -790,6 +810,8 @@ static void plan_free(gl_plan* p) {
   cudaFree(p->tw);
   cudaFree(p->nodes);
   cudaFree(p->comp_scale);
+  cudaFree(p->twx);
+  cudaFree(p->twy);
   delete p;
 }
 
@@ -802,9 +824,15 @@ extern "C" gl_status gl_plan_create(gl_plan** out, const gl_plan_desc* desc) {
     return fail(GL_ERR_INVALID_ARGUMENT, "positive domain lengths and positive even grid sizes are required");
   if (d.nx < 2 || d.ny < 2 || (d.nx % 2) || (d.ny % 2))
     return fail(GL_ERR_INVALID_ARGUMENT, "positive domain lengths and positive even grid sizes are required");
-  if (!is_pow2(d.nx) || !is_pow2(d.ny) || d.nx < 16 || d.ny < 16 || d.nx > TW_N || d.ny > TW_N)
-    return fail(GL_ERR_UNSUPPORTED, "the GPU engine runs power-of-two grids from 16 to %d (got %d x %d)",
-                TW_N, d.ny, d.nx);
+  GenPlan gx, gy;
+  if (d.nx < 16 || d.ny < 16 || d.nx > TW_N || d.ny > TW_N || !gen_plan(d.nx, gx) || !gen_plan(d.ny, gy))
+    return fail(GL_ERR_UNSUPPORTED,
+                "the GPU engine runs even grids from 16 to %d whose sizes have no prime factor above 5 "
+                "(got %d x %d)", TW_N, d.ny, d.nx);
+  const bool gen = !is_pow2(d.nx) || !is_pow2(d.ny);
+  if (gen && d.grid == GL_GRID_REFERENCE)
+    return fail(GL_ERR_UNSUPPORTED,
+                "product stages on a reference grid that is not a power of two are not run (use the compact grid)");
   if (!(d.depth > 0) || !(d.gravity > 0) || !std::isfinite(d.depth) || !std::isfinite(d.gravity))
     return fail(GL_ERR_INVALID_ARGUMENT, "depth and gravity must be positive");
   if (d.max_units < 1) return fail(GL_ERR_INVALID_ARGUMENT, "max_units must be >= 1");
@@ -856,13 +884,22 @@ extern "C" gl_status gl_plan_create(gl_plan** out, const gl_plan_desc* desc) {
   p->ww1 = (p->b1.w + 63) / 64;
   p->ww2 = (p->b2.w + 63) / 64;
   const int deg = o3 ? 3 : (o2 ? 2 : 1);
+  p->gen = gen;
+  p->genx = gx;
+  p->geny = gy;
   if (d.grid == GL_GRID_REFERENCE || deg == 1) {
-    p->ncx = d.nx;
-    p->ncy = d.ny;
+    // (order 1 runs no product stage; its final transforms use nx, ny)
+    p->ncx = gen ? 16 : d.nx;
+    p->ncy = gen ? 16 : d.ny;
   } else {
+    // the smallest power of two covering the stage's box; on a power-of-two
+    // reference grid never longer than it, on another grid possibly longer
+    // (an alias-free product has the same coefficients on any covering period)
     const Box& bd = deg == 3 ? p->b3 : p->b2;
-    p->ncx = std::min(d.nx, std::max(16, next_pow2(bd.w)));
-    p->ncy = std::min(d.ny, std::max(16, next_pow2(bd.h)));
+    p->ncx = std::max(16, next_pow2(bd.w));
+    p->ncy = std::max(16, next_pow2(bd.h));
+    if (is_pow2(d.nx)) p->ncx = std::min(d.nx, p->ncx);
+    if (is_pow2(d.ny)) p->ncy = std::min(d.ny, p->ncy);
   }
   p->lncx = ilog2(p->ncx);
   p->lncy = ilog2(p->ncy);
@@ -936,6 +973,15 @@ extern "C" gl_status gl_plan_create(gl_plan** out, const gl_plan_desc* desc) {
       std::memcpy(host + (4 + k) * MAX_RANK, p->h_weights[k], sizeof(double) * MAX_RANK);
     }
     e = cudaMemcpy(p->nodes, host, sizeof host, cudaMemcpyHostToDevice);
+  }
+  if (gen) {
+    if (e == cudaSuccess) e = cudaMalloc(&p->twx, sizeof(cplx) * d.nx);
+    if (e == cudaSuccess) e = cudaMalloc(&p->twy, sizeof(cplx) * d.ny);
+    if (e == cudaSuccess) {
+      gen_twiddle_kernel<<<(d.nx + 255) / 256, 256>>>(p->twx, d.nx);
+      gen_twiddle_kernel<<<(d.ny + 255) / 256, 256>>>(p->twy, d.ny);
+      e = cudaGetLastError();
+    }
   }
   if (e == cudaSuccess) e = cudaMalloc(&p->comp_scale, sizeof(double) * 6);
   if (e == cudaSuccess)
@@ -1011,6 +1057,15 @@ extern "C" gl_status gl_plan_get_info(const gl_plan* p, gl_plan_info* info) {
     if (p->e44_psi) t += R * (1 + 2) + 1;
   }
   info->transforms_per_unit = t;
+  return GL_OK;
+}
+
+extern "C" gl_status gl_plan_set_wait_test(gl_plan* p, unsigned int surplus_bytes, long long wait_cycles) {
+  if (!p) return fail(GL_ERR_INVALID_ARGUMENT, "null plan");
+  if (wait_cycles < 0 || (surplus_bytes && wait_cycles == 0) || surplus_bytes > (1u << 20))
+    return fail(GL_ERR_INVALID_ARGUMENT, "a wait test needs a positive clock budget and at most 1 MiB of surplus");
+  p->wait_surplus = surplus_bytes;
+  p->wait_cycles = wait_cycles;
   return GL_OK;
 }
 
@@ -1109,6 +1164,43 @@ static gl_status final_output(gl_plan* p, int gu, const Box& box, const double* 
                               const cplx* spec, long long spec_stride, int nb, const int* mults,
                               const int* srcs, int comp_offset, void* outputs, void* scratch,
                               cudaStream_t st, const double* comp_scale_dev, UnitScalars* us) {
+  if (p->gen) {
+    if (nb > 4) return fail(GL_ERR_INVALID_ARGUMENT, "at most 4 final components per launch");
+    GenColArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.nbanks = nb;
+    for (int k = 0; k < nb; ++k) {
+      a.mult[k] = mults[k];
+      a.src_of[k] = srcs[k];
+    }
+    a.box = box;
+    a.geo = geo;
+    a.spec = spec;
+    a.spec_job_stride = spec_stride;
+    a.spec_sub_stride = (long long)box.w * box.h;
+    a.out = reinterpret_cast<cplx*>(scratch);
+    a.gp = p->geny;
+    a.twn = p->twy;
+    a.scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
+    gl_status s = launch_gen_cols(a, gu, st);
+    if (s != GL_OK) return s;
+    GenRowArgs o;
+    std::memset(&o, 0, sizeof o);
+    o.in = reinterpret_cast<cplx*>(scratch);
+    o.w = box.w;
+    o.x0 = box.x0;
+    o.ny = p->d.ny;
+    o.ncomp = nb;
+    o.comp_offset = comp_offset;
+    o.out_ncomp = p->ncomp;
+    o.comp_scale = comp_scale_dev + comp_offset;
+    o.out = outputs;
+    o.real_only = p->d.output == GL_OUT_REAL;
+    o.us = us;
+    o.gp = p->genx;
+    o.twn = p->twx;
+    return launch_gen_rows(o, gu * nb, st);
+  }
   ColArgs a;
   std::memset(&a, 0, sizeof a);
   a.kind = COL_PLAIN;
@@ -1389,6 +1481,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     r.us = us;
     r.jobs_per_unit = J;
     r.gmax = ROW_GMAX;
+    r.wait_surplus = p->wait_surplus;
+    r.wait_cycles = p->wait_cycles;
     if ((s = launch_row(r, njobs, st, p->tw)) != GL_OK) return s;
     ColFftArgs f;
     f.in = Q;
@@ -1470,6 +1564,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     r.us = us;
     r.jobs_per_unit = 4;
     r.gmax = ROW_GMAX;
+    r.wait_surplus = p->wait_surplus;
+    r.wait_cycles = p->wait_cycles;
     if ((s = launch_row(r, njobs_r, st, p->tw)) != GL_OK) return s;
     ColFftArgs f;
     f.in = Q;
@@ -1517,6 +1613,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     rc.us = us;
     rc.jobs_per_unit = 1;
     rc.gmax = ROW_GMAX;
+    rc.wait_surplus = p->wait_surplus;
+    rc.wait_cycles = p->wait_cycles;
     if ((s = launch_row(rc, gu, st, p->tw)) != GL_OK) return s;
     ColFftArgs fc = f;
     fc.in = Qc;
@@ -1602,6 +1700,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       r.us = us;
       r.jobs_per_unit = J * I;
       r.gmax = ROW_GMAX;
+      r.wait_surplus = p->wait_surplus;
+      r.wait_cycles = p->wait_cycles;
       if ((s = launch_row(r, njobs, st, p->tw)) != GL_OK) return s;
       ColFftArgs f;
       f.in = QI;
@@ -1699,6 +1799,8 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       r.us = us;
       r.jobs_per_unit = J;
       r.gmax = ROW_GMAX;
+      r.wait_surplus = p->wait_surplus;
+      r.wait_cycles = p->wait_cycles;
       if ((s = launch_row(r, nuj, st, p->tw)) != GL_OK) return s;
       ColFftArgs f;
       f.in = QO;
@@ -2655,6 +2757,7 @@ static AdjLayout adj_layout(const gl_plan* p, int g) {
 static gl_status adj_check_plan(const gl_plan* p) {
   if (!p) return fail(GL_ERR_INVALID_ARGUMENT, "null plan");
   if (p->e44) return fail(GL_ERR_UNSUPPORTED, "the adjoint covers the eta11/eta22/eta33 graph only");
+  if (p->gen) return fail(GL_ERR_UNSUPPORTED, "the adjoint runs power-of-two reference grids only");
   if (!(p->comps & (GL_COMP_ETA11 | GL_COMP_ETA22 | GL_COMP_ETA33)))
     return fail(GL_ERR_INVALID_ARGUMENT, "the plan has no eta component to differentiate");
   if (adj_eta33(p) && row_smem(23, p->ncx) > ROW_SMEM_LIMIT)
@@ -3832,14 +3935,13 @@ extern "C" gl_status gl_box_synthesize_noalloc(int n_units, int nx, int ny, int 
   const size_t tw_bytes = align_up(sizeof(cplx) * TW_N);
   const size_t geo_bytes = align_up(sizeof(double) * 6 * (size_t)box_w * box_h);
   const size_t mid_bytes = align_up(sizeof(cplx) * (size_t)n_units * box_w * ny);
-  const size_t scale_bytes = 256;  // one slot for the physical scale factor
-  if (tw_bytes + geo_bytes + mid_bytes + scale_bytes > GL_NOALLOC_SCRATCH_BYTES)
+  if (tw_bytes + geo_bytes + mid_bytes > GL_NOALLOC_SCRATCH_BYTES)
     return fail(GL_ERR_WORKSPACE,
                 "no-alloc synthesis needs %zu bytes of scratch but its static array holds %u: "
                 "use fewer units per call (n_units * box_w * ny * 16 bytes must stay below "
                 "about %u bytes)",
-                tw_bytes + geo_bytes + mid_bytes + scale_bytes, GL_NOALLOC_SCRATCH_BYTES,
-                (unsigned)(GL_NOALLOC_SCRATCH_BYTES - tw_bytes - geo_bytes - scale_bytes));
+                tw_bytes + geo_bytes + mid_bytes, GL_NOALLOC_SCRATCH_BYTES,
+                (unsigned)(GL_NOALLOC_SCRATCH_BYTES - tw_bytes - geo_bytes));
   if (n_units == 0) return GL_OK;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   unsigned char* base = nullptr;
@@ -3880,11 +3982,9 @@ extern "C" gl_status gl_box_synthesize_noalloc(int n_units, int nx, int ny, int 
   o.ncomp = 1;
   o.comp_offset = 0;
   o.out_ncomp = 1;
-  // the output kernel reads its physical scale from device memory: keep it in
-  // its own slot of the scratch, written on the caller's stream
-  double* scale_dev = reinterpret_cast<double*>(base + tw_bytes + geo_bytes + mid_bytes);
-  CUDA_TRY(cudaMemcpyAsync(scale_dev, &scale, sizeof(double), cudaMemcpyHostToDevice, st));
-  o.comp_scale = scale_dev;
+  // the scale travels by value in the launch arguments
+  o.comp_scale = nullptr;
+  o.scale_value = scale;
   o.out = d_out;
   o.real_only = real_only ? 1 : 0;
   return launch_out_rows(o, n_units, st, tw);
@@ -3961,10 +4061,25 @@ static unsigned long long wit_candidates(int sector, unsigned long long n) {
   return n * (n + 1) * (n + 2) * (n + 3) / 24;
 }
 
+extern "C" unsigned long long gl_wit_candidates(int sector, int n_modes) {
+  if ((sector != 40 && sector != 42 && sector != 44) || n_modes < 1) return 0;
+  return wit_candidates(sector, (unsigned long long)n_modes);
+}
+
+extern "C" gl_status gl_wit_sector_range(int sector, int n_modes, const int* d_modes, int n_cases,
+                                         const void* d_amp, int nx, int ny, double gravity,
+                                         double depth, double dkx, double dky, double threshold,
+                                         unsigned long long q_begin, unsigned long long q_end,
+                                         void* d_out, void* d_work, size_t work_bytes, void* stream);
+
 extern "C" gl_status gl_wit_sector(int sector, int n_modes, const int* d_modes, int n_cases,
                                    const void* d_amp, int nx, int ny, double gravity, double depth,
                                    double dkx, double dky, double threshold, void* d_out,
-                                   void* d_work, size_t work_bytes, void* stream);
+                                   void* d_work, size_t work_bytes, void* stream) {
+  const unsigned long long all = n_modes > 0 ? wit_candidates(sector, (unsigned long long)n_modes) : 0;
+  return gl_wit_sector_range(sector, n_modes, d_modes, n_cases, d_amp, nx, ny, gravity, depth, dkx,
+                             dky, threshold, 0, all, d_out, d_work, work_bytes, stream);
+}
 
 extern "C" gl_status gl_wit_eta44(int n_modes, const int* d_modes, int n_cases, const void* d_amp,
                                   int nx, int ny, double gravity, double depth, double dkx,
@@ -3974,10 +4089,11 @@ extern "C" gl_status gl_wit_eta44(int n_modes, const int* d_modes, int n_cases, 
                        threshold, d_out, d_work, work_bytes, stream);
 }
 
-extern "C" gl_status gl_wit_sector(int sector, int n_modes, const int* d_modes, int n_cases,
-                                   const void* d_amp, int nx, int ny, double gravity, double depth,
-                                   double dkx, double dky, double threshold, void* d_out,
-                                   void* d_work, size_t work_bytes, void* stream) {
+extern "C" gl_status gl_wit_sector_range(int sector, int n_modes, const int* d_modes, int n_cases,
+                                         const void* d_amp, int nx, int ny, double gravity,
+                                         double depth, double dkx, double dky, double threshold,
+                                         unsigned long long q_begin, unsigned long long q_end,
+                                         void* d_out, void* d_work, size_t work_bytes, void* stream) {
   if (sector != 40 && sector != 42 && sector != 44)
     return fail(GL_ERR_SECTOR, "sector must be 40, 42, or 44");
   if (n_modes < 1 || n_modes > 65535 || n_cases < 1 || !d_modes || !d_amp || !d_out || !d_work)
@@ -3988,6 +4104,9 @@ extern "C" gl_status gl_wit_sector(int sector, int n_modes, const int* d_modes, 
     return fail(GL_ERR_INVALID_ARGUMENT, "gravity, depth, dk and the resonance threshold must be positive");
   if (work_bytes < gl_wit_workspace_size(n_modes))
     return fail(GL_ERR_WORKSPACE, "WIT workspace needs %zu bytes", gl_wit_workspace_size(n_modes));
+  if (q_begin > q_end || q_end > wit_candidates(sector, (unsigned long long)n_modes))
+    return fail(GL_ERR_INVALID_ARGUMENT, "quartet range [%llu, %llu) outside the sector's %llu candidates",
+                q_begin, q_end, wit_candidates(sector, (unsigned long long)n_modes));
   gl_status s = wit_upload_tables();
   if (s != GL_OK) return s;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
@@ -4021,11 +4140,13 @@ extern "C" gl_status gl_wit_sector(int sector, int n_modes, const int* d_modes, 
   a.M = WitModel{gravity, depth};
   a.out = reinterpret_cast<cplx*>(d_out);
   a.stats = reinterpret_cast<WitStats*>(work);
-  a.n_quartets = wit_candidates(sector, (unsigned long long)n_modes);
+  a.q_begin = q_begin;
+  a.n_quartets = q_end;
   a.binom = d_binom;
   a.binom_stride = (int)stride;
   a.sector = sector;
-  const int blocks = (int)std::min<unsigned long long>((a.n_quartets + 127) / 128, 148ull * 32);
+  if (q_end == q_begin) return GL_OK;  // an empty share: zero fields, zero counts
+  const int blocks = (int)std::min<unsigned long long>((q_end - q_begin + 127) / 128, 148ull * 32);
   {
     LaunchScope ls("wit44_kernel", st, 0.0);
     wit44_kernel<<<blocks, 128, 0, st>>>(a);

@@ -153,6 +153,11 @@ gl_status launch_out_rows(const OutArgs& a0, int nuc, cudaStream_t st, const cpl
 gl_status launch_seed_rows(const SeedArgs& a, int nunits, cudaStream_t st, const cplx* tw);
 gl_status launch_combine(const CmbArgs& a, int njobs, cudaStream_t st, const cplx* tw);
 gl_status launch_sfft(const SFft& a, int outer, int sign, cudaStream_t st, const cplx* tw);
+// Final transforms of reference grids that are not powers of two (gl_gen.cuh).
+struct GenColArgs;
+struct GenRowArgs;
+gl_status launch_gen_cols(const GenColArgs& a, int njobs, cudaStream_t st);
+gl_status launch_gen_rows(const GenRowArgs& a, int nuc, cudaStream_t st);
 
 // Row launches by kind family, one translation unit each.  Each returns
 // false when `a.kind` is not in its family or its row length has no

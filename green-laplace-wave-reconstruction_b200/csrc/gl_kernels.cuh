@@ -415,6 +415,11 @@ struct RowArgs {
   int out2_x0, out2_w;
   cplx* out2;              // [job][nout - nout_a][out2_w][n_y]
   int rpb;                 // rows per block (> 1 for short rows; 0 or 1: one)
+  // failure-path test hook (gl_plan_set_wait_test; zero in normal runs):
+  // bytes added to the staged rows' expected transaction count, so that the
+  // bounded wait runs out, and that wait's clock budget (0: BULK_WAIT_CYCLES)
+  unsigned int wait_surplus;
+  long long wait_cycles;
 };
 
 // Pointwise products of each stage; `b` points at the bank rows (bank k at
@@ -802,7 +807,7 @@ __global__ void __launch_bounds__(B192 ? 192 : 256, 2) row_kernel_t(RowArgs a, c
     const int nrows = MULTI ? min(rpb, a.ny - y0) : 1;
     uint32_t bytes = 0;
     for (int q = 0; q < a.ngrp; ++q) bytes += (uint32_t)(a.grp[q].nb * a.grp[q].w * sizeof(cplx));
-    mbar_arrive_expect_tx(bar, bytes * (uint32_t)nrows);
+    mbar_arrive_expect_tx(bar, bytes * (uint32_t)nrows + a.wait_surplus);
     for (int r = 0; r < nrows; ++r) {
       cplx* rb = smem + (size_t)r * nb * L;
       int k0 = 0;
@@ -817,13 +822,18 @@ __global__ void __launch_bounds__(B192 ? 192 : 256, 2) row_kernel_t(RowArgs a, c
     }
   }
   {
-    bool late = !mbar_wait_bounded(bar, 0, BULK_WAIT_CYCLES);
+    const long long budget = a.wait_cycles > 0 ? a.wait_cycles : BULK_WAIT_CYCLES;
+    bool late = !mbar_wait_bounded(bar, 0, budget);
     if (__syncthreads_or(late)) {
       // a copy never landed: flag the unit, give the copies one more bounded
       // wait so none is left writing this block's shared memory, and leave
-      if (threadIdx.x == 0 && a.us && a.jobs_per_unit > 0)
-        atomicCAS(&a.us[job / a.jobs_per_unit].status, 0, (int)GL_ERR_TIMEOUT);
-      mbar_wait_bounded(bar, 0, BULK_WAIT_CYCLES);
+      // (a test's planted surplus is completed first, so that wait ends as
+      // soon as the real copies have landed)
+      if (threadIdx.x == 0) {
+        if (a.us && a.jobs_per_unit > 0) atomicCAS(&a.us[job / a.jobs_per_unit].status, 0, (int)GL_ERR_TIMEOUT);
+        if (a.wait_surplus) mbar_complete_tx(bar, a.wait_surplus);
+      }
+      mbar_wait_bounded(bar, 0, budget);
       return;
     }
   }
@@ -1248,6 +1258,7 @@ struct OutArgs {
   int comp_offset;      // first component slot in the output
   int out_ncomp;        // component slots per unit in the output
   const double* comp_scale;   // physical scale per component of this launch
+  double scale_value;   // the scale of every component when comp_scale is null
   void* out;            // [unit][out_ncomp][ny][nx]
   int real_only;        // write float64 real parts instead of complex
   int rows;             // rows per block
@@ -1273,7 +1284,7 @@ __global__ void __launch_bounds__(256, 2) out_row_kernel(OutArgs a, const cplx* 
   const int yy = active ? y : 0;
   cplx* buf = smem + (size_t)g * L;
   const cplx* row = a.in + ((size_t)uc * a.ny + yy) * a.w;
-  const double s = a.comp_scale[comp];
+  const double s = a.comp_scale ? a.comp_scale[comp] : a.scale_value;
   const size_t base = ((size_t)unit * a.out_ncomp + a.comp_offset + comp) * (size_t)a.ny * n +
                       (size_t)yy * n;
   auto load = [&](int xb) -> cplx {

@@ -7,6 +7,7 @@
 #include "gl_host.h"
 #include "gl_adjoint.cuh"
 #include "gl_modal.cuh"
+#include "gl_gen.cuh"
 
 namespace gl {
 
@@ -168,6 +169,37 @@ gl_status launch_sfft(const SFft& a, int outer, int sign, cudaStream_t st, const
     strided_fft_kernel<-1><<<grid, 256, smem, st>>>(a, tw, cw);
   }
   LAUNCH_CHECK("strided_fft_kernel");
+  return GL_OK;
+}
+
+gl_status launch_gen_cols(const GenColArgs& a0, int njobs, cudaStream_t st) {
+  GenColArgs a = a0;
+  const size_t col_bytes = 2 * (size_t)a.gp.n * sizeof(cplx);
+  a.cw = (int)std::max<size_t>(1, std::min<size_t>((size_t)a.box.w, (96 * 1024) / col_bytes));
+  const size_t smem = (size_t)a.cw * col_bytes;
+  if (smem > SMEM_LIMIT) return fail(GL_ERR_UNSUPPORTED, "column length %d exceeds shared memory", a.gp.n);
+  ensure_smem_attr((const void*)gen_col_kernel, (int)SMEM_LIMIT);
+  dim3 grid((a.box.w + a.cw - 1) / a.cw, njobs, a.nbanks);
+  const double bytes = (double)njobs * a.nbanks * a.box.w * ((double)a.gp.n + a.box.h) * sizeof(cplx);
+  LaunchScope ls("gen_col_kernel", st, bytes);
+  gen_col_kernel<<<grid, 256, smem, st>>>(a);
+  LAUNCH_CHECK("gen_col_kernel");
+  return GL_OK;
+}
+
+gl_status launch_gen_rows(const GenRowArgs& a0, int nuc, cudaStream_t st) {
+  GenRowArgs a = a0;
+  const size_t row_bytes = 2 * (size_t)a.gp.n * sizeof(cplx);
+  a.rows = (int)std::max<size_t>(1, std::min<size_t>((size_t)a.ny, (96 * 1024) / row_bytes));
+  const size_t smem = (size_t)a.rows * row_bytes;
+  if (smem > SMEM_LIMIT) return fail(GL_ERR_UNSUPPORTED, "row length %d exceeds shared memory", a.gp.n);
+  ensure_smem_attr((const void*)gen_row_kernel, (int)SMEM_LIMIT);
+  dim3 grid((a.ny + a.rows - 1) / a.rows, nuc);
+  const double bytes = (double)nuc * a.w * a.ny * sizeof(cplx) +
+                       (double)nuc * a.gp.n * a.ny * (a.real_only ? sizeof(double) : sizeof(cplx));
+  LaunchScope ls("gen_row_kernel", st, bytes);
+  gen_row_kernel<<<grid, 256, smem, st>>>(a);
+  LAUNCH_CHECK("gen_row_kernel");
   return GL_OK;
 }
 

@@ -337,7 +337,8 @@ struct WitArgs {
   WitModel M;
   cplx* out;                // 5 planes [field][case][ny][nx]
   WitStats* stats;
-  unsigned long long n_quartets;   // candidates of the sector
+  unsigned long long q_begin;      // first candidate index of this call
+  unsigned long long n_quartets;   // one past the last candidate index of this call
   const unsigned long long* binom;  // binom[r][v] = C(v, r), r = 1..4, v <= n_modes + 3
   int binom_stride;
   int sector;                       // 44, 40 or 42
@@ -368,7 +369,7 @@ __global__ void __launch_bounds__(128) wit44_kernel(WitArgs a) {
   const unsigned long long* b4 = a.binom + 4 * a.binom_stride;
   const unsigned long long pairs = b2[M + 1];  // M (M + 1) / 2
   (void)b1;
-  for (unsigned long long qi = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (unsigned long long qi = a.q_begin + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
        qi < a.n_quartets; qi += (unsigned long long)gridDim.x * blockDim.x) {
     int idx[4];
     int sign[4] = {1, 1, 1, 1};

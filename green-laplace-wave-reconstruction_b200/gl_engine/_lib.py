@@ -107,6 +107,7 @@ SIGNATURES = {
                                     C.c_size_t, C.c_void_p]),
     "gl_plan_get_info": (C.c_int, [C.c_void_p, C.POINTER(PlanInfo)]),
     "gl_workspace_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
+    "gl_plan_set_wait_test": (C.c_int, [C.c_void_p, C.c_uint, C.c_longlong]),
     "gl_deposit_modes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "gl_execute": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
@@ -138,6 +139,11 @@ SIGNATURES = {
                                 C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                 C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
     "gl_wit_read_sector_stats": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.POINTER(WitStats)]),
+    "gl_wit_candidates": (C.c_ulonglong, [C.c_int, C.c_int]),
+    "gl_wit_sector_range": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                      C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                      C.c_double, C.c_ulonglong, C.c_ulonglong, C.c_void_p,
+                                      C.c_void_p, C.c_size_t, C.c_void_p]),
     "gl_gauss_laguerre": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "gl_dispersion_solve": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.c_double, C.c_double,
                                       C.POINTER(C.c_double)]),

@@ -4,6 +4,13 @@ The GL path shards in two ways:
 
 * independent units (sea states x snapshots): each rank evaluates its own
   contiguous share, no collective on the data path (``shard_units``);
+* the WIT quartet sum: the sector's candidate quartets are split into
+  contiguous, equal-count index ranges (every candidate costs about the
+  same: one 15-subset recursion), each rank sums its share into zeroed field
+  planes, and one all-reduce sums the 5 planes (``wit_sharded`` /
+  ``wit_sector_distributed``): the device form of the reference's
+  per-thread accumulators and serial merge
+  (``paper/order4/cpp/directional_eta4_openmp.cpp:734-745``);
 * one large eta44 field: the GL outer nodes are split across ranks, each rank
   accumulates a partial order-4 spectrum on the small quartic box, one
   all-reduce (NCCL over NVLink on GPUs) sums the partials, and the final
@@ -50,6 +57,68 @@ def eta44_sharded(compute_partial: Callable[[int, int], object], reduce_sum: Cal
     part = compute_partial(b, e) if b < e else zeros()
     total = reduce_sum(part)
     return finalize(part if total is None else total)
+
+
+STAT_SUMS = ("candidates", "kept", "near", "strict_zero_output", "strict_zero_intermediate")
+STAT_MAXES = ("max_residual", "max_strict_zero_source")
+STAT_MINS = ("min_detuning",)
+
+
+def combine_wit_stats(parts: list[dict]) -> dict:
+    """Statistics of the whole sum from those of its shares."""
+    out = {k: sum(int(p[k]) for p in parts) for k in STAT_SUMS}
+    out.update({k: max(float(p[k]) for p in parts) for k in STAT_MAXES})
+    out.update({k: min(float(p[k]) for p in parts) for k in STAT_MINS})
+    return out
+
+
+def wit_sharded(compute_range: Callable[[int, int], tuple], reduce_sum: Callable[[object], object],
+                gather_stats: Callable[[dict], list], count: int, rank: int, world: int):
+    """Quartet-range sharding driver, independent of the backend.
+
+    ``compute_range(begin, end)`` returns (fields, stats) of this rank's
+    share of the ``count`` candidates (zero fields for an empty share),
+    ``reduce_sum(fields)`` sums the field planes over ranks (in place or
+    returned) and ``gather_stats(stats)`` returns every rank's statistics.
+    Every rank returns the full fields and the combined statistics."""
+    b, e = split_range(count, rank, world)
+    fields, stats = compute_range(b, e)
+    total = reduce_sum(fields)
+    return (fields if total is None else total), combine_wit_stats(gather_stats(stats))
+
+
+def wit_sector_distributed(inp, sector: int = 44, *, group=None, device=None):
+    """One WIT sector with its candidate quartets split across the ranks of
+    ``group`` (NCCL on CUDA tensors); every rank returns the summed fields
+    [5][case][ny][nx] (a device tensor) and the combined statistics."""
+    import torch
+    import torch.distributed as dist
+
+    from . import wit
+
+    world = dist.get_world_size(group) if dist.is_initialized() else 1
+    rank = dist.get_rank(group) if dist.is_initialized() else 0
+    m = int(np.asarray(inp.modes).reshape(-1, 2).shape[0])
+    count = wit.candidates(sector, m)
+
+    def compute(b, e):
+        out = wit.wit_sector(inp, sector, device=device, as_numpy=False, q_range=(b, e))
+        planes = torch.stack([out.fields[k] for k in wit.FIELDS])
+        return planes, out.stats
+
+    def reduce_sum(planes):
+        if world > 1:
+            dist.all_reduce(planes, op=dist.ReduceOp.SUM, group=group)
+        return planes
+
+    def gather(stats):
+        if world == 1:
+            return [stats]
+        got = [None] * world
+        dist.all_gather_object(got, stats, group=group)
+        return got
+
+    return wit_sharded(compute, reduce_sum, gather, count, rank, world)
 
 
 def eta44_distributed(spectra, *, dk: float, depth: float, peak_depth: float, rank_gl: int,

@@ -147,29 +147,43 @@ def main(argv=None) -> int:
     return 0
 
 
-def wit_sector(inp: WitInput, sector: int = 44, *, device=None, as_numpy: bool = True) -> WitOutput:
-    """WIT fourth-order fields of one sector (44, 40 or 42) for every amplitude case."""
+def candidates(sector: int, n_modes: int) -> int:
+    """Size of a sector's quartet index space (``gl_wit_candidates``)."""
+    return int(_lib.load().gl_wit_candidates(int(sector), int(n_modes)))
+
+
+def wit_sector(inp: WitInput, sector: int = 44, *, device=None, as_numpy: bool = True,
+               q_range: tuple[int, int] | None = None) -> WitOutput:
+    """WIT fourth-order fields of one sector (44, 40 or 42) for every amplitude case.
+
+    ``q_range`` = (begin, end) restricts the sum to those candidate indices
+    (a rank's share, ``gl_wit_sector_range``); the statistics then count that
+    share only."""
     lib = _lib.load()
     dev = torch.device(device if device is not None else "cuda")
     modes = np.ascontiguousarray(inp.modes, dtype=np.int32).reshape(-1, 2)
     amps = np.ascontiguousarray(inp.amplitudes, dtype=np.complex128).reshape(-1, modes.shape[0])
     m, cases = modes.shape[0], amps.shape[0]
+    total = candidates(sector, m)
+    q0, q1 = (0, total) if q_range is None else (int(q_range[0]), int(q_range[1]))
     with torch.cuda.device(dev):
         d_modes = torch.from_numpy(modes).to(dev)
         d_amp = torch.from_numpy(amps).to(dev)
         out = torch.empty((5, cases, inp.ny, inp.nx), dtype=torch.complex128, device=dev)
         work = torch.empty(int(lib.gl_wit_workspace_size(m)) + 256, dtype=torch.uint8, device=dev)
         stream = torch.cuda.current_stream(dev).cuda_stream
-        _lib.check(lib.gl_wit_sector(int(sector), m, C.c_void_p(d_modes.data_ptr()), cases,
-                                     C.c_void_p(d_amp.data_ptr()), inp.nx, inp.ny, inp.gravity,
-                                     inp.depth, inp.dkx, inp.dky, inp.threshold,
-                                     C.c_void_p(out.data_ptr()), C.c_void_p(work.data_ptr()),
-                                     work.numel(), C.c_void_p(stream)))
+        _lib.check(lib.gl_wit_sector_range(int(sector), m, C.c_void_p(d_modes.data_ptr()), cases,
+                                           C.c_void_p(d_amp.data_ptr()), inp.nx, inp.ny,
+                                           inp.gravity, inp.depth, inp.dkx, inp.dky, inp.threshold,
+                                           q0, q1, C.c_void_p(out.data_ptr()),
+                                           C.c_void_p(work.data_ptr()), work.numel(),
+                                           C.c_void_p(stream)))
         torch.cuda.current_stream(dev).synchronize()
         st = _lib.WitStats()
         _lib.check(lib.gl_wit_read_sector_stats(int(sector), C.c_void_p(work.data_ptr()), m,
                                                 C.byref(st)))
     stats = {name: getattr(st, name) for name, _ in _lib.WitStats._fields_}
+    stats["candidates"] = q1 - q0
     data = out.cpu().numpy() if as_numpy else out
     return WitOutput(fields={name: data[k] for k, name in enumerate(FIELDS)}, stats=stats)
 

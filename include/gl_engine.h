@@ -158,6 +158,16 @@ gl_status gl_eta44_finalize(gl_plan* plan, int n_units, const void* d_partial_su
 /* Device workspace bytes needed by gl_execute (independent of n_units). */
 gl_status gl_workspace_size(const gl_plan* plan, size_t* bytes);
 
+/* Failure-path test hook of the row stages' bounded waits (no counterpart in
+ * the reference; its C++ has no device waits).  With surplus_bytes > 0 every
+ * order-2/3 row launch of this plan expects that many bytes more than its
+ * staged copies deliver, so its wait on them runs out after wait_cycles SM
+ * clocks; the block then marks its unit GL_ERR_TIMEOUT in d_unit_status and
+ * returns with the context intact.  (0, 0) restores normal runs (the wait's
+ * budget is then about 2 s).  Nothing faults and nothing waits without a
+ * bound; the outputs of a timed-out unit are meaningless. */
+gl_status gl_plan_set_wait_test(gl_plan* plan, unsigned int surplus_bytes, long long wait_cycles);
+
 /* Deposit N^2 (a+ib)/h e^{-i omega t} for n_units time snapshots into box
  * spectra [unit][box_h][box_w].  Modes are grouped by destination bin:
  * segment s covers modes seg_offsets[s] .. seg_offsets[s+1]-1 (summed in
@@ -265,20 +275,22 @@ gl_status gl_fft2(int batch, int nx, int ny, const void* d_in, void* d_out, int 
                   void* stream);
 
 /* Physical fields from box spectra without allocating device memory.
- * No counterpart in the reference: it serves callers that cannot call
- * cudaMalloc while they run (work inside a captured CUDA graph or a
- * fixed-budget real-time loop, or a host runtime whose GPU binding only passes
- * buffers it already owns).  out[u] = scale * ifft2(S_u) on the nx x ny grid,
- * S_u being box spectrum u ([n_units][box_h][box_w] complex128, signed-mode
- * origin box_x0, box_y0) embedded at its modes; out is [n_units][ny][nx]
- * complex128, or float64 real parts when real_only != 0.  The same transform
- * gl_execute applies to its final spectra.
+ * No counterpart in the reference.  It serves callers that cannot call
+ * cudaMalloc while they run: a real-time loop with a fixed memory budget,
+ * where an allocation may synchronise the device and miss a deadline, or a
+ * host runtime whose GPU binding only passes buffers it already owns and
+ * allows no allocation behind its own allocator.  out[u] = scale * ifft2(S_u)
+ * on the nx x ny grid, S_u being box spectrum u ([n_units][box_h][box_w]
+ * complex128, signed-mode origin box_x0, box_y0) embedded at its modes; out is
+ * [n_units][ny][nx] complex128, or float64 real parts when real_only != 0.
+ * The same transform gl_execute applies to its final spectra.
  * Scratch: one static device array of 16 MiB per GPU (held until the process
  * exits); n_units * box_w * ny * 16 bytes plus ~66 KB of tables must fit, and
  * larger requests return GL_ERR_WORKSPACE.  The first call on a device looks
- * the array up and fills its tables (synchronising `stream`), so make that
- * first call before any stream capture.  All calls share the array: calls
- * that overlap on the GPU race. */
+ * the array's device address up and fills its tables (synchronising
+ * `stream`), so make that first call before any stream capture.  `scale` is
+ * passed to the kernels by value.  All calls share the array and each one
+ * overwrites what it uses: calls that overlap on the GPU race. */
 gl_status gl_box_synthesize_noalloc(int n_units, int nx, int ny, int box_x0, int box_y0,
                                     int box_w, int box_h, const void* d_box_spectra,
                                     double scale, void* d_out, int real_only, void* stream);
@@ -311,6 +323,22 @@ gl_status gl_wit_sector(int sector, int n_modes, const int* d_modes, int n_cases
                         double dkx, double dky, double threshold, void* d_out, void* d_work,
                         size_t work_bytes, void* stream);
 gl_status gl_wit_read_sector_stats(int sector, const void* d_work, int n_modes, gl_wit_stats* out);
+
+/* Candidate count of a sector (its quartet index space): C(M+3, 4) for 44,
+ * (M(M+1)/2)^2 for 40, C(M+2, 3) M for 42; 0 for bad arguments. */
+unsigned long long gl_wit_candidates(int sector, int n_modes);
+
+/* gl_wit_sector over the candidate indices [q_begin, q_end) only: the device
+ * form of the reference's per-thread quartet shares and their serial merge
+ * (directional_eta4_openmp.cpp:734-745).  Ranks that split [0, candidates)
+ * into contiguous shares and sum their d_out planes (one all-reduce) get
+ * gl_wit_sector's fields; the statistics of the shares add up (counts) or
+ * combine by max / min.  d_out is zeroed by the call, as there. */
+gl_status gl_wit_sector_range(int sector, int n_modes, const int* d_modes, int n_cases,
+                              const void* d_amp, int nx, int ny, double gravity, double depth,
+                              double dkx, double dky, double threshold, unsigned long long q_begin,
+                              unsigned long long q_end, void* d_out, void* d_work,
+                              size_t work_bytes, void* stream);
 
 /* Host FP64 Gauss--Laguerre rule (Golub--Welsch with the moment gate). */
 gl_status gl_gauss_laguerre(int rank, double* nodes, double* weights);

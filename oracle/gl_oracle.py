@@ -327,8 +327,13 @@ INNER_RANKS = (4, 6, 8, 10, 12)
 OUTER_RANKS = (3, 4, 6, 8, 10)
 
 
-def _first_state(damped: np.ndarray, g: Geometry) -> dict:
+def _np_ffts():
+    return np.fft.ifft2, np.fft.fft2
+
+
+def _first_state(damped: np.ndarray, g: Geometry, ffts=None) -> dict:
     """12-field first-order state (``_order3.py:175-193``, multipliers ``:151-172``)."""
+    ifft2, _ = ffts or _np_ffts()
     q2 = g.q**2
     bank = {
         "eta": None,
@@ -344,15 +349,20 @@ def _first_state(damped: np.ndarray, g: Geometry) -> dict:
         "phitz": -g.a,
         "phitzz": -q2,
     }
-    st = {k: np.fft.ifft2(damped if m is None else m * damped) for k, m in bank.items()}
+    st = {k: ifft2(damped if m is None else m * damped) for k, m in bank.items()}
     st["eta_t"] = st["phiz"]
     st["phiz_t"] = st["phitz"]
     st["phizz_t"] = st["phitzz"]
     return st
 
 
-def _pair_state(damped, g: Geometry, out_support, nodes, weights, lam2, shift2) -> dict:
-    """Inner GL loop and the 9 pair fields (``_order3.py:196-272``)."""
+def _pair_state(damped, g: Geometry, out_support, nodes, weights, lam2, shift2,
+                ffts_for=None) -> dict:
+    """Inner GL loop and the 9 pair fields (``_order3.py:196-272``).
+
+    ``ffts_for(i)`` (precision experiments only) gives the (ifft2, fft2) pair
+    of inner node i, ``ffts_for(None)`` that of the 9 pair-field transforms."""
+    ffts_for = ffts_for or (lambda i: _np_ffts())
     q2 = g.q**2
     bank = (None, g.nu, g.nu**2, g.nu**3, g.qx / g.safe_nu, g.qy / g.safe_nu,
             g.qx, g.qy, q2 / g.safe_nu, q2, g.nu * g.qx, g.nu * g.qy)
@@ -360,11 +370,12 @@ def _pair_state(damped, g: Geometry, out_support, nodes, weights, lam2, shift2) 
     et_hat = np.zeros_like(damped)
     p_hat = np.zeros_like(damped)
     pt_hat = np.zeros_like(damped)
-    for x, w in zip(nodes, weights):
+    for i, (x, w) in enumerate(zip(nodes, weights)):
+        ifft2, fft2 = ffts_for(i)
         tau = x / lam2
         d2 = damped * np.exp(-tau * (g.nu - shift2))
         v, v1, v2, v3, hx, hy, jx, jy, rad, qq, njx, njy = (
-            np.fft.ifft2(d2 if m is None else d2 * m) for m in bank
+            ifft2(d2 if m is None else d2 * m) for m in bank
         )
         sources = (
             2.0 * v * v2 + v1**2 - hx**2 - hy**2,
@@ -374,7 +385,7 @@ def _pair_state(damped, g: Geometry, out_support, nodes, weights, lam2, shift2) 
         )
         hats = []
         for src in sources:
-            h = np.fft.fft2(src)
+            h = fft2(src)
             h[~out_support] = 0.0
             hats.append(h)
         sd, sk, sdt, skt = (zero_below_roundoff_floor(h, out_support) for h in hats)
@@ -390,16 +401,17 @@ def _pair_state(damped, g: Geometry, out_support, nodes, weights, lam2, shift2) 
     et_hat = zero_below_roundoff_floor(et_hat, out_support)
     dx = 1j * g.qx
     dy = 1j * g.qy
+    ifft2, _ = ffts_for(None)
     pair = {
-        "eta": np.fft.ifft2(e_hat),
-        "etax": np.fft.ifft2(dx * e_hat),
-        "etay": np.fft.ifft2(dy * e_hat),
-        "phix": np.fft.ifft2(dx * p_hat),
-        "phiy": np.fft.ifft2(dy * p_hat),
-        "phiz": np.fft.ifft2(g.a * p_hat),
-        "phizz": np.fft.ifft2(q2 * p_hat),
-        "phitz": np.fft.ifft2(g.a * pt_hat),
-        "eta_t": np.fft.ifft2(et_hat),
+        "eta": ifft2(e_hat),
+        "etax": ifft2(dx * e_hat),
+        "etay": ifft2(dy * e_hat),
+        "phix": ifft2(dx * p_hat),
+        "phiy": ifft2(dy * p_hat),
+        "phiz": ifft2(g.a * p_hat),
+        "phizz": ifft2(q2 * p_hat),
+        "phitz": ifft2(g.a * pt_hat),
+        "eta_t": ifft2(et_hat),
     }
     pair["phiz_t"] = pair["phitz"]
     return pair
@@ -426,13 +438,18 @@ def _cubic_forcing(f: dict, p: dict):
 
 
 def order3(spectrum: np.ndarray, qx: np.ndarray, qy: np.ndarray, *,
-           inner_rank: int = 4, outer_rank: int = 4, outer_subset=None):
+           inner_rank: int = 4, outer_rank: int = 4, outer_subset=None, ffts_for=None):
     """Nested no-Stokes GL eta33 + psi33 (``_order3.py:18-148``; MATLAB ``gl_no_stokes_eta33.m``).
 
     Returns (eta33/h, psi33/(h sqrt(gh)), audit), complex physical fields.
     ``outer_subset`` (bench sampling only) restricts the outer GL loop to the
     listed node indices, i.e. evaluates that fraction of the graph.
+    ``ffts_for(j, i)`` (precision experiments only) gives the (ifft2, fft2)
+    pair used by outer node j's inner node i, and ``ffts_for(j, None)`` the
+    one of outer node j's own transforms (first-order state, pair fields,
+    forcing); the default is numpy's FP64 pair everywhere.
     """
+    ffts_for = ffts_for or (lambda j, i: _np_ffts())
     if inner_rank not in INNER_RANKS or outer_rank not in OUTER_RANKS:
         raise ValueError("unsupported inner or outer third-order GL rank")
     g = Geometry(qx, qy)
@@ -461,12 +478,14 @@ def order3(spectrum: np.ndarray, qx: np.ndarray, qy: np.ndarray, *,
             continue
         tau = x / lam3
         damped = spectrum * np.exp(-tau * (g.nu - shift3))
-        first = _first_state(damped, g)
-        pair = _pair_state(damped, g, s2, inodes, iweights, lam2, shift2)
+        first = _first_state(damped, g, ffts_for(j, None))
+        pair = _pair_state(damped, g, s2, inodes, iweights, lam2, shift2,
+                           lambda i, j=j: ffts_for(j, i))
         fk, fd, c, ct = _cubic_forcing(first, pair)
+        _, fft2 = ffts_for(j, None)
         hats = []
         for src in (fk, fd, c, ct):
-            h = np.fft.fft2(src)
+            h = fft2(src)
             h[~s3] = 0.0
             hats.append(zero_below_roundoff_floor(h, s3))
         fk_hat, fd_hat, c_hat, ct_hat = hats

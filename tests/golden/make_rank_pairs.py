@@ -5,16 +5,19 @@ The reference's ``green_laplace_order3(spectrum, qx, qy, inner_rank, outer_rank)
 ranks as arguments; its unified API fixes GL4/GL4.  This script evaluates it
 at rank pairs with unequal inner and outer counts on one seeded 64 x 64
 JONSWAP state (t = 0.3 s) and stores its dimensionless eta33 / psi33 fields
-next to the state's mode list, so the oracle's ``order3`` can be checked
-against the reference itself at those ranks.  The analytic spectrum fed to
+next to the state's mode list, so the oracle's ``order3`` and the engine can be
+checked against the reference itself at those ranks.  The equal pairs (6, 6)
+and (8, 8) are the ones the uneven batch workload runs.  The analytic spectrum fed to
 the reference comes from the oracle's deposit restatement, which
 ``test_oracle_golden.py`` pins separately.
 
-Usage: ``python tests/golden/make_rank_pairs.py /path/to/reference``
+Usage: ``python tests/golden/make_rank_pairs.py /path/to/reference`` (or set
+``GL_REFERENCE`` to the reference checkout).
 """
 
 from __future__ import annotations
 
+import os
 import sys
 from pathlib import Path
 
@@ -23,7 +26,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 
-RANK_PAIRS = [(6, 3), (8, 6), (4, 10), (12, 4)]
+RANK_PAIRS = [(6, 3), (8, 6), (4, 10), (12, 4), (6, 6), (8, 8), (10, 10)]
 T = 0.3
 
 
@@ -56,4 +59,7 @@ def main(reference: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    where = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GL_REFERENCE")
+    if not where:
+        sys.exit("usage: make_rank_pairs.py REFERENCE_CHECKOUT (or set GL_REFERENCE)")
+    main(Path(where))

@@ -73,7 +73,7 @@ def _desc(**kw):
 
 @pytest.mark.parametrize("kw,status,text", [
     (dict(order=4), 1, "order"),
-    (dict(nx=48), 2, "power-of-two"),
+    (dict(nx=56), 2, "no prime factor above 5"),
     (dict(nx=63), 1, "even"),
     (dict(box_x0=0), 7, "strict-forward"),
     (dict(box_x0=12, box_w=1), 14, "cubic"),
@@ -98,3 +98,17 @@ def test_null_arguments_are_rejected():
     assert lib.gl_plan_create(None, None) == 1
     assert lib.gl_execute(None, 1, None, 0, None, None, 0, None, None) == 1
     assert lib.gl_workspace_size(None, None) == 1
+
+
+@pytest.mark.parametrize("nx,ny", [(112, 112), (64, 98), (4100, 64), (8, 8)])
+def test_plan_rejects_grids_outside_the_supported_sizes(nx, ny):
+    """Sizes with a prime factor above 5, beyond 4096 or below 16 are refused
+    before any device work (so this runs without a GPU)."""
+    lib = _lib.load()
+    desc = _lib.PlanDesc(nx=nx, ny=ny, lx=100.0, ly=100.0, depth=10.0, gravity=9.81, order=2,
+                         components=0, eta22_rank=4, inner_rank=4, outer_rank=4,
+                         allow_below_model_parent_domain=0, box_x0=1, box_y0=0, box_w=2, box_h=1,
+                         grid=0, max_units=1, output=0)
+    h = C.c_void_p()
+    assert lib.gl_plan_create(C.byref(h), C.byref(desc)) == 2  # GL_ERR_UNSUPPORTED
+    assert "no prime factor above 5" in _lib.last_error()

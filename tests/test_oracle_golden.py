@@ -129,7 +129,8 @@ def test_minkowski_support_matches_direct_sum():
     assert np.array_equal(s2, direct)
 
 
-@pytest.mark.parametrize("inner,outer", [(6, 3), (8, 6), (4, 10), (12, 4)])
+@pytest.mark.parametrize("inner,outer", [(6, 3), (8, 6), (4, 10), (12, 4), (6, 6), (8, 8),
+                                         (10, 10)])
 def test_oracle_order3_rank_pairs_match_reference(rank_pairs, inner, outer):
     """_order3.py:18-26 takes the inner and outer ranks as arguments; the
     oracle's order3 reproduces it at unequal rank pairs."""

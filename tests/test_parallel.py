@@ -132,3 +132,60 @@ def test_eta44_partials_sum_to_monolithic_on_one_gpu():
                                        C.c_size_t(plan.workspace_bytes), C.c_void_p(stream)))
     got = out[0].cpu().numpy()
     assert np.linalg.norm(got - full) / np.linalg.norm(full) < 1e-13
+
+
+def _toy_wit_range(b, e, ny=8, nx=8):
+    """A stand-in share of a quartet sum for the host logic: candidate q adds
+    a value of its own to one bin, and the statistics count and bound it."""
+    out = torch.zeros((5, 1, ny, nx), dtype=torch.complex128)
+    res, det = 0.0, float("inf")
+    for q in range(b, e):
+        out[q % 5, 0, (3 * q) % ny, (7 * q) % nx] += complex(np.sin(q), np.cos(0.5 * q))
+        res = max(res, abs(np.sin(1.3 * q)))
+        det = min(det, 1.0 + abs(np.cos(0.7 * q)))
+    stats = {"candidates": e - b, "kept": (e - b) // 2, "near": (e - b) // 3,
+             "strict_zero_output": 0, "strict_zero_intermediate": e - b - (e - b) // 2,
+             "max_residual": res, "max_strict_zero_source": 0.0, "min_detuning": det}
+    return out, stats
+
+
+def _wit_worker(rank, world, port, q, count):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        def reduce_sum(planes):
+            dist.all_reduce(torch.view_as_real(planes), op=dist.ReduceOp.SUM)
+            return planes
+
+        def gather(stats):
+            got = [None] * world
+            dist.all_gather_object(got, stats)
+            return got
+
+        fields, stats = parallel.wit_sharded(_toy_wit_range, reduce_sum, gather, count, rank, world)
+        q.put((rank, fields.numpy(), stats))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("count", [37, 1])
+def test_wit_quartet_sharding_with_gloo_world2(count):
+    """Two gloo ranks split the candidates, sum their planes with one
+    all-reduce and combine their statistics: both equal the one-rank sum
+    (count 1 leaves rank 1 an empty share)."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_wit_worker, args=(r, 2, port, q, count)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=300) for _ in range(2)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    one, one_stats = _toy_wit_range(0, count)
+    expect = parallel.combine_wit_stats([one_stats])
+    for _, fields, stats in got:
+        assert np.allclose(fields, one.numpy(), rtol=0, atol=1e-12)
+        assert stats == expect

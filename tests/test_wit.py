@@ -109,3 +109,30 @@ def test_wit_reproduces_archived_paper_field():
           f"norm rel {e_norm:.3e}")
     assert res.stats["kept"] == int(gold["n0382/counts"][1])
     assert e_top < 1e-11 and p_top < 1e-11 and e_norm < 1e-11
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tag", ["small24", "s40_small12", "s42_small12"])
+def test_wit_quartet_ranges_sum_to_the_whole_sector(tag):
+    """Sequential stand-in for the multi-GPU split: three contiguous shares of
+    the candidate quartets (one of them empty), summed, give the one-call
+    fields, and their statistics combine to the one-call statistics."""
+    from gl_engine import parallel
+
+    gold = dict(np.load(GOLD / "wit_reference.npz"))
+    inp = _golden_case(gold, tag)
+    sector = int(gold[f"{tag}/sector"])
+    whole = wit.wit_sector(inp, sector)
+    count = wit.candidates(sector, inp.modes.shape[0])
+    assert count == whole.stats["candidates"]
+    cuts = [0, count // 3, count // 3, count]
+    parts = [wit.wit_sector(inp, sector, q_range=(cuts[i], cuts[i + 1])) for i in range(3)]
+    for f in wit.FIELDS:
+        total = sum(p.fields[f] for p in parts)
+        scale = max(np.abs(whole.fields[f]).max(), 1e-300)
+        assert np.abs(total - whole.fields[f]).max() <= 1e-13 * scale, f
+    merged = parallel.combine_wit_stats([p.stats for p in parts])
+    for k in parallel.STAT_SUMS:
+        assert merged[k] == whole.stats[k], k
+    assert merged["min_detuning"] == whole.stats["min_detuning"]
+    assert merged["max_residual"] == whole.stats["max_residual"]

@@ -1,16 +1,19 @@
 """gl_box_synthesize_noalloc: box spectra -> physical field with no device allocation.
 
-Callers that cannot allocate device memory while they run -- work captured
-into a CUDA graph, a fixed-budget real-time loop, or a host runtime whose GPU
-binding only hands over buffers it already owns -- use this entry point.  It
-keeps its scratch in a static device array instead of a caller workspace.
+Callers that cannot allocate device memory while they run -- a real-time
+loop on a fixed memory budget, where cudaMalloc may synchronise the device, or
+a host runtime whose GPU binding only hands over buffers it already owns -- use
+this entry point.  It keeps its scratch in a static device array instead of a
+caller workspace.
 
 These tests call it through the C ABI twice in a row (different sea states,
 boxes and unit counts, so stale scratch from the first call cannot leak into
 the second) and compare each result with the eta11 plane that the workspace-
 based gl_execute computes from the same box spectra: the same transform with
-scale = depth.  Tolerance: relative L2 < 1e-14, the FFT bar of the other GPU
-tests.  The file is collected last so a failure here cannot hide other tests.
+scale = depth.  One more case uses a scale other than the depth and checks the
+result against numpy.fft.ifft2 of the box embedded on the full grid.
+Tolerance: relative L2 < 1e-14, the FFT bar of the other GPU tests.  The file
+is collected last so a failure here cannot hide other tests.
 """
 
 import ctypes as C
@@ -84,6 +87,24 @@ def test_noalloc_real_output_and_repeat():
     second = _noalloc(64, box, spec, st.depth, 2, real_only=True)
     assert rel(first, ref.real) < 1e-14
     assert np.array_equal(first, second)
+
+
+def test_noalloc_matches_numpy_ifft2_of_the_embedded_box():
+    st, box, spec, _ = _workspace_reference(seed=5, n=64, times=[0.4, 1.9])
+    scale = 2.75
+    got = _noalloc(64, box, spec, scale, 2)
+    again = _noalloc(64, box, spec, scale, 2)
+    x0, y0, w, h = box
+    s = spec.cpu().numpy()
+    s = s[..., 0] + 1j * s[..., 1]
+    for u in range(2):
+        full = np.zeros((64, 64), dtype=complex)
+        for iy in range(h):
+            for ix in range(w):
+                full[(y0 + iy) % 64, (x0 + ix) % 64] = s[u, iy, ix]
+        ref = scale * np.fft.ifft2(full)
+        assert rel(got[u], ref) < 1e-14
+        assert rel(again[u], ref) < 1e-14
 
 
 def test_noalloc_rejects_requests_beyond_its_static_scratch():
