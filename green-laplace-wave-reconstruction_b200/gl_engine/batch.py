@@ -1,16 +1,21 @@
 """Uneven batches: many sea states of different grids, orders, ranks and
 depths evaluated as one captured CUDA graph.
 
-Each sea state gets its own plan (grid, box, ranks), all plans share one
-device workspace (their executions are serialised on one stream), every
-input is staged on the device before capture, and the whole batch -- one
-deposit and one gl_execute per sea state -- is captured once and replayed.
-Replays skip the host entirely: no Python, no argument marshalling, no launch
-latency between the ~40 kernels of each sea state.
+Each sea state gets its own plan (grid, box, ranks).  The states are dealt
+to ``lanes`` concurrent streams (longest-first onto the least-loaded lane,
+by estimated transform work); every lane has its own device workspace and
+runs its states one after another, and the lanes run side by side, so the
+small 128^2 / 256^2 states fill the SMs next to the large ones instead of
+leaving them idle.  Every input is staged on the device before capture, and
+the whole batch -- one deposit and one gl_execute per sea state, the lanes as
+parallel branches between one fork and one join -- is captured once and
+replayed.  Replays skip the host entirely: no Python, no argument marshalling,
+no launch latency between the ~40 kernels of each sea state.
 
 ``autotune_group`` times the units-per-launch group size of a plan on the
-device and caches the fastest choice per (grid, order, box) in memory (and in
-a JSON file when ``GL_AUTOTUNE_CACHE`` names one).
+device and ``autotune_lanes`` the lane count of a batch; both cache the
+fastest choice in memory (and in a JSON file when ``GL_AUTOTUNE_CACHE`` names
+one).
 """
 
 from __future__ import annotations
@@ -47,10 +52,17 @@ class _Staged:
     tensors: dict = field(default_factory=dict)
 
 
+def _work_estimate(plan: api.Plan, n_units: int) -> float:
+    """Transform work of one sea state: transforms per unit x the product grid."""
+    info = plan.info
+    return float(info.transforms_per_unit) * info.ncx * info.ncy * max(1, n_units)
+
+
 class BatchRunner:
     """Stage, capture and replay an uneven batch of sea states on one GPU."""
 
-    def __init__(self, items: list[BatchItem], *, device=None, output: str = "real"):
+    def __init__(self, items: list[BatchItem], *, device=None, output: str = "real",
+                 lanes: int = 4):
         self.device = torch.device(device if device is not None else "cuda")
         self.output = _lib.OUT_REAL if output == "real" else _lib.OUT_COMPLEX
         self.items = items
@@ -70,10 +82,24 @@ class BatchRunner:
                                     device=self.device, inner_rank=it.inner_rank,
                                     outer_rank=it.outer_rank)
                 self.staged.append(_Staged(it, plan, dep))
-            ws = max(s.plan.workspace_bytes for s in self.staged)
-            self.workspace = torch.empty(ws + 256, dtype=torch.uint8, device=self.device)
-            self.ws_ptr = (self.workspace.data_ptr() + 255) & ~255
-            self.ws_bytes = ws
+            # lanes: longest first onto the least-loaded lane
+            k = max(1, min(int(lanes), len(self.staged)))
+            load = [0.0] * k
+            self.lane_of = [0] * len(self.staged)
+            order = sorted(range(len(self.staged)), key=lambda i: -_work_estimate(
+                self.staged[i].plan, int(np.size(self.staged[i].item.times))))
+            for i in order:
+                lane = int(np.argmin(load))
+                self.lane_of[i] = lane
+                load[lane] += _work_estimate(self.staged[i].plan, int(np.size(self.staged[i].item.times)))
+            self.lanes = k
+            self.workspaces = []
+            for lane in range(k):
+                ws = max([s.plan.workspace_bytes for i, s in enumerate(self.staged)
+                          if self.lane_of[i] == lane] or [0])
+                buf = torch.empty(ws + 256, dtype=torch.uint8, device=self.device)
+                self.workspaces.append((buf, (buf.data_ptr() + 255) & ~255, ws))
+            self.streams = [torch.cuda.Stream(self.device) for _ in range(k)]
             dtype = torch.float64 if self.output == _lib.OUT_REAL else torch.complex128
             for s in self.staged:
                 dev = self.device
@@ -93,23 +119,38 @@ class BatchRunner:
                 }
         self.units = sum(int(np.size(s.item.times)) for s in self.staged)
 
-    def _enqueue(self, stream: int) -> None:
+    def _enqueue_lane(self, lane: int, stream: int) -> None:
         lib = _lib.load()
         import ctypes as C
 
-        for s in self.staged:
+        _, ws_ptr, ws_bytes = self.workspaces[lane]
+        for i, s in enumerate(self.staged):
+            if self.lane_of[i] != lane:
+                continue
             t = s.tensors
             n = int(t["times"].numel())
             s.plan.deposit(n, t["seg_off"], t["seg_bin"], t["ab"], t["omega"], t["times"],
                            t["spectra"], stream)
             api._engine_call(lib.gl_execute(
                 s.plan.handle, n, C.c_void_p(t["spectra"].data_ptr()), _lib.SPECTRA_BOX,
-                C.c_void_p(t["out"].data_ptr()), C.c_void_p(self.ws_ptr), C.c_size_t(self.ws_bytes),
+                C.c_void_p(t["out"].data_ptr()), C.c_void_p(ws_ptr), C.c_size_t(ws_bytes),
                 C.c_void_p(t["status"].data_ptr()), C.c_void_p(stream)))
+
+    def _enqueue(self, main: torch.cuda.Stream) -> None:
+        """Fork from ``main`` onto the lane streams and join back (in a
+        capture this makes the lanes parallel branches of one graph)."""
+        fork = torch.cuda.Event()
+        fork.record(main)
+        for lane, ls in enumerate(self.streams):
+            ls.wait_event(fork)
+            self._enqueue_lane(lane, ls.cuda_stream)
+            done = torch.cuda.Event()
+            done.record(ls)
+            main.wait_event(done)
 
     def run_eager(self) -> None:
         with torch.cuda.device(self.device):
-            self._enqueue(torch.cuda.current_stream(self.device).cuda_stream)
+            self._enqueue(torch.cuda.current_stream(self.device))
 
     def capture(self) -> None:
         """Warm up once (kernel attributes, caches), then capture the batch."""
@@ -120,7 +161,7 @@ class BatchRunner:
             side = torch.cuda.Stream(self.device)
             with torch.cuda.stream(side):
                 with torch.cuda.graph(g, stream=side):
-                    self._enqueue(side.cuda_stream)
+                    self._enqueue(side)
             self.graph = g
 
     def replay(self) -> None:
@@ -169,16 +210,57 @@ def config3_items(n_states: int = 64, snapshots: int = 8, seed0: int = 0, modes:
 _TUNE: dict = {}
 
 
+def _tune_cache_load() -> None:
+    path = os.environ.get("GL_AUTOTUNE_CACHE")
+    if path and not _TUNE and os.path.exists(path):
+        for k, v in json.load(open(path)).items():
+            _TUNE[k] = v
+
+
+def _tune_cache_store() -> None:
+    path = os.environ.get("GL_AUTOTUNE_CACHE")
+    if path:
+        with open(path, "w") as f:
+            json.dump(_TUNE, f)
+
+
+def autotune_lanes(items: list[BatchItem], *, candidates=(1, 2, 4, 8), device=None,
+                   repeats: int = 2) -> int:
+    """Concurrent lanes that minimise the device time of this batch's replay."""
+    key = repr(("lanes", tuple(sorted((it.nx, it.coeffs.order, it.inner_rank,
+                                       int(it.coeffs.options["eta22_rank"]),
+                                       int(np.size(it.times))) for it in items)), tuple(candidates)))
+    _tune_cache_load()
+    if key in _TUNE:
+        return int(_TUNE[key])
+    best, best_t = None, float("inf")
+    for k in candidates:
+        runner = BatchRunner(items, device=device, lanes=k)
+        runner.capture()
+        runner.replay()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(repeats):
+            runner.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1)
+        del runner
+        if t < best_t:
+            best, best_t = k, t
+    _TUNE[key] = best
+    _tune_cache_store()
+    return int(best)
+
+
 def autotune_group(item: BatchItem, *, candidates=(1, 2, 4, 8, 16), device=None,
                    repeats: int = 3) -> int:
     """Units per launch that minimise device time for this item's plan shape."""
     key = (item.nx, item.ny, item.coeffs.order, item.inner_rank, item.outer_rank,
            api.prepare_deposit(item.coeffs, item.lx, item.ly, item.nx, item.ny).box,
            tuple(item.components))
-    path = os.environ.get("GL_AUTOTUNE_CACHE")
-    if path and not _TUNE and os.path.exists(path):
-        for k, v in json.load(open(path)).items():
-            _TUNE[k] = v
+    _tune_cache_load()
     skey = repr(key)
     if skey in _TUNE:
         return int(_TUNE[skey])
@@ -188,7 +270,7 @@ def autotune_group(item: BatchItem, *, candidates=(1, 2, 4, 8, 16), device=None,
         if g > n:
             continue
         trial = BatchItem(**{**item.__dict__, "group": g})
-        runner = BatchRunner([trial], device=device)
+        runner = BatchRunner([trial], device=device, lanes=1)
         runner.run_eager()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -201,7 +283,5 @@ def autotune_group(item: BatchItem, *, candidates=(1, 2, 4, 8, 16), device=None,
         if t < best_t:
             best, best_t = g, t
     _TUNE[skey] = best
-    if path:
-        with open(path, "w") as f:
-            json.dump(_TUNE, f)
+    _tune_cache_store()
     return int(best)

@@ -107,3 +107,47 @@ def small_order3(seed: int = 0, n: int = 64, modes: int = 24, depth: float = 30.
     length = float(length if length is not None else 2.0 * n)
     return jonswap_sea_state(n=n, length=length, depth=depth, hs=2.0, tp=8.0, modes=modes,
                              seed=seed, order=3)
+
+
+def config5_case(*, peak_kh: float = 1.5, steepness: float = 0.08, modes: int = 1024,
+                 n: int = 1024, seed: int = 0, sigma: float = 0.35, spreading: float = 10.0):
+    """Dimensionless order-4 sea state (g = h = 1) on an n x n grid.
+
+    The lattice step is chosen so the peak sits at |m| = 50 (dk = peak_kh / 50),
+    cells with kh in [0.8, 3] and 4 |m| < n / 2 (the quartic alias guard) are
+    admissible, their density is a Gaussian in kh about ``peak_kh`` (width
+    ``sigma``) times cos^(2 s)(theta / 2) about +x, and the ``modes`` densest
+    cells are kept (deterministic top-density cells, like the reference's
+    dimensionless generator).  Amplitudes |c| ~ sqrt(density), phases uniform
+    from ``seed``, scaled so that steepness = k_p sqrt(sum |c|^2) (k_p |c| for
+    one mode).  Returns a wit.WitInput with one amplitude case."""
+    from .wit import WitInput
+
+    dk = peak_kh / 50.0
+    lim = n // 8
+    m = np.arange(-lim + 1, lim)
+    mx, my = np.meshgrid(m, m)
+    k = dk * np.hypot(mx, my)
+    theta = np.arctan2(my, mx)
+    ok = (mx >= 1) & (k >= 0.8) & (k <= 3.0)
+    dens = np.where(ok, np.exp(-0.5 * ((k - peak_kh) / sigma) ** 2)
+                    * np.cos(theta / 2.0) ** (2.0 * spreading), 0.0)
+    idx = np.argsort(dens.ravel(), kind="stable")[::-1][:modes]
+    if idx.size < modes or dens.ravel()[idx[-1]] <= 0:
+        raise ValueError("not enough admissible lattice cells for the requested mode count")
+    rng = np.random.default_rng(seed)
+    amp = np.sqrt(dens.ravel()[idx]) * np.exp(2j * np.pi * rng.random(modes))
+    amp *= steepness / (peak_kh * np.sqrt(np.sum(np.abs(amp) ** 2)))
+    cells = np.stack([mx.ravel()[idx], my.ravel()[idx]], axis=1).astype(np.int32)
+    return WitInput(modes=cells, amplitudes=amp[None, :], nx=n, ny=n, gravity=1.0, depth=1.0,
+                    dkx=dk, dky=dk, threshold=1e-6)
+
+
+def largest_modes(inp, count: int):
+    """The ``count`` modes of largest amplitude (their original order kept)."""
+    from .wit import WitInput
+
+    keep = np.sort(np.argsort(-np.abs(inp.amplitudes[0]), kind="stable")[:count])
+    return WitInput(modes=inp.modes[keep], amplitudes=inp.amplitudes[:, keep], nx=inp.nx,
+                    ny=inp.ny, gravity=inp.gravity, depth=inp.depth, dkx=inp.dkx, dky=inp.dky,
+                    threshold=inp.threshold)

@@ -5,14 +5,18 @@ published eta44 GL / WIT timings (``paper/order4/data/runtime/*.csv``); the
 bench's order-4 workload reads the copies, since the reference checkout does
 not exist where the bench runs.
 
-Usage: python tests/golden/copy_runtime_inputs.py /path/to/reference
+Usage: python tests/golden/copy_runtime_inputs.py /path/to/reference (or set GL_REFERENCE)
 """
 
+import os
 import shutil
 import sys
 from pathlib import Path
 
-src = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference") / "paper/order4/inputs/runtime"
+where = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GL_REFERENCE")
+if not where:
+    sys.exit("usage: copy_runtime_inputs.py REFERENCE_CHECKOUT (or set GL_REFERENCE)")
+src = Path(where) / "paper/order4/inputs/runtime"
 dst = Path(__file__).resolve().parent / "runtime"
 dst.mkdir(exist_ok=True)
 for d in sorted(src.glob("n*")):

@@ -16,6 +16,7 @@ Usage: ``python tests/golden/make_modal_golden.py /path/to/reference``
 from __future__ import annotations
 
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -83,4 +84,7 @@ def main(reference: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    where = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GL_REFERENCE")
+    if not where:
+        sys.exit("usage: %s REFERENCE_CHECKOUT (or set GL_REFERENCE)" % Path(__file__).name)
+    main(Path(where))

@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import shutil
 import subprocess
+import os
 import sys
 import tempfile
 from pathlib import Path
@@ -84,4 +85,7 @@ def main(reference: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    where = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GL_REFERENCE")
+    if not where:
+        sys.exit("usage: %s REFERENCE_CHECKOUT (or set GL_REFERENCE)" % Path(__file__).name)
+    main(Path(where))

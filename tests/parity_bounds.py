@@ -1,14 +1,25 @@
 """Per-case parity bounds for FP64 engine-vs-oracle tests.
 
-The reference's FFT graph zeroes spectral bins below a roundoff floor
-(``python/src/green_laplace/_spectral.py:52-64``).  Which bins fall below it
-depends on FFT roundoff, so two correct FP64 implementations of the graph
-differ by more than FFT roundoff wherever bins sit near the floor.  The
-oracle measures that spread on each case: it runs the same inputs a second
-time with every 2-D FFT taken in the other axis order (same mathematics,
-different roundoff) and compares the two answers.  The engine must then
-agree with the oracle within ``SPREAD_FACTOR`` times that spread, and never
-worse than the FP64 bar of 1e-12 where the spread is smaller.
+The reference's FFT graph zeroes spectral bins below a roundoff floor,
+16 eps log2(Nx Ny) times the spectrum's peak
+(``python/src/green_laplace/_spectral.py:52-64``), and multiplies node
+spectra by cosh(sqrt(A) tau) responses that amplify whatever survives it.
+Whether a bin within roundoff of that floor is kept is decided by roundoff,
+so two correct FP64 implementations of the graph differ by more than FFT
+roundoff.  The oracle measures that spread on each case by re-running the
+same inputs with only roundoff-level changes:
+
+* every 2-D FFT taken in the other axis order;
+* the input spectrum scaled by 1 + 2^-52 and by 1 - 2^-52;
+* the floor threshold moved by one ulp of the peak, i.e. scaled by
+  1 + 1/(16 log2(Nx Ny)) and 1 - 1/(16 log2(Nx Ny)): a bin whose modulus lies
+  within one ulp of the peak from the threshold has no roundoff-free
+  decision, and any FFT decides it by its own roundoff (on deep-water states
+  at high GL rank one such bin moves eta33 by 1e-5).
+
+The spread is the largest relative L2 change over these runs.  The engine
+must agree with the oracle within ``SPREAD_FACTOR`` times the spread, and
+never worse than the FP64 bar of 1e-12 where the spread is smaller.
 """
 
 from __future__ import annotations
@@ -44,13 +55,56 @@ def swapped_fft_axes():
         F.fft2, F.ifft2 = f2, i2
 
 
-def oracle_with_spread(run):
-    """``run()`` -> {name: field}.  Returns the oracle's fields and, per field,
-    the relative L2 change when only the oracle's FFT roundoff changes."""
+@contextlib.contextmanager
+def floor_threshold_scaled(factor: float):
+    """The oracle's roundoff floor with its threshold times ``factor``."""
+    from oracle import gl_oracle as O
+
+    orig = O.zero_below_roundoff_floor
+
+    def floor(spectrum, support):
+        out = spectrum.copy()
+        mags = np.abs(out[support])
+        if mags.size == 0:
+            return out
+        peak = float(np.max(mags))
+        if peak == 0.0:
+            return out
+        thr = 16.0 * O.EPS * max(1.0, np.log2(out.size)) * factor
+        out[support & (np.abs(out) < thr * peak)] = 0.0
+        return out
+
+    O.zero_below_roundoff_floor = floor
+    try:
+        yield
+    finally:
+        O.zero_below_roundoff_floor = orig
+
+
+PERTURBATIONS = ("axes", "scale+", "scale-", "floor+", "floor-")
+
+
+def perturbed(run, kind: str, grid_points: int):
+    """One roundoff-level re-run of ``run(scale)`` (see the module docstring)."""
+    eps = 2.0 ** -52
+    ulp = 1.0 / (16.0 * np.log2(grid_points))
+    if kind == "axes":
+        with swapped_fft_axes():
+            return run()
+    if kind in ("scale+", "scale-"):
+        return run(1.0 + eps if kind == "scale+" else 1.0 - eps)
+    with floor_threshold_scaled(1.0 + ulp if kind == "floor+" else 1.0 - ulp):
+        return run()
+
+
+def oracle_with_spread(run, grid_points: int):
+    """``run(scale)`` -> {name: field} for the input spectrum times ``scale``
+    (``run()`` uses 1) on a grid of ``grid_points`` = Nx Ny bins.  Returns the
+    oracle's fields and, per field, the largest relative L2 change over the
+    roundoff-level perturbations."""
     base = run()
-    with swapped_fft_axes():
-        alt = run()
-    return base, {k: rel(alt[k], base[k]) for k in base}
+    alts = [perturbed(run, k, grid_points) for k in PERTURBATIONS]
+    return base, {k: max(rel(a[k], base[k]) for a in alts) for k in base}
 
 
 def bound(spread: float) -> float:
@@ -74,26 +128,31 @@ def oracle_surface_with_spread(args: dict):
     arguments, so a spawned process pool can run cases side by side."""
     from oracle import gl_oracle as O
 
-    def run():
+    def run(scale=1.0):
         oc = O.spectral_coefficients(args["order"], args["gravity"], args["depth"], args["a"],
                                      args["b"], args["kx"], args["ky"],
                                      options={"eta22_rank": args["eta22_rank"]})
         n = args["n"]
+        h = args["depth"]
+        kxg, kyg = O.fft_wavenumber_grid(args["lx"], args["ly"], n, n)
+        s = scale * O.deposit_modes(oc["a"], oc["b"], oc["kx"], oc["ky"], oc["omega"], h,
+                                    args["lx"], args["ly"], n, n, args["t"])
         if args["order"] == 3:
-            kxg, kyg = O.fft_wavenumber_grid(args["lx"], args["ly"], n, n)
-            s = O.deposit_modes(oc["a"], oc["b"], oc["kx"], oc["ky"], oc["omega"], args["depth"],
-                                args["lx"], args["ly"], n, n, args["t"])
-            h = args["depth"]
             e, p, _ = O.order3(s, h * kxg, h * kyg, inner_rank=args["inner"],
                                outer_rank=args["outer"])
             ps = h * np.sqrt(args["gravity"] * h)
             full = {"eta33": h * e, "psi33": ps * p}
         else:
-            r = O.spectral_surface(oc, args["lx"], args["ly"], n, n, args["t"])
+            r = O.evaluate_spectrum(s, h * kxg, h * kyg, depth=h, gravity=args["gravity"],
+                                    order=args["order"], eta22_rank=args["eta22_rank"])
             full = {k[:-5]: r[k] for k in r if k.endswith("_plus")}
-        return {k: full[k] for k in args["names"]}
+        # the perturbed runs are compared at the unperturbed scale
+        return {k: full[k] / scale for k in args["names"]}
 
-    return oracle_with_spread(run)
+    if "perturbation" in args:  # one run of a spread, for a process pool
+        kind = args["perturbation"]
+        return run() if kind == "base" else perturbed(run, kind, args["n"] * args["n"])
+    return oracle_with_spread(run, args["n"] * args["n"])
 
 
 def oracle_fields_with_spread(order, gravity, depth, a, b, kx, ky, lx, ly, nx, ny, t,
@@ -102,10 +161,14 @@ def oracle_fields_with_spread(order, gravity, depth, a, b, kx, ky, lx, ly, nx, n
     real parts) with their roundoff spreads."""
     from oracle import gl_oracle as O
 
-    def run():
+    def run(scale=1.0):
         oc = O.spectral_coefficients(order, gravity, depth, a, b, kx, ky,
                                      options={"eta22_rank": eta22_rank})
-        r = O.spectral_surface(oc, lx, ly, nx, ny, t)
-        return {k: v for k, v in r.items() if isinstance(v, np.ndarray)}
+        kxg, kyg = O.fft_wavenumber_grid(lx, ly, nx, ny)
+        s = scale * O.deposit_modes(oc["a"], oc["b"], oc["kx"], oc["ky"], oc["omega"], depth, lx,
+                                    ly, nx, ny, t, oc["options"]["grid_tolerance"])
+        r = O.evaluate_spectrum(s, depth * kxg, depth * kyg, depth=depth, gravity=gravity,
+                                order=order, eta22_rank=eta22_rank)
+        return {k: v / scale for k, v in r.items() if isinstance(v, np.ndarray)}
 
-    return oracle_with_spread(run)
+    return oracle_with_spread(run, nx * ny)

@@ -50,8 +50,30 @@ def test_graph_replay_equals_eager_and_single_calls():
         assert torch.equal(one.fields, got)
 
 
+def test_concurrent_lanes_equal_one_lane():
+    """States dealt to three concurrent lanes (own workspaces, parallel graph
+    branches) give the one-lane results bit for bit."""
+    items = _items()
+    one = batch.BatchRunner(items, lanes=1)
+    one.run_eager()
+    three = batch.BatchRunner(items, lanes=3)
+    assert three.lanes == 3 and len(set(three.lane_of)) == 3
+    three.capture()
+    for t in three.outputs():
+        t[2].zero_()
+    three.replay()
+    torch.cuda.synchronize()
+    one.check()
+    three.check()
+    for (_, _, a), (_, _, b) in zip(one.outputs(), three.outputs()):
+        assert torch.equal(a, b)
+
+
 def test_autotuner_picks_a_candidate():
     item = _items()[1]
     g = batch.autotune_group(item, candidates=(1, 3))
     assert g in (1, 3)
     assert batch.autotune_group(item, candidates=(1, 3)) == g  # cached
+    k = batch.autotune_lanes(_items(), candidates=(1, 2))
+    assert k in (1, 2)
+    assert batch.autotune_lanes(_items(), candidates=(1, 2)) == k

@@ -8,7 +8,8 @@ classes and order-3 GL4/GL4 are checked; order 3 at (6, 6) and (8, 8) on
 1024^2 would take the single-threaded oracle minutes per snapshot, and those
 rank pairs are covered by the 512^2 classes and by the reference's own
 fields in test_gpu_rank_pairs.py.  Bounds: per case, from the oracle's
-roundoff spread (parity_bounds).  The oracle runs in a spawned process pool.
+roundoff spread (parity_bounds).  The oracle's base and perturbed runs go to
+a spawned process pool, one task each.
 """
 
 import multiprocessing as mp
@@ -18,7 +19,7 @@ import pytest
 import torch
 
 from gl_engine import batch
-from parity_bounds import check_fields, oracle_surface_with_spread
+from parity_bounds import PERTURBATIONS, check_fields, oracle_surface_with_spread, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -50,15 +51,21 @@ def test_config3_classes_match_oracle_through_the_graph():
                          eta22_rank=int(c.options["eta22_rank"]), inner=it.inner_rank,
                          outer=it.outer_rank, lx=it.lx, ly=it.ly, n=it.nx, t=float(it.times[0]),
                          names=tuple(it.components)))
+    kinds = ("base",) + PERTURBATIONS
+    tasks = [dict(job, perturbation=k) for job in jobs for k in kinds]
     ctx = mp.get_context("spawn")
-    with ctx.Pool(min(16, mp.cpu_count())) as pool:
-        pending = pool.map_async(oracle_surface_with_spread, jobs)
+    with ctx.Pool(min(32, mp.cpu_count())) as pool:
+        pending = pool.map_async(oracle_surface_with_spread, tasks, chunksize=1)
         runner = batch.BatchRunner(items, output="complex")
         runner.capture()
         runner.replay()
         torch.cuda.synchronize()
         runner.check()
-        results = pending.get()
+        runs = pending.get()
+    results = []
+    for c in range(len(jobs)):
+        base, alts = runs[c * len(kinds)], runs[c * len(kinds) + 1:(c + 1) * len(kinds)]
+        results.append((base, {k: max(rel(a[k], base[k]) for a in alts) for k in base}))
     for (it, names, out), (ref, spread) in zip(runner.outputs(), results):
         got = out[0].cpu().numpy()
         engine = {nm: got[k] for k, nm in enumerate(names)}
