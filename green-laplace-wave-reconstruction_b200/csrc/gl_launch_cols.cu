@@ -49,7 +49,10 @@ const char* col_ifft_name(int kind) {
 gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
   if (!is_pow2(a.n) && !mixed_len(a.n)) return fail(GL_ERR_UNSUPPORTED, "column length %d has no transform", a.n);
   const int cw = fft_cols_per_block(a.n, a.box.w);
-  const size_t smem = ((size_t)cw * padded_len(a.n) + (size_t)cw * a.box.h) * sizeof(cplx);
+  // the damped base spectrum of the block's columns is staged only for the
+  // kinds that share one base across their banks (col_ifft_kernel)
+  const bool shared_base = a.kind != COL_PLAIN && a.kind != COL_OUTER2 && a.kind != COL_FLOORED;
+  const size_t smem = ((size_t)cw * padded_len(a.n) + (shared_base ? (size_t)cw * a.box.h : 0)) * sizeof(cplx);
   // banks per block: at most 4, spread evenly over grid.z (9 banks: 3 x 3)
   const int nz = (a.nbanks + 3) / 4;
   const int bpb = (a.nbanks + nz - 1) / nz;
