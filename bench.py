@@ -650,9 +650,12 @@ def run_config3(args, rank: int, world: int, local_rank: int) -> None:
     torch.cuda.set_device(device)
     items = batch.config3_items(n_states=args.states, snapshots=8, seed0=rank * args.states)
     t_tune = time.perf_counter()
-    lanes = batch.autotune_lanes(items, candidates=(1, 2, 4, 8), device=device)
+    lanes = batch.autotune_lanes(items, candidates=(1, 2, 4, 8, 12, 16), device=device)
     t_tune = time.perf_counter() - t_tune
-    runner = batch.BatchRunner(items, device=device, lanes=lanes)
+    t_tiles = time.perf_counter()
+    runner = batch.BatchRunner(items, device=device, lanes=lanes, tiles="auto")
+    t_tiles = time.perf_counter() - t_tiles
+    tuned = sum(1 for s in runner.staged if any(getattr(s.plan, "tuning", (0, 0, 0))))
     runner.capture()
     for _ in range(max(args.warmup, 1)):
         runner.replay()
@@ -682,13 +685,22 @@ def run_config3(args, rank: int, world: int, local_rank: int) -> None:
     torch.cuda.synchronize()
     kstats = sorted(_lib.profile_end(), key=lambda r: -r["ms_total"])
     ktot = sum(r["ms_total"] for r in kstats) or 1.0
-    # the same batch with one lane (the states one after another), for reference
-    serial = batch.BatchRunner(items, device=device, lanes=1)
+    # the same batch with one lane (the states one after another), and with
+    # the built-in launch shapes, for reference
+    serial = batch.BatchRunner(items, device=device, lanes=1, tiles="auto")
     serial.capture()
     serial.replay()
     torch.cuda.synchronize()
     serial_s = timed(serial.replay)
     del serial
+    for s in runner.staged:
+        s.plan.set_tuning(0, 0, 0)
+    untuned = batch.BatchRunner(items, device=device, lanes=lanes)
+    untuned.capture()
+    untuned.replay()
+    torch.cuda.synchronize()
+    untuned_s = timed(untuned.replay)
+    del untuned
     line = {
         "metric": "config-3 uneven batch units/s (captured graph)", "value": units * args.steps / graph_s,
         "unit": "units/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -701,6 +713,9 @@ def run_config3(args, rank: int, world: int, local_rank: int) -> None:
                   "kernel_launches_per_step": int(launches)},
         "lanes": {"chosen": lanes, "autotune_seconds": t_tune,
                   "one_lane_value": units * args.steps / serial_s},
+        "tiles": {"plans_tuned_off_default": tuned, "plans": len(runner.staged),
+                  "autotune_seconds": t_tiles,
+                  "builtin_shapes_value": units * args.steps / untuned_s},
         "kernel_shares": [{"name": r["name"], "launches": r["launches"],
                            "share": round(r["ms_total"] / ktot, 4)} for r in kstats[:10]],
     }

@@ -11,6 +11,7 @@
 #include <vector>
 #include <atomic>
 #include <mutex>
+#include <initializer_list>
 
 #include "../../include/gl_engine.h"
 #include "gl_kernels.cuh"
@@ -701,6 +702,8 @@ struct gl_plan {
   GenPlan genx, geny;
   cplx* twx = nullptr;
   cplx* twy = nullptr;
+  // launch shapes picked by a tuner (gl_plan_set_tuning); zeros: built-in choices
+  gl_tuning tune = {0, 0, 0};
   // failure-path test hook of the order-2/3 row stages (gl_plan_set_wait_test)
   unsigned int wait_surplus = 0;
   long long wait_cycles = 0;
@@ -1069,6 +1072,21 @@ extern "C" gl_status gl_plan_set_wait_test(gl_plan* p, unsigned int surplus_byte
   return GL_OK;
 }
 
+extern "C" gl_status gl_plan_set_tuning(gl_plan* p, const gl_tuning* t) {
+  if (!p || !t) return fail(GL_ERR_INVALID_ARGUMENT, "null plan or tuning");
+  auto one_of = [](int v, std::initializer_list<int> ok) {
+    for (int o : ok)
+      if (v == o) return true;
+    return false;
+  };
+  if (!one_of(t->pair_row_groups, {0, 2, 4, 8, 16}) || !one_of(t->triple_row_groups, {0, 4, 6, 8, 12, 16}) ||
+      !one_of(t->col_block_columns, {0, 1, 2, 4, 8, 16}))
+    return fail(GL_ERR_INVALID_ARGUMENT,
+                "tuning: pair row groups 0/2/4/8/16, triple row groups 0/4/6/8/12/16, column block 0/1/2/4/8/16");
+  p->tune = *t;
+  return GL_OK;
+}
+
 extern "C" gl_status gl_workspace_size(const gl_plan* p, size_t* bytes) {
   if (!p || !bytes) return fail(GL_ERR_INVALID_ARGUMENT, "null plan or size pointer");
   *bytes = p->ws_total;
@@ -1158,6 +1176,20 @@ static void mink_args(MinkArgs& m, const unsigned long long* a, int ha, int wa, 
   m.skip_dup = 0;
 }
 
+// The plan's tuned launch shapes applied to one stage's arguments.
+static RowArgs tuned(const gl_plan* p, RowArgs r) {
+  r.groups = r.kind == ROW_OUTER ? p->tune.triple_row_groups : p->tune.pair_row_groups;
+  return r;
+}
+static ColArgs tuned(const gl_plan* p, ColArgs a) {
+  a.cw_max = p->tune.col_block_columns;
+  return a;
+}
+static ColFftArgs tuned(const gl_plan* p, ColFftArgs f) {
+  f.cw_max = p->tune.col_block_columns;
+  return f;
+}
+
 // Final transform of box spectra `spec` ([unit][nb][box]) to the reference
 // grid, writing output planes comp_offset.. of each unit.
 static gl_status final_output(gl_plan* p, int gu, const Box& box, const double* geo,
@@ -1219,7 +1251,7 @@ static gl_status final_output(gl_plan* p, int gu, const Box& box, const double* 
   a.n = p->d.ny;
   a.log2n = p->lny;
   a.scale = 1.0 / ((double)p->d.nx * (double)p->d.ny);
-  gl_status s = launch_col_ifft(a, gu, st, p->tw);
+  gl_status s = launch_col_ifft(tuned(p, a), gu, st, p->tw);
   if (s != GL_OK) return s;
   OutArgs o;
   std::memset(&o, 0, sizeof o);
@@ -1465,7 +1497,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     a.n = ncy2;
     a.log2n = p->lncy2;
     a.scale = inv_scale;
-    if ((s = launch_col_ifft(a, njobs, st, p->tw)) != GL_OK) return s;
+    if ((s = launch_col_ifft(tuned(p, a), njobs, st, p->tw)) != GL_OK) return s;
     RowArgs r;
     std::memset(&r, 0, sizeof r);
     r.kind = ROW_ETA22;
@@ -1483,7 +1515,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     r.gmax = ROW_GMAX;
     r.wait_surplus = p->wait_surplus;
     r.wait_cycles = p->wait_cycles;
-    if ((s = launch_row(r, njobs, st, p->tw)) != GL_OK) return s;
+    if ((s = launch_row(tuned(p, r), njobs, st, p->tw)) != GL_OK) return s;
     ColFftArgs f;
     f.in = Q;
     f.out = R;
@@ -1495,7 +1527,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     f.mask = s2;
     f.maxslot = mx;
     f.scale = fwd_scale2;
-    if ((s = launch_col_fft(f, njobs * 2, st, p->tw)) != GL_OK) return s;
+    if ((s = launch_col_fft(tuned(p, f), njobs * 2, st, p->tw)) != GL_OK) return s;
     AccArgs c;
     std::memset(&c, 0, sizeof c);
     c.us = us;
@@ -1546,7 +1578,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     a.n = ncy2;
     a.log2n = p->lncy2;
     a.scale = inv_scale;
-    if ((s = launch_col_ifft(a, njobs_c, st, p->tw)) != GL_OK) return s;
+    if ((s = launch_col_ifft(tuned(p, a), njobs_c, st, p->tw)) != GL_OK) return s;
     RowArgs r;
     std::memset(&r, 0, sizeof r);
     r.kind = ROW_PSI22;
@@ -1566,7 +1598,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     r.gmax = ROW_GMAX;
     r.wait_surplus = p->wait_surplus;
     r.wait_cycles = p->wait_cycles;
-    if ((s = launch_row(r, njobs_r, st, p->tw)) != GL_OK) return s;
+    if ((s = launch_row(tuned(p, r), njobs_r, st, p->tw)) != GL_OK) return s;
     ColFftArgs f;
     f.in = Q;
     f.out = R;
@@ -1578,7 +1610,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     f.mask = nullptr;
     f.maxslot = nullptr;
     f.scale = fwd_scale2;
-    if ((s = launch_col_fft(f, njobs_r * 8, st, p->tw)) != GL_OK) return s;
+    if ((s = launch_col_fft(tuned(p, f), njobs_r * 8, st, p->tw)) != GL_OK) return s;
     // Taylor contact 0.5 eta11 phi1z
     ColArgs cc;
     std::memset(&cc, 0, sizeof cc);
@@ -1597,7 +1629,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     cc.n = ncy2;
     cc.log2n = p->lncy2;
     cc.scale = inv_scale;
-    if ((s = launch_col_ifft(cc, gu, st, p->tw)) != GL_OK) return s;
+    if ((s = launch_col_ifft(tuned(p, cc), gu, st, p->tw)) != GL_OK) return s;
     RowArgs rc;
     std::memset(&rc, 0, sizeof rc);
     rc.kind = ROW_CONTACT22;
@@ -1615,13 +1647,13 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     rc.gmax = ROW_GMAX;
     rc.wait_surplus = p->wait_surplus;
     rc.wait_cycles = p->wait_cycles;
-    if ((s = launch_row(rc, gu, st, p->tw)) != GL_OK) return s;
+    if ((s = launch_row(tuned(p, rc), gu, st, p->tw)) != GL_OK) return s;
     ColFftArgs fc = f;
     fc.in = Qc;
     fc.out = Rc;
     fc.nsrc = 1;
     fc.jobs_per_unit = 1;
-    if ((s = launch_col_fft(fc, gu, st, p->tw)) != GL_OK) return s;
+    if ((s = launch_col_fft(tuned(p, fc), gu, st, p->tw)) != GL_OK) return s;
     AccArgs c;
     std::memset(&c, 0, sizeof c);
     c.us = us;
@@ -1684,7 +1716,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       a.n = ncy2;
       a.log2n = p->lncy2;
       a.scale = inv_scale;
-      if ((s = launch_col_ifft(a, njobs, st, p->tw)) != GL_OK) return s;
+      if ((s = launch_col_ifft(tuned(p, a), njobs, st, p->tw)) != GL_OK) return s;
       RowArgs r;
       std::memset(&r, 0, sizeof r);
       r.kind = ROW_INNER;
@@ -1702,7 +1734,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       r.gmax = ROW_GMAX;
       r.wait_surplus = p->wait_surplus;
       r.wait_cycles = p->wait_cycles;
-      if ((s = launch_row(r, njobs, st, p->tw)) != GL_OK) return s;
+      if ((s = launch_row(tuned(p, r), njobs, st, p->tw)) != GL_OK) return s;
       ColFftArgs f;
       f.in = QI;
       f.out = RI;
@@ -1714,7 +1746,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       f.mask = s2;
       f.maxslot = maxRI;
       f.scale = fwd_scale2;
-      if ((s = launch_col_fft(f, njobs * 4, st, p->tw, "col_fft_kernel[inner]")) != GL_OK) return s;
+      if ((s = launch_col_fft(tuned(p, f), njobs * 4, st, p->tw, "col_fft_kernel[inner]")) != GL_OK) return s;
       AccArgs c;
       std::memset(&c, 0, sizeof c);
       c.us = us;
@@ -1762,7 +1794,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       a.n = ncy3;
       a.log2n = p->lncy3;
       a.scale = inv_scale;
-      if ((s = launch_col_ifft(a, nuj, st, p->tw)) != GL_OK) return s;
+      if ((s = launch_col_ifft(tuned(p, a), nuj, st, p->tw)) != GL_OK) return s;
       ColArgs a2;
       std::memset(&a2, 0, sizeof a2);
       a2.kind = COL_OUTER2;
@@ -1782,7 +1814,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       a2.n = ncy3;
       a2.log2n = p->lncy3;
       a2.scale = inv_scale;
-      if ((s = launch_col_ifft(a2, nuj, st, p->tw)) != GL_OK) return s;
+      if ((s = launch_col_ifft(tuned(p, a2), nuj, st, p->tw)) != GL_OK) return s;
       RowArgs r;
       std::memset(&r, 0, sizeof r);
       r.kind = ROW_OUTER;
@@ -1801,7 +1833,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       r.gmax = ROW_GMAX;
       r.wait_surplus = p->wait_surplus;
       r.wait_cycles = p->wait_cycles;
-      if ((s = launch_row(r, nuj, st, p->tw)) != GL_OK) return s;
+      if ((s = launch_row(tuned(p, r), nuj, st, p->tw)) != GL_OK) return s;
       ColFftArgs f;
       f.in = QO;
       f.out = RO;
@@ -1813,7 +1845,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       f.mask = s3;
       f.maxslot = maxRO;
       f.scale = fwd_scale3;
-      if ((s = launch_col_fft(f, nuj * 4, st, p->tw, "col_fft_kernel[outer]")) != GL_OK) return s;
+      if ((s = launch_col_fft(tuned(p, f), nuj * 4, st, p->tw, "col_fft_kernel[outer]")) != GL_OK) return s;
       AccArgs c;
       std::memset(&c, 0, sizeof c);
       c.us = us;

@@ -197,6 +197,7 @@ struct ColArgs {
   int twins;
   int nout;
   int out_of[MAX_BANKS], twin[MAX_BANKS], twin_fac[MAX_BANKS];
+  int cw_max;              // > 0: at most this many columns per block (a power of two; tuning)
 };
 
 // Damping base value of the job at box bin i (COL_ETA22/PSI22/INNER/OUTER1).
@@ -420,6 +421,7 @@ struct RowArgs {
   // bounded wait runs out, and that wait's clock budget (0: BULK_WAIT_CYCLES)
   unsigned int wait_surplus;
   long long wait_cycles;
+  int groups;              // > 0: transform groups per row block (tuning); 0: built-in choice
 };
 
 // Pointwise products of each stage; `b` points at the bank rows (bank k at
@@ -918,6 +920,7 @@ struct ColFftArgs {
   unsigned long long* maxslot; // [js] or null
   double scale;            // (Nx Ny)/(Ncx Ncy)
   int conj_io = 0;         // 1: + sign transform, conj(F(conj x)) (adjoint seeds)
+  int cw_max = 0;          // > 0: at most this many columns per block (a power of two; tuning)
 };
 
 // One block: `cw` kept columns of one (job, source) spectrum.  Rows of the

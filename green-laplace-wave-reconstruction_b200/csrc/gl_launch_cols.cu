@@ -48,7 +48,7 @@ const char* col_ifft_name(int kind) {
 
 gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, const cplx* tw) {
   if (!is_pow2(a.n) && !mixed_len(a.n)) return fail(GL_ERR_UNSUPPORTED, "column length %d has no transform", a.n);
-  const int cw = fft_cols_per_block(a.n, a.box.w);
+  const int cw = a.cw_max > 0 ? std::min(a.cw_max, fft_cols_per_block(a.n, a.box.w)) : fft_cols_per_block(a.n, a.box.w);
   // the damped base spectrum of the block's columns is staged only for the
   // kinds that share one base across their banks (col_ifft_kernel)
   const bool shared_base = a.kind != COL_PLAIN && a.kind != COL_OUTER2 && a.kind != COL_FLOORED;
@@ -67,7 +67,7 @@ gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, const cp
 
 gl_status launch_col_fft(const ColFftArgs& a, int njs, cudaStream_t st, const cplx* tw, const char* name) {
   if (!is_pow2(a.n) && !mixed_len(a.n)) return fail(GL_ERR_UNSUPPORTED, "column length %d has no transform", a.n);
-  const int cw = fft_cols_per_block(a.n, a.box.w);
+  const int cw = a.cw_max > 0 ? std::min(a.cw_max, fft_cols_per_block(a.n, a.box.w)) : fft_cols_per_block(a.n, a.box.w);
   const size_t smem = (size_t)cw * padded_len(a.n) * sizeof(cplx);
   dim3 grid((a.box.w + cw - 1) / cw, njs);
   const double bytes = (double)njs * a.box.w * (a.n + a.box.h) * sizeof(cplx);

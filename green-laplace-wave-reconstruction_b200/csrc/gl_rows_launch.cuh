@@ -22,6 +22,7 @@ void row_launch(dim3 grid, int T, size_t smem, cudaStream_t st, const RowArgs& a
     G = (nb + rounds - 1) / rounds;
     while ((G * T) % 32 != 0) ++G;
   }
+  if (a.groups > 0) G = std::max(1, std::min(a.groups, 256 / std::max(1, T)));  // a plan's tuning
   // Short rows (fewer than 16 threads per transform) carry little work per
   // block, so a block takes several rows (one team of G groups each) while it
   // stays within 256 threads and ~76 KB of shared memory (3 blocks per SM).

@@ -73,6 +73,11 @@ class Eta20Desc(C.Structure):
                 ("weights", C.POINTER(C.c_double))]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("pair_row_groups", C.c_int), ("triple_row_groups", C.c_int),
+                ("col_block_columns", C.c_int)]
+
+
 class PlanInfo(C.Structure):
     _fields_ = [
         ("ncx", C.c_int), ("ncy", C.c_int),
@@ -108,6 +113,7 @@ SIGNATURES = {
     "gl_plan_get_info": (C.c_int, [C.c_void_p, C.POINTER(PlanInfo)]),
     "gl_workspace_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "gl_plan_set_wait_test": (C.c_int, [C.c_void_p, C.c_uint, C.c_longlong]),
+    "gl_plan_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
     "gl_deposit_modes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "gl_execute": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,

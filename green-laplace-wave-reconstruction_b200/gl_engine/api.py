@@ -220,6 +220,13 @@ class Plan:
     def box(self) -> tuple[int, int, int, int]:
         return tuple(self.info.box1)
 
+    def set_tuning(self, pair_row_groups: int = 0, triple_row_groups: int = 0,
+                   col_block_columns: int = 0) -> None:
+        """Launch shapes of this plan's transform kernels (0: built-in choice)."""
+        t = _lib.Tuning(pair_row_groups, triple_row_groups, col_block_columns)
+        _engine_call(self.lib.gl_plan_set_tuning(self.handle, C.byref(t)))
+        self.tuning = (pair_row_groups, triple_row_groups, col_block_columns)
+
     def _ws_ptr(self) -> int:
         ptr = self.workspace.data_ptr()
         return (ptr + 255) & ~255

@@ -13,9 +13,11 @@ replayed.  Replays skip the host entirely: no Python, no argument marshalling,
 no launch latency between the ~40 kernels of each sea state.
 
 ``autotune_group`` times the units-per-launch group size of a plan on the
-device and ``autotune_lanes`` the lane count of a batch; both cache the
-fastest choice in memory (and in a JSON file when ``GL_AUTOTUNE_CACHE`` names
-one).
+device, ``autotune_tiles`` the launch shapes of its transform kernels
+(transform groups per row block of the pair and triple stages, columns per
+column block: ``Plan.set_tuning``), and ``autotune_lanes`` the lane count of
+a batch; all cache the fastest choice in memory (and in a JSON file when
+``GL_AUTOTUNE_CACHE`` names one).
 """
 
 from __future__ import annotations
@@ -62,7 +64,7 @@ class BatchRunner:
     """Stage, capture and replay an uneven batch of sea states on one GPU."""
 
     def __init__(self, items: list[BatchItem], *, device=None, output: str = "real",
-                 lanes: int = 4):
+                 lanes: int = 4, tiles: str | None = None):
         self.device = torch.device(device if device is not None else "cuda")
         self.output = _lib.OUT_REAL if output == "real" else _lib.OUT_COMPLEX
         self.items = items
@@ -82,6 +84,9 @@ class BatchRunner:
                                     device=self.device, inner_rank=it.inner_rank,
                                     outer_rank=it.outer_rank)
                 self.staged.append(_Staged(it, plan, dep))
+            if tiles == "auto":  # tuned launch shapes per plan shape (cached)
+                for st in self.staged:
+                    st.plan.set_tuning(*autotune_tiles(st.item, device=self.device))
             # lanes: longest first onto the least-loaded lane
             k = max(1, min(int(lanes), len(self.staged)))
             load = [0.0] * k
@@ -285,3 +290,54 @@ def autotune_group(item: BatchItem, *, candidates=(1, 2, 4, 8, 16), device=None,
     _TUNE[skey] = best
     _tune_cache_store()
     return int(best)
+
+
+TILE_CANDIDATES = {"pair_row_groups": (0, 4, 16), "triple_row_groups": (0, 8, 16),
+                   "col_block_columns": (0, 8, 4)}
+
+
+def autotune_tiles(item: BatchItem, *, device=None, repeats: int = 3) -> tuple:
+    """Launch shapes (pair row groups, triple row groups, columns per column
+    block) that minimise one eager run of this item's plan, by coordinate
+    descent from the built-in choices (0) over ``TILE_CANDIDATES``; the plan's
+    shape -- grid, order, ranks, box -- is the cache key."""
+    dep = api.prepare_deposit(item.coeffs, item.lx, item.ly, item.nx, item.ny)
+    key = repr(("tiles", item.nx, item.ny, item.coeffs.order, item.inner_rank, item.outer_rank,
+                int(item.coeffs.options["eta22_rank"]), dep.box, tuple(item.components),
+                int(np.size(item.times)), item.group))
+    _tune_cache_load()
+    if key in _TUNE:
+        return tuple(_TUNE[key])
+    runner = BatchRunner([item], device=device, lanes=1)
+    plan = runner.staged[0].plan
+
+    def timed(cfg):
+        plan.set_tuning(*cfg)
+        runner.run_eager()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(repeats):
+            runner.run_eager()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    best = [0, 0, 0]
+    best_t = timed(tuple(best))
+    for k, name in enumerate(("pair_row_groups", "triple_row_groups", "col_block_columns")):
+        if name == "triple_row_groups" and item.coeffs.order < 3:
+            continue
+        for v in TILE_CANDIDATES[name]:
+            if v == best[k]:
+                continue
+            cfg = list(best)
+            cfg[k] = v
+            t = timed(tuple(cfg))
+            if t < best_t:
+                best, best_t = cfg, t
+    plan.set_tuning(0, 0, 0)
+    _TUNE[key] = list(best)
+    _tune_cache_store()
+    return tuple(best)
+

@@ -80,7 +80,8 @@ typedef enum gl_status {
 typedef struct gl_plan gl_plan;
 
 typedef struct gl_plan_desc {
-  int nx, ny;                 /* reference grid (powers of two, 16..4096)   */
+  int nx, ny;                 /* reference grid: even, 16..4096, prime
+                                 factors 2, 3, 5 only                        */
   double lx, ly;              /* periodic domain lengths                    */
   double depth, gravity;      /* h, g                                       */
   int order;                  /* 1, 2 or 3                                  */
@@ -157,6 +158,21 @@ gl_status gl_eta44_finalize(gl_plan* plan, int n_units, const void* d_partial_su
 
 /* Device workspace bytes needed by gl_execute (independent of n_units). */
 gl_status gl_workspace_size(const gl_plan* plan, size_t* bytes);
+
+/* Launch shapes of a plan's transform kernels, picked by a tuner (no
+ * counterpart in the reference; the batch autotuner of gl_engine/batch.py
+ * times them per plan shape).  Zero keeps the built-in choice.  Results do
+ * not depend on these: only how the rows and columns are spread over
+ * blocks. */
+typedef struct gl_tuning {
+  int pair_row_groups;    /* transform groups per row block of the pair stages
+                             (eta22, psi22, order-3 inner): 0, 2, 4, 8, 16   */
+  int triple_row_groups;  /* the same for the order-3 outer rows: 0, 4, 6, 8,
+                             12, 16                                         */
+  int col_block_columns;  /* at most this many columns per column-transform
+                             block: 0, 1, 2, 4, 8, 16                        */
+} gl_tuning;
+gl_status gl_plan_set_tuning(gl_plan* plan, const gl_tuning* tuning);
 
 /* Failure-path test hook of the row stages' bounded waits (no counterpart in
  * the reference; its C++ has no device waits).  With surplus_bytes > 0 every

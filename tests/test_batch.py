@@ -6,7 +6,7 @@ import pytest
 import torch
 
 import gl_engine
-from gl_engine import api, batch, seastate
+from gl_engine import _lib, api, batch, seastate
 
 pytestmark = pytest.mark.gpu
 
@@ -69,11 +69,35 @@ def test_concurrent_lanes_equal_one_lane():
         assert torch.equal(a, b)
 
 
+def test_launch_shapes_do_not_change_results():
+    """Every tuning of the row groups and column blocks gives the built-in
+    launch's fields bit for bit (only the spreading over blocks changes)."""
+    items = _items()
+    ref = batch.BatchRunner(items, lanes=1)
+    ref.run_eager()
+    torch.cuda.synchronize()
+    want = [t.clone() for _, _, t in ref.outputs()]
+    for cfg in [(4, 8, 8), (16, 16, 4), (2, 12, 1), (8, 6, 16)]:
+        for s in ref.staged:
+            s.plan.set_tuning(*cfg)
+        ref.run_eager()
+        torch.cuda.synchronize()
+        for (_, _, got), w in zip(ref.outputs(), want):
+            assert torch.equal(got, w), cfg
+    for s in ref.staged:
+        s.plan.set_tuning(0, 0, 0)
+    with pytest.raises(_lib.EngineError):
+        ref.staged[0].plan.set_tuning(3, 0, 0)
+
+
 def test_autotuner_picks_a_candidate():
     item = _items()[1]
     g = batch.autotune_group(item, candidates=(1, 3))
     assert g in (1, 3)
     assert batch.autotune_group(item, candidates=(1, 3)) == g  # cached
+    tiles = batch.autotune_tiles(item)
+    assert all(v in batch.TILE_CANDIDATES[n] for v, n in
+               zip(tiles, ("pair_row_groups", "triple_row_groups", "col_block_columns")))
     k = batch.autotune_lanes(_items(), candidates=(1, 2))
     assert k in (1, 2)
     assert batch.autotune_lanes(_items(), candidates=(1, 2)) == k
