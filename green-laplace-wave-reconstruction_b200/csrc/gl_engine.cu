@@ -2243,7 +2243,8 @@ static gl_status e44_finalize(gl_plan* p, int gu, const cplx* OUT, unsigned long
 // the accumulated order-4 spectra (before the final floor) are written there
 // and nothing else is produced; otherwise the fields are finished.
 static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, int o0, int Ro,
-                         cplx* partial, void* outputs, void* ws, int* status, cudaStream_t st) {
+                         cplx* partial, void* outputs, void* ws, int* status, cudaStream_t st,
+                         int part = -2) {
   const int T = 256, R = p->R44;
   const Box B1 = p->b1, B2 = p->b2, B3 = p->b3, B4 = p->b4;
   const int pl1 = B1.w * B1.h, pl2 = B2.w * B2.h, pl3 = B3.w * B3.h, pl4 = B4.w * B4.h;
@@ -2493,9 +2494,13 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     }
     LAUNCH_CHECK("acc_e44_pair_kernel");
   }
-  // ---- stage 2: third level (Ro R jobs per unit)
+  // ---- stage 2: third level (Ro R jobs per unit); the split mode's base part
+  // (part -1) has no third state, and part t >= 0 sums third-level node t alone
   cur = stage_grid(p->ncx3, p->ncy3);
-  {
+  if (part == -1) {
+    CUDA_TRY(cudaMemsetAsync(TS, 0, sizeof(cplx) * (size_t)gu * Ro * nts * pl3, st));
+    CUDA_TRY(cudaMemsetAsync(maxT, 0, (size_t)gu * Ro * nts * 8, st));
+  } else {
     const int nj = gu * Ro * R;
     Bump b;
     cplx* PF = reinterpret_cast<cplx*>(tr + b.take((size_t)nj * 16 * B1.w * cur.ny * sizeof(cplx)));
@@ -2539,6 +2544,7 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     c.outer0 = o0;
     c.floor_rel = p->floor_rel;
     c.nspec = nts;
+    c.only_t1 = part >= 0 ? part + 1 : 0;
     dim3 g(grid_for(pl3, T, 64), gu * Ro);
     {
       LaunchScope ls_("acc_e44_third_kernel", st, 0.0);
@@ -2575,6 +2581,7 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     a3.floor_nsrc = nts;
     if ((s = launch_col_ifft(a3, nj, st, p->tw)) != GL_OK) return s;
     RowArgs r = rowargs(psi ? ROW_E44_ORDER4_PSI : ROW_E44_ORDER4, nf4, B4, Q);
+    r.e44_part = part == -1 ? 1 : part >= 0 ? 2 : 0;
     r.grp[0] = BankGroup{PF, 19, B1.x0, B1.w};
     r.grp[1] = BankGroup{PP, 18, B2.x0, B2.w};
     r.grp[2] = BankGroup{PT, ntb, B3.x0, B3.w};
@@ -2636,6 +2643,39 @@ extern "C" gl_status gl_eta44_execute_partial(gl_plan* p, int n_units, const voi
                           outer_begin, outer_end - outer_begin,
                           reinterpret_cast<cplx*>(d_partial) + (size_t)u0 * part_unit, nullptr, d_ws,
                           d_status ? d_status + u0 : nullptr, st);
+    if (s != GL_OK) return s;
+    if (d_status) {
+      UnitScalars* us = at<UnitScalars>(d_ws, p->o_us);
+      {
+        LaunchScope ls_("status_kernel", st, 0.0);
+        status_kernel<<<(gu + 63) / 64, 64, 0, st>>>(us, gu, d_status + u0);
+      }
+      LAUNCH_CHECK("status_kernel");
+    }
+  }
+  return GL_OK;
+}
+
+extern "C" gl_status gl_eta44_execute_part(gl_plan* p, int n_units, const void* d_spectra, int layout,
+                                           int outer_index, int part_index, void* d_partial, void* d_ws,
+                                           size_t ws_bytes, int* d_status, void* stream) {
+  if (!p || !p->e44) return fail(GL_ERR_INVALID_ARGUMENT, "not an eta44 plan");
+  if (p->e44_psi) return fail(GL_ERR_UNSUPPORTED, "the split mode computes eta44 only");
+  if (outer_index < 0 || outer_index >= p->R44) return fail(GL_ERR_INVALID_ARGUMENT, "outer index");
+  if (part_index >= p->R44 || part_index < -2) return fail(GL_ERR_INVALID_ARGUMENT, "part index");
+  if (n_units < 0 || !d_spectra || !d_partial) return fail(GL_ERR_INVALID_ARGUMENT, "bad arguments");
+  if (layout != GL_SPECTRA_FULL && layout != GL_SPECTRA_BOX)
+    return fail(GL_ERR_INVALID_ARGUMENT, "unknown spectra layout");
+  if (!d_ws || ws_bytes < p->ws_total || (reinterpret_cast<uintptr_t>(d_ws) & 255))
+    return fail(GL_ERR_WORKSPACE, "workspace must be 256-byte aligned and at least %zu bytes", p->ws_total);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const size_t in_unit = layout == GL_SPECTRA_FULL ? (size_t)p->d.nx * p->d.ny : (size_t)p->b1.w * p->b1.h;
+  const size_t part_unit = (size_t)p->ncomp * p->b4.w * p->b4.h;
+  for (int u0 = 0; u0 < n_units; u0 += p->group) {
+    const int gu = std::min(p->group, n_units - u0);
+    gl_status s = e44_run(p, gu, reinterpret_cast<const cplx*>(d_spectra) + (size_t)u0 * in_unit, layout,
+                          outer_index, 1, reinterpret_cast<cplx*>(d_partial) + (size_t)u0 * part_unit,
+                          nullptr, d_ws, d_status ? d_status + u0 : nullptr, st, part_index);
     if (s != GL_OK) return s;
     if (d_status) {
       UnitScalars* us = at<UnitScalars>(d_ws, p->o_us);

@@ -30,6 +30,7 @@ struct E44Acc {
   double floor_rel;
   int nspec;                // third stage: spectra written (3, or 4 with eta_t);
                             // order 4: forcing rows read (2, or 4 with the contact rows)
+  int only_t1;              // third stage: 0 every third-level node, t + 1 node t alone
 };
 
 GL_D void e44_max_reduce(double* v, int n, unsigned long long* slots) {
@@ -116,6 +117,7 @@ __global__ void acc_e44_third_kernel(E44Acc a) {
     const double A = G.a(), sqa = __ldg(a.geo + 5 * plane + i);
     cplx es = czero(), ps = czero(), pts = czero(), ets = czero();
     for (int t = 0; t < R; ++t) {
+      if (a.only_t1 && t != a.only_t1 - 1) continue;
       const int job = uo * R + t;
       const double tt = s_t[t];
       const double co = s_co[t];

@@ -422,6 +422,9 @@ struct RowArgs {
   unsigned int wait_surplus;
   long long wait_cycles;
   int groups;              // > 0: transform groups per row block (tuning); 0: built-in choice
+  // order-4 rows of one part of the reference's split mode: 0 every
+  // partition, 1 the base partitions 22, 211, 1111 only, 2 partition 31 only
+  int e44_part;
 };
 
 // Pointwise products of each stage; `b` points at the bank rows (bank k at
@@ -518,7 +521,7 @@ GL_D void row_products(int kind, cplx* b, int L, int p, int chan_count) {
 // Pointwise products of the order-4 stages (gl_eta44_fftw.cpp), compiled into
 // their own row kernel so that the wide order-4 rows do not weigh on the
 // register allocation of the order-2/3 stages.
-GL_D void row_products_e44(int kind, cplx* b, int L, int p) {
+GL_D void row_products_e44(int kind, cplx* b, int L, int p, int part) {
 #define BK(k) b[(k) * L + p]
   switch (kind) {
     case ROW_E44_PAIR: {  // gl_eta44_fftw.cpp:375-381: six pair sources from 16 banks
@@ -670,8 +673,9 @@ GL_D void row_products_e44(int kind, cplx* b, int L, int p) {
         BK(2) = c;
         BK(3) = ct;
       }
-      BK(0) = cadd(cscale(0.5, k31), kb);
-      BK(1) = cadd(cscale(0.5, d31), db);
+      // split-mode parts (gl_eta44_fftw.cpp:706-735): base partitions or 31 alone
+      BK(0) = part == 1 ? kb : part == 2 ? cscale(0.5, k31) : cadd(cscale(0.5, k31), kb);
+      BK(1) = part == 1 ? db : part == 2 ? cscale(0.5, d31) : cadd(cscale(0.5, d31), db);
       break;
     }
   }
@@ -874,7 +878,7 @@ __global__ void __launch_bounds__(B192 ? 192 : 256, 2) row_kernel_t(RowArgs a, c
       const int chan_count = KIND == ROW_PSI22 ? a.us[job / a.jobs_per_unit].chan_count : 0;
       for (int p = tl; p < n; p += team) row_products(KIND, banks, L, phys(p), chan_count);
     } else if constexpr (FAMILY == 2) {
-      for (int p = tl; p < n; p += team) row_products_e44(KIND, banks, L, phys(p));
+      for (int p = tl; p < n; p += team) row_products_e44(KIND, banks, L, phys(p), a.e44_part);
     } else {
       for (int p = tl; p < n; p += team) row_products_adj(KIND, banks, L, phys(p));
     }

@@ -108,6 +108,9 @@ SIGNATURES = {
     "gl_eta44_execute_partial": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                            C.c_int, C.c_void_p, C.c_void_p, C.c_size_t,
                                            C.c_void_p, C.c_void_p]),
+    "gl_eta44_execute_part": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                        C.c_int, C.c_void_p, C.c_void_p, C.c_size_t,
+                                        C.c_void_p, C.c_void_p]),
     "gl_eta44_finalize": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_size_t, C.c_void_p]),
     "gl_plan_get_info": (C.c_int, [C.c_void_p, C.POINTER(PlanInfo)]),

@@ -172,6 +172,51 @@ def eta44(spectra, *, dk: float, depth: float, peak_depth: float, rank: int, nod
     return (res[:, 0], res[:, 1]) if psi44 else res[:, 0]
 
 
+def eta44_part(spectrum, *, dk: float, depth: float, peak_depth: float, rank: int, outer: int,
+               part: int = -2, nodes=None, weights=None, device=None) -> np.ndarray:
+    """Physical analytic eta44 field of one part of the reference's split mode
+    (``paper/order4/cpp/gl_eta44_fftw.cpp:639-749``): outer GL node ``outer``
+    alone; ``part`` -2 every forcing partition, -1 the base partitions 22,
+    211 and 1111, t >= 0 partition 31 with third-level node t alone.  The
+    part's spectrum gets its own final roundoff floor, as each split process
+    of the reference does; summing the parts' fields is what
+    ``merge_eta44_outer`` does (``merge_main``)."""
+    spectrum = np.asarray(spectrum, dtype=np.complex128)
+    n = spectrum.shape[0]
+    box = _box(np.abs(spectrum))
+    dev = torch.device(device if device is not None else "cuda")
+    keep = None
+    nd = wd = None
+    if nodes is not None:
+        keep = (np.ascontiguousarray(nodes, dtype=float), np.ascontiguousarray(weights, dtype=float))
+        nd = keep[0].ctypes.data_as(C.POINTER(C.c_double))
+        wd = keep[1].ctypes.data_as(C.POINTER(C.c_double))
+    desc = _lib.Eta44Desc(n=n, dk=dk, depth=depth, peak_depth=peak_depth, rank=rank, nodes=nd,
+                          weights=wd, box_x0=box[0], box_y0=box[1], box_w=box[2], box_h=box[3],
+                          max_units=1, output=_lib.OUT_COMPLEX, components=_lib.COMP_ETA44,
+                          gravity=1.0)
+    plan = Eta44Plan(desc, dev, keep)
+    lib = plan.lib
+    b4 = (4 * (box[3] - 1) + 1, 4 * (box[2] - 1) + 1)
+    with torch.cuda.device(dev):
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        spec = torch.view_as_real(torch.from_numpy(np.ascontiguousarray(spectrum[None])).to(dev))
+        partial = torch.zeros((1, 1) + b4, dtype=torch.complex128, device=dev)
+        out = torch.empty((1, 1, n, n), dtype=torch.complex128, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        _engine_call(lib.gl_eta44_execute_part(
+            plan.handle, 1, C.c_void_p(spec.data_ptr()), _lib.SPECTRA_FULL, int(outer), int(part),
+            C.c_void_p(partial.data_ptr()), C.c_void_p(plan._ws_ptr()),
+            C.c_size_t(plan.workspace_bytes), C.c_void_p(status.data_ptr()), C.c_void_p(stream)))
+        _engine_call(lib.gl_eta44_finalize(
+            plan.handle, 1, C.c_void_p(partial.data_ptr()), C.c_void_p(out.data_ptr()),
+            C.c_void_p(plan._ws_ptr()), C.c_size_t(plan.workspace_bytes), C.c_void_p(stream)))
+        st = int(status.item())
+        if st != 0:
+            raise _status_error(st)
+        return out[0, 0].cpu().numpy()
+
+
 def gl_pure_sum_order4(s, qx, qy, qp: float, rank: int = 4, *, device=None):
     """``[eta44, psi44, audit] = gl_pure_sum_order4(s, qx, qy, qp, rank)``
     (``src/gl_pure_sum_order4.m:1-15``): dimensionless analytic eta44/h and
@@ -199,11 +244,11 @@ def gl_pure_sum_order4(s, qx, qy, qp: float, rank: int = 4, *, device=None):
 def main(argv=None) -> int:
     """Command-line twin of the reference's ``gl_eta44`` executable
     (``paper/order4/cpp/gl_eta44_fftw.cpp:639-764``):
-    ``INPUT OUTPUT RANK THREADS``, GLRTI001 in (the rule of RANK taken from
-    the file), GLE44O01 out (the dimensionless field).  The reference's
-    per-outer-node split mode (``[OUTER4_INDEX [PART_INDEX]]``) is a CPU
-    process split; on the GPU the whole graph is one call and multi-GPU
-    sharding goes through ``gl_eta44_execute_partial`` instead."""
+    ``INPUT OUTPUT RANK THREADS [OUTER4_INDEX [PART_INDEX]]``, GLRTI001 in
+    (the rule of RANK taken from the file), GLE44O01 out (the dimensionless
+    field).  With OUTER4_INDEX (and PART_INDEX) it computes that part of the
+    split mode (``eta44_part``), so the reference's split launcher
+    (``paper/order4/run_gl_split.sh``) and merger can drive it."""
     import sys
     import time
 
@@ -211,22 +256,62 @@ def main(argv=None) -> int:
     try:
         if len(argv) not in (5, 6, 7):
             raise ValueError("usage INPUT OUTPUT RANK THREADS [OUTER4_INDEX [PART_INDEX]]")
-        if len(argv) > 5:
-            raise ValueError("split mode (OUTER4_INDEX) is not offered: the GPU runs every outer "
-                             "node in one call")
         rank, threads = int(argv[3]), int(argv[4])
+        requested = int(argv[5]) if len(argv) >= 6 else -1
+        part = int(argv[6]) if len(argv) == 7 else -2
+        if requested >= rank:
+            raise ValueError("outer index")
+        if part >= rank or part < -2:
+            raise ValueError("part index")
+        if len(argv) == 7 and requested < 0:
+            raise ValueError("split mode requires one outer4 index")
         inp = read_glrti(argv[1])
         if rank not in inp.rules:
             raise ValueError("rank")
         nodes, weights = inp.rules[rank]
         t0 = time.perf_counter()
-        field = eta44(inp.spectrum, dk=inp.dk, depth=inp.depth, peak_depth=inp.peak_depth,
-                      rank=rank, nodes=nodes, weights=weights) / inp.depth
+        if requested >= 0:
+            field = eta44_part(inp.spectrum, dk=inp.dk, depth=inp.depth,
+                               peak_depth=inp.peak_depth, rank=rank, outer=requested, part=part,
+                               nodes=nodes, weights=weights) / inp.depth
+        else:
+            field = eta44(inp.spectrum, dk=inp.dk, depth=inp.depth, peak_depth=inp.peak_depth,
+                          rank=rank, nodes=nodes, weights=weights) / inp.depth
         elapsed = time.perf_counter() - t0
         write_gle44(argv[2], inp.n, rank, field, threads=threads, elapsed=elapsed)
     except Exception as exc:  # the reference's error line and exit code
         print(f"CPP_GL_ETA44_ERROR {exc}", file=sys.stderr)
         return 1
-    print(f"CPP_GL_ETA44_DONE n={inp.n} rank={rank} threads={threads} outer=-1 part=-2 "
-          f"elapsed={elapsed}", file=sys.stderr)
+    print(f"CPP_GL_ETA44_DONE n={inp.n} rank={rank} threads={threads} outer={requested} "
+          f"part={part} elapsed={elapsed}", file=sys.stderr)
+    return 0
+
+
+def merge_main(argv=None) -> int:
+    """Command-line twin of the reference's ``merge_eta44_outer``
+    (``paper/order4/cpp/merge_eta44_outer.cpp:12``): ``OUTPUT INPUT1 INPUT2
+    ...``; sums the GLE44O01 fields of the split parts (same n and rank),
+    writes one GLE44O01 whose thread slot holds the part count and whose time
+    is the slowest part's."""
+    import sys
+
+    argv = list(sys.argv if argv is None else argv)
+    try:
+        if len(argv) < 4:
+            raise ValueError("usage OUTPUT INPUT1 INPUT2 ...")
+        total, n, rank, wall = None, 0, 0, 0.0
+        for path in argv[2:]:
+            part = read_gle44(path)
+            if total is None:
+                n, rank, total = part["n"], part["rank"], np.zeros((part["n"], part["n"]), complex)
+            elif part["n"] != n or part["rank"] != rank:
+                raise ValueError("incompatible partial outputs")
+            wall = max(wall, part["elapsed"])
+            total = total + part["field"]
+        write_gle44(argv[1], n, rank, total, threads=len(argv) - 2, elapsed=wall)
+    except Exception as exc:
+        print(f"CPP_GL_ETA44_MERGE_ERROR {exc}", file=sys.stderr)
+        return 1
+    print(f"CPP_GL_ETA44_MERGE rank={rank} partials={len(argv) - 2} max_node_seconds={wall}",
+          file=sys.stderr)
     return 0

@@ -152,6 +152,19 @@ gl_status gl_eta44_execute_partial(gl_plan* plan, int n_units, const void* d_spe
                                    int spectra_layout, int outer_begin, int outer_end,
                                    void* d_partial, void* d_workspace, size_t workspace_bytes,
                                    int* d_unit_status, void* stream);
+/* One part of the reference's split mode (gl_eta44_fftw.cpp:639-647, the
+ * OUTER4_INDEX [PART_INDEX] arguments driven by paper/order4/run_gl_split.sh:
+ * 31-38): outer node `outer_index` alone, and of its quartic forcing every
+ * partition (part_index -2), the base partitions 22, 211 and 1111 (-1), or
+ * partition 31 with the third-level node part_index alone (0 .. rank-1, its
+ * third state floored on its own).  Writes that part's order-4 spectra to
+ * d_partial like gl_eta44_execute_partial; gl_eta44_finalize on it gives the
+ * part's field, which is what the reference writes per part and
+ * merge_eta44_outer.cpp sums.  eta44 plans only (no psi44). */
+gl_status gl_eta44_execute_part(gl_plan* plan, int n_units, const void* d_spectra,
+                                int spectra_layout, int outer_index, int part_index,
+                                void* d_partial, void* d_workspace, size_t workspace_bytes,
+                                int* d_unit_status, void* stream);
 gl_status gl_eta44_finalize(gl_plan* plan, int n_units, const void* d_partial_sum,
                             void* d_outputs, void* d_workspace, size_t workspace_bytes,
                             void* stream);

@@ -228,10 +228,23 @@ def third(g: Grid, s, only=None, eta_t=False):
 
 def order4_forcing(f, p, t):
     """Partitions 31, 22, 211, 1111 of the quartic forcing (``gl_eta44_fftw.cpp:712-735``)."""
+    k31, d31 = order4_forcing_31(f, t)
+    kb, db = order4_forcing_base(f, p)
+    return k31 / 2 + kb, d31 / 2 + db
+
+
+def order4_forcing_31(f, t):
+    """Partition 31 of the quartic forcing (``gl_eta44_fftw.cpp:716-717``)."""
     k31 = (f["px"] * t["ex"] + f["py"] * t["ey"] + t["px"] * f["ex"] + t["py"] * f["ey"]
            - f["eta"] * t["pzz"] - t["eta"] * f["pzz"])
     d31 = (f["eta"] * t["pzt"] + t["eta"] * f["ptz"] + f["px"] * t["px"] + f["py"] * t["py"]
            + f["pz"] * t["pz"])
+    return k31, d31
+
+
+def order4_forcing_base(f, p):
+    """Partitions 22, 211 and 1111 of the quartic forcing, weighted
+    (``gl_eta44_fftw.cpp:721-731``)."""
     k22 = p["px"] * p["ex"] + p["py"] * p["ey"] - p["eta"] * p["pzz"]
     d22 = p["eta"] * p["ptz"] + 0.5 * (p["px"] * p["px"] + p["py"] * p["py"] + p["pz"] * p["pz"])
     fe = f["eta"]
@@ -249,9 +262,7 @@ def order4_forcing(f, p, t):
     d1111 = (fe * fe * fe * f["pzzz_t"] / 6
              + 0.5 * fe * fe * (f["px"] * f["pxzz"] + f["py"] * f["pyzz"] + f["pz"] * f["pzzz"])
              + 0.5 * fe * fe * (f["pxz"] * f["pxz"] + f["pyz"] * f["pyz"] + f["pzz"] * f["pzz"]))
-    ksum = k31 / 2 + (k1111 / 8 + k211 / 4 + k22 / 2)
-    dsum = d31 / 2 + (d1111 / 8 + d211 / 4 + d22 / 2)
-    return ksum, dsum
+    return k1111 / 8 + k211 / 4 + k22 / 2, d1111 / 8 + d211 / 4 + d22 / 2
 
 
 def order4_contact(f, p, t):
@@ -342,6 +353,36 @@ def eta44_partial(spectrum, dk, depth, peak, nodes, weights, outer_subset):
         sh, ch = g.sh_ch(tm)
         out = out + co * (g.A * sh * fd - 1j * ch * fk)
     return out, g.m4
+
+
+def eta44_split_part(spectrum, dk, depth, peak, nodes, weights, outer, part):
+    """One part of the reference's split mode (``gl_eta44_fftw.cpp:639-749``
+    with OUTER4_INDEX = ``outer``, PART_INDEX = ``part``): outer node
+    ``outer`` alone; ``part`` -2 every partition, -1 the base partitions 22,
+    211, 1111 (no third state), t >= 0 partition 31 with the third state of
+    third-level node t alone.  The part's spectrum gets its own final floor
+    and transform; the reference's merger sums the parts' fields."""
+    g = Grid(spectrum, dk, depth, peak, nodes, weights)
+    x, w = g.nodes[outer], g.weights[outer]
+    tm = x / g.l4
+    damp = spectrum * np.exp(-tm * (g.nu - g.shift4))
+    include31 = part == -2 or part >= 0
+    include_base = part in (-2, -1)
+    f = first(g, damp, True)
+    k = d = 0.0
+    if include31:
+        t = third(g, damp, only=part if part >= 0 else None)
+        k31, d31 = order4_forcing_31(f, t)
+        k, d = k + k31 / 2, d + d31 / 2
+    if include_base:
+        p = pair(g, damp, True)
+        kb, db = order4_forcing_base(f, p)
+        k, d = k + kb, d + db
+    fk, fd = (zero_suppress(_fft(a), g.m4) for a in (k, d))
+    co = w * np.exp(x) / g.l4 * np.exp(-4 * g.shift4 * tm)
+    sh, ch = g.sh_ch(tm)
+    out = co * (g.A * sh * fd - 1j * ch * fk)
+    return _ifft(zero_suppress(out, g.m4))
 
 
 def eta44_finalize(out_sum, quartic_mask):

@@ -31,8 +31,15 @@ def test_wit_cli_usage_and_sector_errors(tmp_path):
 def test_gl_eta44_cli_usage_errors(tmp_path):
     r = _run("gl_eta44", "a", "b")
     assert r.returncode == 1 and r.stderr.startswith("CPP_GL_ETA44_ERROR usage")
-    r = _run("gl_eta44", "a", "b", "6", "1", "0")
-    assert r.returncode == 1 and "split mode" in r.stderr
+    # the split mode's argument checks, in the reference's order (before the input is read)
+    r = _run("gl_eta44", "a", "b", "6", "1", "6")
+    assert r.returncode == 1 and r.stderr.strip() == "CPP_GL_ETA44_ERROR outer index"
+    r = _run("gl_eta44", "a", "b", "6", "1", "2", "6")
+    assert r.returncode == 1 and r.stderr.strip() == "CPP_GL_ETA44_ERROR part index"
+    r = _run("gl_eta44", "a", "b", "6", "1", "-1", "0")
+    assert r.returncode == 1 and "split mode requires one outer4 index" in r.stderr
+    r = _run("merge_eta44_outer", "out.bin", "only-one.bin")
+    assert r.returncode == 1 and r.stderr.startswith("CPP_GL_ETA44_MERGE_ERROR usage")
 
 
 @pytest.mark.gpu
@@ -74,3 +81,43 @@ def test_gl_eta44_cli_matches_library_call(tmp_path):
     want = E44.eta44(s, dk=0.25, depth=1.0, peak_depth=1.0, rank=4, nodes=nodes, weights=weights)
     assert got["n"] == 32 and got["rank"] == 4
     assert np.array_equal(got["field"], want / 1.0)
+
+
+@pytest.mark.gpu
+def test_gl_eta44_split_mode_and_merge_follow_the_reference(tmp_path):
+    """The reference's split launcher (paper/order4/run_gl_split.sh:29-38): one
+    process per outer node for the base partitions (PART -1) and one per
+    (outer node, third-level node) for partition 31, then merge_eta44_outer.
+    Each part equals the CPU restatement of that part; the merged field equals
+    the restatement's merge and, here, the one-call field."""
+    from oracle import gl_eta44 as OE
+
+    rng = np.random.default_rng(6)
+    modes = np.array([(1, 0), (2, 1), (3, -1), (2, -2)])
+    c = 0.02 * (rng.standard_normal(4) + 1j * rng.standard_normal(4))
+    s = E44.spectrum_from_modes(modes, c, 32, 1.0)
+    rank = 3
+    nodes, weights = O.gauss_laguerre(rank)
+    E44.write_glrti(tmp_path / "in.bin", E44.GlInput(n=32, dk=0.25, depth=1.0, peak_depth=1.0,
+                                                     rules={rank: (nodes, weights)}, spectrum=s))
+    parts, want = [], 0
+    for outer in range(rank):
+        for part in [-1] + list(range(rank)):
+            out = tmp_path / f"p_{outer}_{part}.bin"
+            r = _run("gl_eta44", tmp_path / "in.bin", out, rank, 1, outer, part)
+            assert r.returncode == 0, r.stderr
+            assert f"outer={outer} part={part}" in r.stderr
+            ref = OE.eta44_split_part(s, 0.25, 1.0, 1.0, nodes, weights, outer, part)
+            got = E44.read_gle44(out)["field"]
+            assert np.linalg.norm(got - ref) <= 1e-9 * np.linalg.norm(ref), (outer, part)
+            parts.append(out)
+            want = want + ref
+    r = _run("merge_eta44_outer", tmp_path / "merged.bin", *parts)
+    assert r.returncode == 0, r.stderr
+    assert f"partials={len(parts)}" in r.stderr
+    merged = E44.read_gle44(tmp_path / "merged.bin")
+    assert merged["rank"] == rank and merged["threads"] == len(parts)
+    assert np.linalg.norm(merged["field"] - want) <= 1e-9 * np.linalg.norm(want)
+    mono = OE.eta44(s, 0.25, 1.0, 1.0, nodes, weights)
+    assert np.linalg.norm(merged["field"] - mono) <= 1e-9 * np.linalg.norm(mono)
+

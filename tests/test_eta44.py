@@ -164,3 +164,18 @@ def test_psi44_approaches_wit_with_rank():
         errs.append(100 * rel(np.real(p), ref))
         print(f"GL{rank} psi44 vs WIT psi: raw rel L2 {errs[-1]:.4f} %")
     assert errs[0] > errs[1] > errs[2]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed,rank,outer,part", [(0, 2, 1, -2), (1, 3, 0, -1), (1, 3, 2, 1),
+                                                  (2, 4, 3, 0), (2, 4, 1, 3)])
+def test_split_parts_match_cpu_restatement(seed, rank, outer, part):
+    """One part of the reference's split mode (outer node, base or partition
+    31 with one third-level node) against its CPU restatement."""
+    s = _small(seed)
+    nodes, weights = O.gauss_laguerre(rank)
+    ref = OE.eta44_split_part(s, 0.25, 1.0, 1.0, nodes, weights, outer, part)
+    got = E44.eta44_part(s, dk=0.25, depth=1.0, peak_depth=1.0, rank=rank, outer=outer, part=part)
+    err = rel(got, ref)
+    print(f"seed {seed} GL{rank} outer {outer} part {part}: rel L2 {err:.3e}")
+    assert err < 1e-9
