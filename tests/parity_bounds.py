@@ -81,11 +81,35 @@ def floor_threshold_scaled(factor: float):
         O.zero_below_roundoff_floor = orig
 
 
+@contextlib.contextmanager
+def eta44_floor_threshold_scaled(factor: float):
+    """The order-4 oracle's roundoff floor (``oracle/gl_eta44.py``) with its
+    threshold times ``factor``."""
+    from oracle import gl_eta44 as OE
+
+    orig = OE.zero_suppress
+
+    def zero_suppress(x, mask):
+        x = np.where(mask, x, 0.0)
+        peak = float(np.max(np.abs(x[mask]))) if np.any(mask) else 0.0
+        thr = 16 * OE.EPS * max(1.0, np.log2(x.size)) * factor
+        if peak:
+            x = np.where(mask & (np.abs(x) < thr * peak), 0.0, x)
+        return x
+
+    OE.zero_suppress = zero_suppress
+    try:
+        yield
+    finally:
+        OE.zero_suppress = orig
+
+
 PERTURBATIONS = ("axes", "scale+", "scale-", "floor+", "floor-")
 
 
-def perturbed(run, kind: str, grid_points: int):
-    """One roundoff-level re-run of ``run(scale)`` (see the module docstring)."""
+def perturbed(run, kind: str, grid_points: int, floor_scaled=floor_threshold_scaled):
+    """One roundoff-level re-run of ``run(scale)`` (see the module docstring);
+    ``floor_scaled`` is the oracle's floor-threshold context."""
     eps = 2.0 ** -52
     ulp = 1.0 / (16.0 * np.log2(grid_points))
     if kind == "axes":
@@ -93,18 +117,28 @@ def perturbed(run, kind: str, grid_points: int):
             return run()
     if kind in ("scale+", "scale-"):
         return run(1.0 + eps if kind == "scale+" else 1.0 - eps)
-    with floor_threshold_scaled(1.0 + ulp if kind == "floor+" else 1.0 - ulp):
+    with floor_scaled(1.0 + ulp if kind == "floor+" else 1.0 - ulp):
         return run()
 
 
-def oracle_with_spread(run, grid_points: int):
+def oracle_with_spread(run, grid_points: int, floor_scaled=floor_threshold_scaled):
     """``run(scale)`` -> {name: field} for the input spectrum times ``scale``
     (``run()`` uses 1) on a grid of ``grid_points`` = Nx Ny bins.  Returns the
     oracle's fields and, per field, the largest relative L2 change over the
     roundoff-level perturbations."""
     base = run()
-    alts = [perturbed(run, k, grid_points) for k in PERTURBATIONS]
+    alts = [perturbed(run, k, grid_points, floor_scaled) for k in PERTURBATIONS]
     return base, {k: max(rel(a[k], base[k]) for a in alts) for k in base}
+
+
+def eta44_oracle_with_spread(call, spectrum):
+    """``call(spectrum)`` -> field of the order-4 oracle.  Returns its field
+    and its roundoff spread (same perturbations, the order-4 floor)."""
+    def run(scale=1.0):
+        return {"f": call(spectrum * scale) / scale}
+
+    base, spread = oracle_with_spread(run, spectrum.size, eta44_floor_threshold_scaled)
+    return base["f"], spread["f"]
 
 
 def bound(spread: float) -> float:

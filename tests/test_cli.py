@@ -88,9 +88,11 @@ def test_gl_eta44_split_mode_and_merge_follow_the_reference(tmp_path):
     """The reference's split launcher (paper/order4/run_gl_split.sh:29-38): one
     process per outer node for the base partitions (PART -1) and one per
     (outer node, third-level node) for partition 31, then merge_eta44_outer.
-    Each part equals the CPU restatement of that part; the merged field equals
-    the restatement's merge and, here, the one-call field."""
+    Each part equals the CPU restatement of that part within the
+    restatement's roundoff spread (parity_bounds); the merged field equals the
+    restatement's merge and, here, the one-call field."""
     from oracle import gl_eta44 as OE
+    from parity_bounds import bound, eta44_oracle_with_spread
 
     rng = np.random.default_rng(6)
     modes = np.array([(1, 0), (2, 1), (3, -1), (2, -2)])
@@ -100,24 +102,28 @@ def test_gl_eta44_split_mode_and_merge_follow_the_reference(tmp_path):
     nodes, weights = O.gauss_laguerre(rank)
     E44.write_glrti(tmp_path / "in.bin", E44.GlInput(n=32, dk=0.25, depth=1.0, peak_depth=1.0,
                                                      rules={rank: (nodes, weights)}, spectrum=s))
-    parts, want = [], 0
+    parts, want, budget = [], 0, 0.0
     for outer in range(rank):
         for part in [-1] + list(range(rank)):
             out = tmp_path / f"p_{outer}_{part}.bin"
             r = _run("gl_eta44", tmp_path / "in.bin", out, rank, 1, outer, part)
             assert r.returncode == 0, r.stderr
             assert f"outer={outer} part={part}" in r.stderr
-            ref = OE.eta44_split_part(s, 0.25, 1.0, 1.0, nodes, weights, outer, part)
+            ref, spread = eta44_oracle_with_spread(
+                lambda x, o=outer, q=part: OE.eta44_split_part(x, 0.25, 1.0, 1.0, nodes, weights,
+                                                              o, q), s)
             got = E44.read_gle44(out)["field"]
-            assert np.linalg.norm(got - ref) <= 1e-9 * np.linalg.norm(ref), (outer, part)
+            assert np.linalg.norm(got - ref) <= bound(spread) * np.linalg.norm(ref), (outer, part)
             parts.append(out)
             want = want + ref
+            budget += bound(spread) * np.linalg.norm(ref)
     r = _run("merge_eta44_outer", tmp_path / "merged.bin", *parts)
     assert r.returncode == 0, r.stderr
     assert f"partials={len(parts)}" in r.stderr
     merged = E44.read_gle44(tmp_path / "merged.bin")
     assert merged["rank"] == rank and merged["threads"] == len(parts)
-    assert np.linalg.norm(merged["field"] - want) <= 1e-9 * np.linalg.norm(want)
+    # the merge adds the parts' deviations at most
+    assert np.linalg.norm(merged["field"] - want) <= budget + 1e-12 * np.linalg.norm(want)
     mono = OE.eta44(s, 0.25, 1.0, 1.0, nodes, weights)
-    assert np.linalg.norm(merged["field"] - mono) <= 1e-9 * np.linalg.norm(mono)
+    assert np.linalg.norm(want - mono) <= 1e-12 * np.linalg.norm(mono)
 
