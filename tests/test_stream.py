@@ -11,12 +11,17 @@ from gl_engine import api, seastate
 pytestmark = pytest.mark.gpu
 
 
-def test_stream_results_equal_device_batches():
+@pytest.mark.parametrize("graphs", [True, False])
+def test_stream_results_equal_device_batches(graphs):
+    """Replayed graphs (inputs copied from pinned staging each batch) and
+    eager launches both give the device-resident evaluation bit for bit,
+    also when the batch size changes mid-stream."""
     st = seastate.small_order3(seed=9, n=64, modes=16)
     c = api.gl_spectral_coefficients(3, st.gravity, st.depth, st.a, st.b, st.kx, st.ky,
                                      0, 0, {"eta22_rank": 4})
-    batches = [[0.0, 0.4], [1.1, 2.5], [3.0, 0.2], [7.5, 9.0], [0.0, 0.4]]
-    ss = api.SurfaceStream(c, st.lx, st.ly, 64, 64, components=["eta33", "psi33"], output="real")
+    batches = [[0.0, 0.4], [1.1, 2.5], [3.0, 0.2], [7.5, 9.0, 4.0], [0.0, 0.4], [2.2, 3.3]]
+    ss = api.SurfaceStream(c, st.lx, st.ly, 64, 64, components=["eta33", "psi33"], output="real",
+                           graphs=graphs)
     tickets, got = [], []
     for times in batches:
         tickets.append(ss.submit(times))
