@@ -707,6 +707,16 @@ struct gl_plan {
   // failure-path test hook of the order-2/3 row stages (gl_plan_set_wait_test)
   unsigned int wait_surplus = 0;
   long long wait_cycles = 0;
+  // concurrent lanes (gl_plan_set_lanes): `lanes` workspace regions of
+  // lane_bytes each, one per stream; lane 0 is the caller's stream, the others
+  // are the plan's own streams, forked from and joined back to the caller's
+  // stream by events; the mutex keeps one call's fork/join records together
+  int device = 0;
+  int lanes = 1;
+  size_t lane_bytes = 0;
+  cudaStream_t lane_st[GL_MAX_LANES] = {};
+  cudaEvent_t lane_ev[GL_MAX_LANES] = {};
+  std::mutex lane_mu;
 };
 
 // Smallest column-transform length >= v: a power of two (>= 16) or one of the
@@ -783,7 +793,6 @@ static size_t stage_scratch(const gl_plan* p, int g) {
     out.take(g * J * 9 * p->b2.w * ncy * c);
     out.take(g * J * 4 * p->b3.w * ncy * c);
     out.take(g * J * 4 * b3 * c);
-    out.take(g * J * 2 * b3 * c);
     upd(out.off);
     (void)base;
   }
@@ -815,7 +824,41 @@ static void plan_free(gl_plan* p) {
   cudaFree(p->comp_scale);
   cudaFree(p->twx);
   cudaFree(p->twy);
+  for (int l = 0; l < GL_MAX_LANES; ++l) {
+    if (p->lane_st[l]) cudaStreamDestroy(p->lane_st[l]);
+    if (p->lane_ev[l]) cudaEventDestroy(p->lane_ev[l]);
+  }
   delete p;
+}
+
+// Workspace layout of an order-1..3 plan for groups of g units (byte offsets
+// into one lane's region); returns the lane's size, a multiple of 256 bytes.
+static size_t layout_units(gl_plan* p, int g) {
+  p->group = g;
+  const size_t c = sizeof(cplx);
+  const size_t b1 = (size_t)p->b1.w * p->b1.h, b2 = (size_t)p->b2.w * p->b2.h,
+               b3 = (size_t)p->b3.w * p->b3.h;
+  Bump b;
+  p->o_slots = b.take(g * sizeof(UnitSlots));
+  p->o_us = b.take(g * sizeof(UnitScalars));
+  p->o_box = b.take(g * b1 * c);
+  p->o_s1 = b.take(g * b1);
+  p->o_s1f = b.take((size_t)g * p->b1.h * p->ww1 * 8);
+  p->o_s1r = b.take((size_t)g * p->b1.h * p->ww1 * 8);
+  p->o_s2 = b.take(g * b2);
+  p->o_s2f = b.take((size_t)g * p->b2.h * p->ww2 * 8);
+  p->o_s2r = b.take((size_t)g * p->b2.h * p->ww2 * 8);
+  p->o_s3 = b.take(g * b3);
+  p->o_ch = b.take(g * 2 * b1);
+  p->o_chf = b.take((size_t)g * 2 * p->b1.h * p->ww1 * 8);
+  p->o_chr = b.take((size_t)g * 2 * p->b1.h * p->ww1 * 8);
+  p->o_pm = b.take(g * 3 * b2);
+  p->o_out22 = b.take(g * b2 * c);
+  p->o_outp22 = b.take(g * b2 * c);
+  p->o_out33 = b.take(g * 2 * b3 * c);
+  p->scratch_bytes = stage_scratch(p, g);
+  p->o_scratch = b.take(p->scratch_bytes);
+  return b.off;
 }
 
 extern "C" gl_status gl_plan_create(gl_plan** out, const gl_plan_desc* desc) {
@@ -994,33 +1037,10 @@ extern "C" gl_status gl_plan_create(gl_plan** out, const gl_plan_desc* desc) {
     plan_free(p);
     return fail(GL_ERR_CUDA, "plan set-up failed: %s", cudaGetErrorString(e));
   }
-  // workspace layout
-  const int g = d.max_units;
-  p->group = g;
-  const size_t c = sizeof(cplx);
-  const size_t b1 = (size_t)p->b1.w * p->b1.h, b2 = (size_t)p->b2.w * p->b2.h,
-               b3 = (size_t)p->b3.w * p->b3.h;
-  Bump b;
-  p->o_slots = b.take(g * sizeof(UnitSlots));
-  p->o_us = b.take(g * sizeof(UnitScalars));
-  p->o_box = b.take(g * b1 * c);
-  p->o_s1 = b.take(g * b1);
-  p->o_s1f = b.take((size_t)g * p->b1.h * p->ww1 * 8);
-  p->o_s1r = b.take((size_t)g * p->b1.h * p->ww1 * 8);
-  p->o_s2 = b.take(g * b2);
-  p->o_s2f = b.take((size_t)g * p->b2.h * p->ww2 * 8);
-  p->o_s2r = b.take((size_t)g * p->b2.h * p->ww2 * 8);
-  p->o_s3 = b.take(g * b3);
-  p->o_ch = b.take(g * 2 * b1);
-  p->o_chf = b.take((size_t)g * 2 * p->b1.h * p->ww1 * 8);
-  p->o_chr = b.take((size_t)g * 2 * p->b1.h * p->ww1 * 8);
-  p->o_pm = b.take(g * 3 * b2);
-  p->o_out22 = b.take(g * b2 * c);
-  p->o_outp22 = b.take(g * b2 * c);
-  p->o_out33 = b.take(g * 2 * b3 * c);
-  p->scratch_bytes = stage_scratch(p, g);
-  p->o_scratch = b.take(p->scratch_bytes);
-  p->ws_total = b.off;
+  // workspace layout (one lane of max_units units until gl_plan_set_lanes)
+  p->lane_bytes = layout_units(p, d.max_units);
+  p->ws_total = p->lane_bytes;
+  if (cudaGetDevice(&p->device) != cudaSuccess) p->device = 0;
   *out = p;
   return GL_OK;
 }
@@ -1084,6 +1104,32 @@ extern "C" gl_status gl_plan_set_tuning(gl_plan* p, const gl_tuning* t) {
     return fail(GL_ERR_INVALID_ARGUMENT,
                 "tuning: pair row groups 0/2/4/8/16, triple row groups 0/4/6/8/12/16, column block 0/1/2/4/8/16");
   p->tune = *t;
+  return GL_OK;
+}
+
+extern "C" gl_status gl_plan_set_lanes(gl_plan* p, int lanes) {
+  if (!p) return fail(GL_ERR_INVALID_ARGUMENT, "null plan");
+  if (p->e44) return fail(GL_ERR_UNSUPPORTED, "concurrent lanes run the order-1..3 plans only");
+  if (lanes < 1 || lanes > GL_MAX_LANES)
+    return fail(GL_ERR_INVALID_ARGUMENT, "lanes must be 1..%d (got %d)", GL_MAX_LANES, lanes);
+  lanes = std::min(lanes, p->d.max_units);  // at least one unit per lane
+  std::lock_guard<std::mutex> lk(p->lane_mu);
+  int cur = 0;
+  CUDA_TRY(cudaGetDevice(&cur));
+  CUDA_TRY(cudaSetDevice(p->device));
+  cudaError_t e = cudaSuccess;
+  for (int l = 0; l < lanes && e == cudaSuccess; ++l) {
+    if (l > 0 && !p->lane_st[l]) e = cudaStreamCreateWithFlags(&p->lane_st[l], cudaStreamNonBlocking);
+    if (e == cudaSuccess && !p->lane_ev[l]) e = cudaEventCreateWithFlags(&p->lane_ev[l], cudaEventDisableTiming);
+  }
+  cudaSetDevice(cur);
+  if (e != cudaSuccess) return fail(GL_ERR_CUDA, "lane streams: %s", cudaGetErrorString(e));
+  // lanes x groups of ceil(max_units / lanes) units: the workspace stays about
+  // the size of one group of max_units
+  const int g = (p->d.max_units + lanes - 1) / lanes;
+  p->lane_bytes = layout_units(p, g);
+  p->ws_total = (size_t)lanes * p->lane_bytes;
+  p->lanes = lanes;
   return GL_OK;
 }
 
@@ -1774,7 +1820,6 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
     cplx* P2 = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 9 * B2.w * ncy3 * sizeof(cplx)));
     cplx* QO = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 4 * B3.w * ncy3 * sizeof(cplx)));
     cplx* RO = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 4 * pl3 * sizeof(cplx)));
-    cplx* FO = reinterpret_cast<cplx*>(scratch + bo.take((size_t)nuj * 2 * pl3 * sizeof(cplx)));
     {
       ColArgs a;
       std::memset(&a, 0, sizeof a);
@@ -1853,19 +1898,17 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       c.box = B3;
       c.in = RO;
       c.maxin = maxRO;
-      c.out = FO;
       c.maxout = maxF;
       c.mask = s3;
       c.floor_rel = p->floor_rel;
       c.nsub = J;
       dim3 g(grid_for(pl3, T, 128), nuj);
       {
-        LaunchScope ls_("acc_outer_combine_kernel", st, 0.0);
-        acc_outer_combine_kernel<<<g, T, 0, st>>>(c);
+        LaunchScope ls_("acc_outer_max_kernel", st, 0.0);
+        acc_outer_max_kernel<<<g, T, 0, st>>>(c);
       }
-      LAUNCH_CHECK("acc_outer_combine_kernel");
+      LAUNCH_CHECK("acc_outer_max_kernel");
       c.out = out33;
-      c.extra = FO;
       c.nodes = dn + 3 * MAX_RANK;
       c.weights = dn + 7 * MAX_RANK;
       c.nnodes = J;
@@ -2728,14 +2771,44 @@ extern "C" gl_status gl_execute(gl_plan* p, int n_units, const void* d_spectra, 
                                                    : (size_t)p->b1.w * p->b1.h;
   const size_t out_unit = (size_t)p->ncomp * p->d.nx * p->d.ny *
                           (p->d.output == GL_OUT_REAL ? sizeof(double) : sizeof(cplx));
-  for (int u0 = 0; u0 < n_units; u0 += p->group) {
+  const int ngroups = (n_units + p->group - 1) / p->group;
+  const int L = std::min(p->lanes, ngroups);
+  if (L <= 1) {
+    for (int u0 = 0; u0 < n_units; u0 += p->group) {
+      const int gu = std::min(p->group, n_units - u0);
+      const void* in = reinterpret_cast<const cplx*>(d_spectra) + (size_t)u0 * in_unit;
+      void* outp = reinterpret_cast<char*>(d_outputs) + (size_t)u0 * out_unit;
+      gl_status s = run_group(p, gu, in, layout, outp, d_ws, d_status ? d_status + u0 : nullptr, st);
+      if (s != GL_OK) return s;
+    }
+    return GL_OK;
+  }
+  // concurrent lanes: group i runs on lane i mod L in that lane's workspace
+  // region; the lanes start after the work already on the caller's stream and
+  // the caller's stream continues after all of them (also inside a stream
+  // capture, where this is a fork/join of graph branches)
+  std::lock_guard<std::mutex> lk(p->lane_mu);
+  CUDA_TRY(cudaEventRecord(p->lane_ev[0], st));
+  for (int l = 1; l < L; ++l) CUDA_TRY(cudaStreamWaitEvent(p->lane_st[l], p->lane_ev[0], 0));
+  gl_status s = GL_OK;
+  for (int gi = 0; gi < ngroups && s == GL_OK; ++gi) {
+    const int l = gi % L;
+    const int u0 = gi * p->group;
     const int gu = std::min(p->group, n_units - u0);
     const void* in = reinterpret_cast<const cplx*>(d_spectra) + (size_t)u0 * in_unit;
     void* outp = reinterpret_cast<char*>(d_outputs) + (size_t)u0 * out_unit;
-    gl_status s = run_group(p, gu, in, layout, outp, d_ws, d_status ? d_status + u0 : nullptr, st);
-    if (s != GL_OK) return s;
+    void* ws = reinterpret_cast<char*>(d_ws) + (size_t)l * p->lane_bytes;
+    s = run_group(p, gu, in, layout, outp, ws, d_status ? d_status + u0 : nullptr,
+                  l == 0 ? st : p->lane_st[l]);
   }
-  return GL_OK;
+  // joined even after a failed launch, so that the caller's stream never runs
+  // ahead of lane work already queued
+  for (int l = 1; l < L; ++l) {
+    const cudaError_t e1 = cudaEventRecord(p->lane_ev[l], p->lane_st[l]);
+    const cudaError_t e2 = e1 == cudaSuccess ? cudaStreamWaitEvent(st, p->lane_ev[l], 0) : e1;
+    if (e2 != cudaSuccess && s == GL_OK) s = fail(GL_ERR_CUDA, "lane join: %s", cudaGetErrorString(e2));
+  }
+  return s;
 }
 
 // ---------------------------------------------------------------------------

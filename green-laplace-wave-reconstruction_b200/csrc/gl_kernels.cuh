@@ -1177,29 +1177,42 @@ __global__ void __launch_bounds__(256, 4) acc_inner_kernel(AccArgs a) {
   }
 }
 
-// order-3 outer combine: floors of the four forcing spectra, then the psi
-// forcings fk + A c and fd - c_t with their own maxima (_order3.py:103-122).
-__global__ void acc_outer_combine_kernel(AccArgs a) {
+// The order-3 outer forcings of one (unit, outer node) at bin i: the four
+// forcing spectra fk, fd, c, c_t with their roundoff floors, and the psi
+// forcings fk + A c and fd - c_t (_order3.py:103-122).  Written with explicit
+// fused multiply-adds so that the two kernels that form them (the maxima and
+// the accumulation) round them identically.
+struct OuterForcing {
+  cplx fk, fd, kpsi, dpsi;
+};
+
+GL_D OuterForcing outer_forcing(const cplx* src, int plane, int i, double ga, double floor_rel,
+                                const unsigned long long* mx) {
+  OuterForcing o;
+  o.fk = floored(src[i], floor_rel, mx[0]);
+  o.fd = floored(src[plane + i], floor_rel, mx[1]);
+  const cplx c = floored(src[2 * plane + i], floor_rel, mx[2]);
+  const cplx ct = floored(src[3 * plane + i], floor_rel, mx[3]);
+  o.kpsi = cmk(__fma_rn(ga, c.x, o.fk.x), __fma_rn(ga, c.y, o.fk.y));
+  o.dpsi = csub(o.fd, ct);
+  return o;
+}
+
+// order-3 outer forcing maxima: the maxima of |fk + A c| and |fd - c_t| over
+// the box, which set those forcings' own roundoff floors.  The forcings
+// themselves are formed again by acc_outer_kernel from the same spectra, so
+// they never travel through memory.
+__global__ void acc_outer_max_kernel(AccArgs a) {
   const int uj = blockIdx.y;
   const int plane = a.box.w * a.box.h;
-  cplx* src = const_cast<cplx*>(a.in) + (size_t)uj * 4 * plane;
+  const cplx* src = a.in + (size_t)uj * 4 * plane;
   double l0 = 0.0, l1 = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
-    BinGeo g = load_geo(a.geo, plane, i);
-    cplx fk = floored(src[i], a.floor_rel, a.maxin[uj * 4 + 0]);
-    cplx fd = floored(src[plane + i], a.floor_rel, a.maxin[uj * 4 + 1]);
-    cplx c = floored(src[2 * plane + i], a.floor_rel, a.maxin[uj * 4 + 2]);
-    cplx ct = floored(src[3 * plane + i], a.floor_rel, a.maxin[uj * 4 + 3]);
-    src[i] = fk;
-    src[plane + i] = fd;
-    cplx kpsi = cadd(fk, cscale(g.a, c));
-    cplx dpsi = csub(fd, ct);
-    // both already vanish off the triple support (their inputs were masked)
-    cplx* dst = a.out + (size_t)uj * 2 * plane;
-    dst[i] = kpsi;
-    dst[plane + i] = dpsi;
-    l0 = keep_max_abs(l0, kpsi);
-    l1 = keep_max_abs(l1, dpsi);
+    const OuterForcing o = outer_forcing(src, plane, i, a.geo[4 * plane + i], a.floor_rel,
+                                         a.maxin + uj * 4);
+    // both vanish off the triple support (their inputs were masked)
+    l0 = keep_max_abs(l0, o.kpsi);
+    l1 = keep_max_abs(l1, o.dpsi);
   }
   for (int o = 16; o > 0; o >>= 1) {
     const double o0 = __shfl_xor_sync(0xffffffffu, l0, o);
@@ -1213,8 +1226,9 @@ __global__ void acc_outer_combine_kernel(AccArgs a) {
   }
 }
 
-// order-3 outer accumulation into eta33 / psi33 spectra (_order3.py:124-138).
-// `extra` holds the psi forcings, `in` the floored fk, fd.
+// order-3 outer accumulation into eta33 / psi33 spectra (_order3.py:124-138):
+// `in` holds the four forcing spectra of each outer node, `maxin` their
+// maxima and `maxpsi` the psi forcings' maxima (acc_outer_max_kernel).
 __global__ void acc_outer_kernel(AccArgs a, const unsigned long long* maxpsi) {
   const int unit = blockIdx.y;
   const int plane = a.box.w * a.box.h;
@@ -1236,12 +1250,11 @@ __global__ void acc_outer_kernel(AccArgs a, const unsigned long long* maxpsi) {
       const double sh = sinh_over_root(g.sqa, tau);
       const double ch = cosh(g.sqa * tau);
       const double coef = s_coef[j];
-      const cplx* fsrc = a.in + (size_t)uj * 4 * plane;
-      const cplx fk = fsrc[i], fd = fsrc[plane + i];
-      const cplx* psrc = a.extra + (size_t)uj * 2 * plane;
-      const cplx kpsi = floored(psrc[i], a.floor_rel, maxpsi[uj * 2 + 0]);
-      const cplx dpsi = floored(psrc[plane + i], a.floor_rel, maxpsi[uj * 2 + 1]);
-      cplx te = csub(cscale(g.a * sh, fd), cmul(cmk(0.0, ch), fk));
+      const OuterForcing o = outer_forcing(a.in + (size_t)uj * 4 * plane, plane, i, g.a,
+                                           a.floor_rel, a.maxin + uj * 4);
+      const cplx kpsi = floored(o.kpsi, a.floor_rel, maxpsi[uj * 2 + 0]);
+      const cplx dpsi = floored(o.dpsi, a.floor_rel, maxpsi[uj * 2 + 1]);
+      cplx te = csub(cscale(g.a * sh, o.fd), cmul(cmk(0.0, ch), o.fk));
       cplx tp = csub(cmul(cmk(0.0, -ch), dpsi), cscale(sh, kpsi));
       eta = cadd(eta, cscale(coef, te));
       psi = cadd(psi, cscale(coef, tp));

@@ -33,6 +33,7 @@ COMP_NAMES = {COMP_ETA11: "eta11", COMP_PSI11: "psi11", COMP_ETA22: "eta22",
 GRID_COMPACT, GRID_REFERENCE = 0, 1
 OUT_COMPLEX, OUT_REAL = 0, 1
 SPECTRA_FULL, SPECTRA_BOX = 0, 1
+MAX_LANES = 8  # GL_MAX_LANES
 
 
 class PlanDesc(C.Structure):
@@ -117,6 +118,7 @@ SIGNATURES = {
     "gl_workspace_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "gl_plan_set_wait_test": (C.c_int, [C.c_void_p, C.c_uint, C.c_longlong]),
     "gl_plan_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(Tuning)]),
+    "gl_plan_set_lanes": (C.c_int, [C.c_void_p, C.c_int]),
     "gl_deposit_modes": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "gl_execute": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,

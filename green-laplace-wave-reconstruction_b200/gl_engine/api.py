@@ -203,6 +203,8 @@ class Plan:
             _engine_call(self.lib.gl_workspace_size(handle, C.byref(size)))
             self.workspace_bytes = int(size.value)
             self._workspace = None
+            self._retired: list[torch.Tensor] = []
+            self.lanes = 1
 
     @property
     def workspace(self) -> torch.Tensor:
@@ -226,6 +228,23 @@ class Plan:
         t = _lib.Tuning(pair_row_groups, triple_row_groups, col_block_columns)
         _engine_call(self.lib.gl_plan_set_tuning(self.handle, C.byref(t)))
         self.tuning = (pair_row_groups, triple_row_groups, col_block_columns)
+
+    def set_lanes(self, lanes: int) -> None:
+        """Run this plan's unit groups on ``lanes`` concurrent streams
+        (``gl_plan_set_lanes``): groups of ceil(max_units / lanes) units, group
+        i on lane i mod lanes, bitwise the same outputs.  Re-sizes the
+        workspace."""
+        with torch.cuda.device(self.device):
+            _engine_call(self.lib.gl_plan_set_lanes(self.handle, int(lanes)))
+            size = C.c_size_t()
+            _engine_call(self.lib.gl_workspace_size(self.handle, C.byref(size)))
+        self.workspace_bytes = int(size.value)
+        if self._workspace is not None:
+            # graphs captured before this call keep launching into the old
+            # workspace with the old layout: keep it alive with the plan
+            self._retired.append(self._workspace)
+        self._workspace = None
+        self.lanes = min(int(lanes), int(self.desc.max_units))
 
     def _ws_ptr(self) -> int:
         ptr = self.workspace.data_ptr()

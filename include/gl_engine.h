@@ -187,6 +187,23 @@ typedef struct gl_tuning {
 } gl_tuning;
 gl_status gl_plan_set_tuning(gl_plan* plan, const gl_tuning* tuning);
 
+/* Concurrent lanes of an order-1..3 plan (no counterpart in the reference,
+ * whose Python evaluates one snapshot at a time).  With lanes = L > 1,
+ * gl_execute splits its units into groups of ceil(max_units / L) and runs
+ * group i on lane i mod L: lane 0 on the caller's stream, the others on
+ * streams the plan owns, forked from the caller's stream by an event and
+ * joined back to it before gl_execute returns (inside a stream capture these
+ * are parallel branches of the graph).  One stage's kernels then overlap
+ * another group's, e.g. the memory-bound floor/accumulation kernels with the
+ * transforms.  Outputs are bitwise those of lanes = 1.  The workspace becomes
+ * L regions of one group each (about the size of one max_units group):
+ * query gl_workspace_size again after this call.  1 <= lanes <= GL_MAX_LANES
+ * (more lanes than max_units run as max_units lanes of one unit); eta44
+ * plans return GL_ERR_UNSUPPORTED.  Not to be called while a
+ * gl_execute on the same plan is being enqueued. */
+#define GL_MAX_LANES 8
+gl_status gl_plan_set_lanes(gl_plan* plan, int lanes);
+
 /* Failure-path test hook of the row stages' bounded waits (no counterpart in
  * the reference; its C++ has no device waits).  With surplus_bytes > 0 every
  * order-2/3 row launch of this plan expects that many bytes more than its
