@@ -1292,24 +1292,46 @@ struct OutArgs {
 // kernel.
 template <bool REAL>
 __global__ void __launch_bounds__(256, 2) out_row_kernel(OutArgs a, const cplx* __restrict__ tw) {
-  extern __shared__ cplx smem[];
+  extern __shared__ __align__(128) cplx smem[];
+  __shared__ __align__(8) unsigned long long stage_bar;
   const int n = a.nx;
   const int L = padded_len(n);
   int g, G;
   const FftGroup f = fft_group(n, a.log2nx, g, G);
-  const int y = blockIdx.x * G + g;
+  const int y0 = blockIdx.x * G;
+  const int y = y0 + g;
   const int uc = blockIdx.y;
   const int unit = uc / a.ncomp, comp = uc % a.ncomp;
   const bool active = y < a.ny;
   const int yy = active ? y : 0;
   cplx* buf = smem + (size_t)g * L;
-  const cplx* row = a.in + ((size_t)uc * a.ny + yy) * a.w;
+  // Stage the block's input rows (w box columns each) into the front of
+  // their groups' row buffers with bulk async copies issued at block start;
+  // the first transform pass reads them into registers before the group
+  // writes the padded row over them.
+  const uint32_t bar = smem_u32(&stage_bar);
+  if (threadIdx.x == 0) mbar_init(bar, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nrows = min(G, a.ny - y0);
+    const uint32_t bytes = (uint32_t)(a.w * sizeof(cplx));
+    mbar_arrive_expect_tx(bar, bytes * (uint32_t)nrows);
+    for (int r = 0; r < nrows; ++r)
+      bulk_g2s(smem_u32(smem + (size_t)r * L), a.in + ((size_t)uc * a.ny + y0 + r) * a.w, bytes, bar);
+  }
+  if (__syncthreads_or(!mbar_wait_bounded(bar, 0, BULK_WAIT_CYCLES))) {
+    // a copy never landed: flag the unit, give the copies one more bounded
+    // wait so none is left writing this block's shared memory, and leave
+    if (threadIdx.x == 0 && a.us) atomicCAS(&a.us[unit].status, 0, (int)GL_ERR_TIMEOUT);
+    mbar_wait_bounded(bar, 0, BULK_WAIT_CYCLES);
+    return;
+  }
   const double s = a.comp_scale ? a.comp_scale[comp] : a.scale_value;
   const size_t base = ((size_t)unit * a.out_ncomp + a.comp_offset + comp) * (size_t)a.ny * n +
                       (size_t)yy * n;
   auto load = [&](int xb) -> cplx {
     const int xi = wrap(xb - a.x0, n);
-    return xi < a.w ? row[xi] : czero();
+    return xi < a.w ? buf[xi] : czero();  // staged box row
   };
   bool bad = false;  // the output check of the unit's status, folded into the store
   if constexpr (REAL) {

@@ -117,13 +117,15 @@ gl_status launch_out_rows(const OutArgs& a0, int nuc, cudaStream_t st, const cpl
   const double bytes = (double)nuc * a.w * a.ny * sizeof(cplx) +
                        (double)nuc * a.nx * a.ny * (a.real_only ? sizeof(double) : sizeof(cplx));
   LaunchScope ls("out_row_kernel", st, bytes);
-  if (a.real_only) {
-    ensure_smem_attr((const void*)out_row_kernel<true>, (int)SMEM_LIMIT);
+  // the kernel's static shared memory (its mbarrier) comes out of the same
+  // 227 KB as the dynamic rows
+  const void* k = a.real_only ? (const void*)out_row_kernel<true> : (const void*)out_row_kernel<false>;
+  const cudaError_t e = ensure_smem_attr(k, (int)ROW_SMEM_LIMIT);
+  if (e != cudaSuccess) return fail(GL_ERR_CUDA, "out_row_kernel shared-memory limit: %s", cudaGetErrorString(e));
+  if (a.real_only)
     out_row_kernel<true><<<grid, 256, smem, st>>>(a, tw);
-  } else {
-    ensure_smem_attr((const void*)out_row_kernel<false>, (int)SMEM_LIMIT);
+  else
     out_row_kernel<false><<<grid, 256, smem, st>>>(a, tw);
-  }
   LAUNCH_CHECK("out_row_kernel");
   return GL_OK;
 }
