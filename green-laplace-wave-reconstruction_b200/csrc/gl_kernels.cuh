@@ -1290,8 +1290,8 @@ struct OutArgs {
 // columns) and writes scaled complex values or (REAL, OutArgs::real_only)
 // real parts; one instantiation per output type keeps one store path per
 // kernel.
-template <bool REAL>
-__global__ void __launch_bounds__(256, 2) out_row_kernel(OutArgs a, const cplx* __restrict__ tw) {
+template <bool REAL, bool B192 = false>
+__global__ void __launch_bounds__(B192 ? 192 : 256, 2) out_row_kernel(OutArgs a, const cplx* __restrict__ tw) {
   extern __shared__ __align__(128) cplx smem[];
   __shared__ __align__(8) unsigned long long stage_bar;
   const int n = a.nx;

@@ -110,22 +110,31 @@ gl_status launch_row(const RowArgs& a, int njobs, cudaStream_t st, const cplx* t
 
 gl_status launch_out_rows(const OutArgs& a0, int nuc, cudaStream_t st, const cplx* tw) {
   OutArgs a = a0;
-  const int G = 256 / (a.nx / 16);
+  // rows of up to 1024 points run in 192-thread blocks: two such blocks per
+  // SM leave each thread 168 registers (the 256-thread form is held to 128
+  // and spills ~180 bytes), for 12 instead of 16 resident warps (same-box
+  // A/B at 1024^2: the kernel 7 % faster)
+  const int T = a.nx / 16;
+  const bool b192 = T <= 64;
+  const int threads = b192 ? 192 : 256;
+  const int G = threads / T;
   a.rows = G;
   const size_t smem = (size_t)G * padded_len(a.nx) * sizeof(cplx);
   dim3 grid((a.ny + G - 1) / G, nuc);
   const double bytes = (double)nuc * a.w * a.ny * sizeof(cplx) +
                        (double)nuc * a.nx * a.ny * (a.real_only ? sizeof(double) : sizeof(cplx));
   LaunchScope ls("out_row_kernel", st, bytes);
-  // the kernel's static shared memory (its mbarrier) comes out of the same
-  // 227 KB as the dynamic rows
-  const void* k = a.real_only ? (const void*)out_row_kernel<true> : (const void*)out_row_kernel<false>;
+  const void* k = a.real_only ? (b192 ? (const void*)out_row_kernel<true, true> : (const void*)out_row_kernel<true>)
+                              : (b192 ? (const void*)out_row_kernel<false, true> : (const void*)out_row_kernel<false>);
   const cudaError_t e = ensure_smem_attr(k, (int)ROW_SMEM_LIMIT);
   if (e != cudaSuccess) return fail(GL_ERR_CUDA, "out_row_kernel shared-memory limit: %s", cudaGetErrorString(e));
-  if (a.real_only)
-    out_row_kernel<true><<<grid, 256, smem, st>>>(a, tw);
-  else
-    out_row_kernel<false><<<grid, 256, smem, st>>>(a, tw);
+  if (a.real_only) {
+    if (b192) out_row_kernel<true, true><<<grid, 192, smem, st>>>(a, tw);
+    else out_row_kernel<true><<<grid, 256, smem, st>>>(a, tw);
+  } else {
+    if (b192) out_row_kernel<false, true><<<grid, 192, smem, st>>>(a, tw);
+    else out_row_kernel<false><<<grid, 256, smem, st>>>(a, tw);
+  }
   LAUNCH_CHECK("out_row_kernel");
   return GL_OK;
 }

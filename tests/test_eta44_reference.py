@@ -82,7 +82,9 @@ def test_split_parts_match_reference_executor(tmp_path, outer, part):
 @pytest.mark.gpu
 @needs_ref
 @pytest.mark.parametrize("n,seed,count,dk,peak,rank", [
-    (32, 8, 8, 0.3, 1.0, 10),
+    # (the engine refuses grids on which the quartic support reaches Nyquist,
+    # where the executor aliases silently, so these grids leave it room)
+    (64, 8, 8, 0.3, 1.0, 10),
     (64, 9, 10, 0.2, 1.2, 6),
     (64, 9, 10, 0.2, 1.2, 8),
 ])
