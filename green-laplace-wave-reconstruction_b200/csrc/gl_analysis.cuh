@@ -69,16 +69,34 @@ GL_D unsigned long long window64(const unsigned long long* row, int words, int n
   return (lo >> sh) | (hi << (64 - sh));
 }
 
+// First and last set bit of a row of `words` words (32767, -32768 when empty).
+GL_D void row_extent(const unsigned long long* row, int words, int& first, int& last) {
+  first = 32767;
+  last = -32768;
+  for (int w = 0; w < words; ++w) {
+    const unsigned long long v = row[w];
+    if (v == 0ull) continue;
+    if (first == 32767) first = 64 * w + __ffsll((long long)v) - 1;
+    last = 64 * w + 63 - __clzll((long long)v);
+  }
+}
+
 // out(oy, ox) = exists py,bx: A[py][bx] and B[oy-py][ox-bx]; A, B are
 // bitset rows with box origins a, b; the output box has origin a+b.
+// aext/bext: [row][2] first and last set column of each row of A and B (an
+// empty row holds (32767, -32768)); a row pair whose column ranges cannot
+// reach ox is skipped before its words are compared.
 GL_D bool minkowski_bin(const unsigned long long* A, int ha, int wa, int wwa,
                         const unsigned long long* Brev, int hb, int wb, int wwb,
-                        int ox, int oy) {
+                        int ox, int oy, const short* aext, const short* bext) {
   int py_lo = oy - (hb - 1);
   if (py_lo < 0) py_lo = 0;
   int py_hi = oy < ha - 1 ? oy : ha - 1;
   const int c = wb - 1 - ox;
   for (int py = py_lo; py <= py_hi; ++py) {
+    const int q = oy - py;
+    if (ox < (int)aext[2 * py] + (int)bext[2 * q] || ox > (int)aext[2 * py + 1] + (int)bext[2 * q + 1])
+      continue;
     const unsigned long long* arow = A + (size_t)py * wwa;
     const unsigned long long* brow = Brev + (size_t)(oy - py) * wwb;
     for (int i = 0; i < wwa; ++i) {

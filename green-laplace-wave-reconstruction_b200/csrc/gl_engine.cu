@@ -385,17 +385,38 @@ struct MinkArgs {
   int skip_dup;                 // 1: units flagged dup are filled by mink_copy_kernel instead
 };
 
+// Dynamic shared memory: 2 (ha + hb) shorts, the column extents of A's and
+// B's rows (each block derives them from the bit rows).
 __global__ void minkowski_kernel(MinkArgs m) {
+  extern __shared__ short ext[];
   const int job = blockIdx.y;
   if (m.skip_dup && m.slots[job].dup) return;
   const unsigned long long* A = m.a + job * m.a_job_stride;
   const unsigned long long* B = m.brev + job * m.b_job_stride;
   unsigned char* C = m.c + job * m.c_job_stride;
+  short* aext = ext;
+  short* bext = ext + 2 * m.ha;
+  for (int r = threadIdx.x; r < m.ha + m.hb; r += blockDim.x) {
+    int first, last;
+    if (r < m.ha) {
+      row_extent(A + (size_t)r * m.wwa, m.wwa, first, last);
+      aext[2 * r] = (short)first;
+      aext[2 * r + 1] = (short)last;
+    } else {
+      // reversed rows: bit j is column wb - 1 - j
+      const int q = r - m.ha;
+      row_extent(B + (size_t)q * m.wwb, m.wwb, first, last);
+      const bool empty = last < first;
+      bext[2 * q] = empty ? (short)32767 : (short)(m.wb - 1 - last);
+      bext[2 * q + 1] = empty ? (short)-32768 : (short)(m.wb - 1 - first);
+    }
+  }
+  __syncthreads();
   const int plane = m.hc * m.wc;
   double lmax = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
     const int ox = i % m.wc, oy = i / m.wc;
-    const bool in = minkowski_bin(A, m.ha, m.wa, m.wwa, B, m.hb, m.wb, m.wwb, ox, oy);
+    const bool in = minkowski_bin(A, m.ha, m.wa, m.wwa, B, m.hb, m.wb, m.wwb, ox, oy, aext, bext);
     C[i] = in ? 1 : 0;
     if (in && m.geoc) lmax = fmax(lmax, m.geoc[5 * plane + i]);
   }
@@ -1199,6 +1220,8 @@ static T* at(void* ws, size_t off) {
   return reinterpret_cast<T*>(reinterpret_cast<char*>(ws) + off);
 }
 
+static size_t mink_smem(const MinkArgs& m) { return (size_t)2 * (m.ha + m.hb) * sizeof(short); }
+
 static void mink_args(MinkArgs& m, const unsigned long long* a, int ha, int wa, int wwa,
                       const unsigned long long* brev, int hb, int wb, int wwb, unsigned char* c,
                       const double* geoc, UnitSlots* slots, int which) {
@@ -1410,7 +1433,7 @@ static gl_status analyse_group(gl_plan* p, int gu, const void* spectra, int layo
     dim3 g2(grid_for(pl2, T, 256), gu);
     {
       LaunchScope ls_("minkowski_kernel", st, 0.0);
-      minkowski_kernel<<<g2, T, 0, st>>>(m);
+      minkowski_kernel<<<g2, T, mink_smem(m), st>>>(m);
     }
     LAUNCH_CHECK("minkowski_kernel");
     if (gu > 1) {
@@ -1432,7 +1455,7 @@ static gl_status analyse_group(gl_plan* p, int gu, const void* spectra, int layo
     dim3 g3(grid_for(pl3, T, 512), gu);
     {
       LaunchScope ls_("minkowski_kernel", st, 0.0);
-      minkowski_kernel<<<g3, T, 0, st>>>(m);
+      minkowski_kernel<<<g3, T, mink_smem(m), st>>>(m);
     }
     LAUNCH_CHECK("minkowski_kernel");
     if (gu > 1) {
@@ -1460,7 +1483,7 @@ static gl_status analyse_group(gl_plan* p, int gu, const void* spectra, int layo
       dim3 g2(grid_for(pl2, T, 256), gu);
       {
         LaunchScope ls_("minkowski_kernel", st, 0.0);
-        minkowski_kernel<<<g2, T, 0, st>>>(m);
+        minkowski_kernel<<<g2, T, mink_smem(m), st>>>(m);
       }
       LAUNCH_CHECK("minkowski_kernel");
     }
@@ -1902,7 +1925,7 @@ static gl_status run_group(gl_plan* p, int gu, const void* spectra, int layout, 
       c.mask = s3;
       c.floor_rel = p->floor_rel;
       c.nsub = J;
-      dim3 g(grid_for(pl3, T, 128), nuj);
+      dim3 g(grid_for(pl3, T, 48), nuj);
       {
         LaunchScope ls_("acc_outer_max_kernel", st, 0.0);
         acc_outer_max_kernel<<<g, T, 0, st>>>(c);
@@ -2365,7 +2388,7 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     dim3 g2(grid_for(pl2, T, 256), gu);
     {
       LaunchScope ls_("minkowski_kernel", st, 0.0);
-      minkowski_kernel<<<g2, T, 0, st>>>(m);
+      minkowski_kernel<<<g2, T, mink_smem(m), st>>>(m);
     }
     LAUNCH_CHECK("minkowski_kernel");
     dim3 gb(grid_for(B2.h * p->ww2, T, 64), gu);
@@ -2378,7 +2401,7 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     dim3 g3(grid_for(pl3, T, 512), gu);
     {
       LaunchScope ls_("minkowski_kernel", st, 0.0);
-      minkowski_kernel<<<g3, T, 0, st>>>(m);
+      minkowski_kernel<<<g3, T, mink_smem(m), st>>>(m);
     }
     LAUNCH_CHECK("minkowski_kernel");
     dim3 gb3(grid_for(B3.h * p->ww3, T, 64), gu);
@@ -2391,7 +2414,7 @@ static gl_status e44_run(gl_plan* p, int gu, const void* spectra, int layout, in
     dim3 g4(grid_for(pl4, T, 512), gu);
     {
       LaunchScope ls_("minkowski_kernel", st, 0.0);
-      minkowski_kernel<<<g4, T, 0, st>>>(m);
+      minkowski_kernel<<<g4, T, mink_smem(m), st>>>(m);
     }
     LAUNCH_CHECK("minkowski_kernel");
   }
@@ -3329,7 +3352,7 @@ static gl_status run_adjoint_group(gl_plan* p, int gu, const void* spectra, int 
       aa.jobs_per_unit = Jo;
       aa.floor_rel = p->floor_rel;
       {
-        dim3 g(grid_for(pl3, T, 128), nuj);
+        dim3 g(grid_for(pl3, T, 48), nuj);
         LaunchScope ls_("adj_outer_kernel", st, 0.0);
         adj_outer_kernel<<<g, T, 0, st>>>(aa);
       }

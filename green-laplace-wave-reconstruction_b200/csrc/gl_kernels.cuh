@@ -1186,33 +1186,58 @@ struct OuterForcing {
   cplx fk, fd, kpsi, dpsi;
 };
 
-GL_D OuterForcing outer_forcing(const cplx* src, int plane, int i, double ga, double floor_rel,
-                                const unsigned long long* mx) {
+// From the four spectra's values v[0..3] = fk, fd, c, c_t at the bin.
+GL_D OuterForcing outer_forcing_of(const cplx* v, double ga, double floor_rel,
+                                   const unsigned long long* mx) {
   OuterForcing o;
-  o.fk = floored(src[i], floor_rel, mx[0]);
-  o.fd = floored(src[plane + i], floor_rel, mx[1]);
-  const cplx c = floored(src[2 * plane + i], floor_rel, mx[2]);
-  const cplx ct = floored(src[3 * plane + i], floor_rel, mx[3]);
+  o.fk = floored(v[0], floor_rel, mx[0]);
+  o.fd = floored(v[1], floor_rel, mx[1]);
+  const cplx c = floored(v[2], floor_rel, mx[2]);
+  const cplx ct = floored(v[3], floor_rel, mx[3]);
   o.kpsi = cmk(__fma_rn(ga, c.x, o.fk.x), __fma_rn(ga, c.y, o.fk.y));
   o.dpsi = csub(o.fd, ct);
   return o;
 }
 
+GL_D OuterForcing outer_forcing(const cplx* src, int plane, int i, double ga, double floor_rel,
+                                const unsigned long long* mx) {
+  const cplx v[4] = {src[i], src[plane + i], src[2 * plane + i], src[3 * plane + i]};
+  return outer_forcing_of(v, ga, floor_rel, mx);
+}
+
 // order-3 outer forcing maxima: the maxima of |fk + A c| and |fd - c_t| over
 // the box, which set those forcings' own roundoff floors.  The forcings
 // themselves are formed again by acc_outer_kernel from the same spectra, so
-// they never travel through memory.
+// they never travel through memory.  Each thread takes two bins per
+// iteration with all ten loads issued first (the kernel is a pure stream of
+// four planes); the launch keeps the grid small (48 blocks per unit and
+// outer node) so that few blocks share each maximum's atomic slot.
 __global__ void acc_outer_max_kernel(AccArgs a) {
   const int uj = blockIdx.y;
   const int plane = a.box.w * a.box.h;
   const cplx* src = a.in + (size_t)uj * 4 * plane;
+  const unsigned long long* mx = a.maxin + uj * 4;
   double l0 = 0.0, l1 = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
-    const OuterForcing o = outer_forcing(src, plane, i, a.geo[4 * plane + i], a.floor_rel,
-                                         a.maxin + uj * 4);
-    // both vanish off the triple support (their inputs were masked)
-    l0 = keep_max_abs(l0, o.kpsi);
-    l1 = keep_max_abs(l1, o.dpsi);
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += 2 * stride) {
+    const bool two = i + stride < plane;
+    const int i2 = two ? i + stride : i;
+    cplx v[8];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      v[k] = __ldg(src + (size_t)k * plane + i);
+      v[4 + k] = __ldg(src + (size_t)k * plane + i2);
+    }
+    const double ga0 = __ldg(a.geo + 4 * plane + i), ga1 = __ldg(a.geo + 4 * plane + i2);
+    // both forcings vanish off the triple support (their inputs were masked)
+    const OuterForcing o0 = outer_forcing_of(v, ga0, a.floor_rel, mx);
+    l0 = keep_max_abs(l0, o0.kpsi);
+    l1 = keep_max_abs(l1, o0.dpsi);
+    if (two) {
+      const OuterForcing o1 = outer_forcing_of(v + 4, ga1, a.floor_rel, mx);
+      l0 = keep_max_abs(l0, o1.kpsi);
+      l1 = keep_max_abs(l1, o1.dpsi);
+    }
   }
   for (int o = 16; o > 0; o >>= 1) {
     const double o0 = __shfl_xor_sync(0xffffffffu, l0, o);
