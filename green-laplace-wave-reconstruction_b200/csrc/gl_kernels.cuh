@@ -1139,7 +1139,14 @@ __global__ void __launch_bounds__(256, 4) acc_inner_kernel(AccArgs a) {
       const int i = i0 + b;
       const int uj = unit * J + j;
       double local = 0.0;
-      if (i < plane) {
+      if (i < plane && !a.mask[(size_t)unit * plane + i]) {
+        // off the pair support the four spectra are zero: no loads, no sums
+        cplx* dst = a.out + (size_t)uj * 4 * plane;
+        dst[i] = czero();
+        dst[plane + i] = czero();
+        dst[2 * plane + i] = czero();
+        dst[3 * plane + i] = czero();
+      } else if (i < plane) {
         const double ga = a.geo[4 * plane + i];
         cplx e = czero(), et = czero(), p = czero(), pt = czero();
         for (int ii = 0; ii < I; ++ii) {
@@ -1158,7 +1165,6 @@ __global__ void __launch_bounds__(256, 4) acc_inner_kernel(AccArgs a) {
           p = cadd(p, cmul(cmk(0.0, coef), csub(cscale(ch, sd), cscale(sh, sk))));
           pt = cadd(pt, cscale(coef, csub(cscale(ch, sdt), cscale(sh, skt))));
         }
-        if (!a.mask[(size_t)unit * plane + i]) { e = czero(); et = czero(); p = czero(); pt = czero(); }
         cplx* dst = a.out + (size_t)uj * 4 * plane;
         dst[i] = e;
         dst[plane + i] = et;
@@ -1267,6 +1273,13 @@ __global__ void acc_outer_kernel(AccArgs a, const unsigned long long* maxpsi) {
   }
   __syncthreads();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < plane; i += gridDim.x * blockDim.x) {
+    // off the triple support the output is zero: the bin skips its loads
+    // and node responses
+    if (!a.mask[(size_t)unit * plane + i]) {
+      a.out[((size_t)unit * 2 + 0) * plane + i] = czero();
+      a.out[((size_t)unit * 2 + 1) * plane + i] = czero();
+      continue;
+    }
     BinGeo g = load_geo(a.geo, plane, i);
     cplx eta = czero(), psi = czero();
     for (int j = 0; j < a.nnodes; ++j) {
@@ -1284,7 +1297,6 @@ __global__ void acc_outer_kernel(AccArgs a, const unsigned long long* maxpsi) {
       eta = cadd(eta, cscale(coef, te));
       psi = cadd(psi, cscale(coef, tp));
     }
-    if (!a.mask[(size_t)unit * plane + i]) { eta = czero(); psi = czero(); }
     a.out[((size_t)unit * 2 + 0) * plane + i] = eta;
     a.out[((size_t)unit * 2 + 1) * plane + i] = psi;
   }
