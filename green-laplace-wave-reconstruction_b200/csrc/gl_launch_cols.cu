@@ -53,12 +53,13 @@ gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, const cp
   // kinds that share one base across their banks (col_ifft_kernel)
   const bool shared_base = a.kind != COL_PLAIN && a.kind != COL_OUTER2 && a.kind != COL_FLOORED;
   const size_t smem = ((size_t)cw * padded_len(a.n) + (shared_base ? (size_t)cw * a.box.h : 0)) * sizeof(cplx);
-  // banks per block, spread evenly over grid.z: at most 6 for the inner
-  // stage (12 banks in 2 slices: its 16 jobs per unit give plenty of blocks,
-  // and fewer slices recompute the damped base less), at most 4 elsewhere
-  // (12 banks: 3 x 4, 9 banks: 3 x 3); same-box A/B at config 2: inner 6
-  // +0.5 %, outer first-order 6 and any stage at 2 or 3 slower
-  const int per = a.kind == COL_INNER ? 6 : 4;
+  // banks per block, spread evenly over grid.z: all of them for the inner
+  // stage (its 16 jobs per unit give plenty of blocks, and each block then
+  // computes its columns' damped base once), at most 4 elsewhere (12 banks:
+  // 3 x 4, 9 banks: 3 x 3); same-box A/Bs at config 2: inner in 2 slices
+  // of 6 +0.5 %, in one slice +1.0 %; the outer first-order banks in slices
+  // of 6, or any stage in slices of 2 or 3, slower or no faster
+  const int per = a.kind == COL_INNER ? a.nbanks : 4;
   const int nz = (a.nbanks + per - 1) / per;
   const int bpb = (a.nbanks + nz - 1) / nz;
   dim3 grid((a.box.w + cw - 1) / cw, njobs, (a.nbanks + bpb - 1) / bpb);
