@@ -56,7 +56,7 @@ gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, const cp
   // banks per block, spread evenly over grid.z: all of them for the inner
   // stage (its 16 jobs per unit give plenty of blocks, and each block then
   // computes its columns' damped base once), at most 4 elsewhere (12 banks:
-  // 3 x 4, 9 banks: 3 x 3); same-box A/Bs at config 2: inner in 2 slices
+  // 3 x 4, 9 banks: 3 x 3); same-box A/Bs on the 1024^2 order-3 workload: inner in 2 slices
   // of 6 +0.5 %, in one slice +1.0 %; the outer first-order banks in slices
   // of 6, or any stage in slices of 2 or 3, slower or no faster
   const int per = a.kind == COL_INNER ? a.nbanks : 4;
