@@ -98,6 +98,8 @@ def test_null_arguments_are_rejected():
     assert lib.gl_plan_create(None, None) == 1
     assert lib.gl_execute(None, 1, None, 0, None, None, 0, None, None) == 1
     assert lib.gl_workspace_size(None, None) == 1
+    assert lib.gl_plan_set_lanes(None, 2) == 1
+    assert lib.gl_plan_set_tuning(None, None) == 1
 
 
 @pytest.mark.parametrize("nx,ny", [(112, 112), (64, 98), (4100, 64), (8, 8)])
