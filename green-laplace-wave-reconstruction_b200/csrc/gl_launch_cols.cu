@@ -53,13 +53,18 @@ gl_status launch_col_ifft(const ColArgs& a, int njobs, cudaStream_t st, const cp
   // kinds that share one base across their banks (col_ifft_kernel)
   const bool shared_base = a.kind != COL_PLAIN && a.kind != COL_OUTER2 && a.kind != COL_FLOORED;
   const size_t smem = ((size_t)cw * padded_len(a.n) + (shared_base ? (size_t)cw * a.box.h : 0)) * sizeof(cplx);
-  // banks per block, spread evenly over grid.z: all of them for the inner
-  // stage (its 16 jobs per unit give plenty of blocks, and each block then
-  // computes its columns' damped base once), at most 4 elsewhere (12 banks:
-  // 3 x 4, 9 banks: 3 x 3); same-box A/Bs on the 1024^2 order-3 workload: inner in 2 slices
-  // of 6 +0.5 %, in one slice +1.0 %; the outer first-order banks in slices
-  // of 6, or any stage in slices of 2 or 3, slower or no faster
-  const int per = a.kind == COL_INNER ? a.nbanks : 4;
+  // banks per block, spread evenly over grid.z: at most 4 (12 banks: 3 x 4,
+  // 9 banks: 3 x 3), or all of them for the inner stage when one slice
+  // still gives at least two blocks per SM slot pair (each block then
+  // computes its columns' damped base once instead of once per slice).
+  // Same-box A/Bs on the 1024^2 order-3 workload (16 units in two lanes of
+  // 8: 640 blocks per slice): inner in one slice +1.0 %, in 2 slices of 6
+  // +0.5 %; the outer first-order banks in slices of 6, or any stage in
+  // slices of 2 or 3, slower or no faster.  A single 512^2 unit (64 blocks
+  // per slice) keeps the three slices: one slice left most SMs idle.
+  const int col_blocks = (a.box.w + cw - 1) / cw;
+  const bool one_slice = a.kind == COL_INNER && (long long)col_blocks * njobs >= 4LL * 148;
+  const int per = one_slice ? a.nbanks : 4;
   const int nz = (a.nbanks + per - 1) / per;
   const int bpb = (a.nbanks + nz - 1) / nz;
   dim3 grid((a.box.w + cw - 1) / cw, njobs, (a.nbanks + bpb - 1) / bpb);
